@@ -1,0 +1,73 @@
+"""ctypes binding of the in-tree native library `libchompack_b200.so`
+(host symbolic analysis + the sm_100a sweeps behind include/chompack_b200.h).
+
+There is no fallback: importing the package fails loudly when the library
+has not been built (`python chompack_b200/build.py` or
+`__graft_entry__.build()`).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchompack_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("chompack_b200 native library not built: %s is missing "
+                      "(run `python chompack_b200/build.py`)" % LIB_PATH)
+
+lib = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+
+i64 = ctypes.c_int64
+P64 = ctypes.POINTER(ctypes.c_int64)
+vp = ctypes.c_void_p
+MERGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, i64, i64, i64, i64)
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+sym_etree = _sig("chb_sym_etree", ctypes.c_int, [i64, P64, P64, P64])
+sym_post_order = _sig("chb_sym_post_order", ctypes.c_int, [i64, P64, P64])
+sym_counts = _sig("chb_sym_counts", ctypes.c_int, [i64, P64, P64, P64, P64, P64])
+sym_supernodes = _sig("chb_sym_supernodes", ctypes.c_int, [i64, P64, P64, P64, P64, P64, P64, P64])
+sym_amalgamate = _sig("chb_sym_amalgamate", ctypes.c_int,
+                      [i64, P64, P64, P64, P64, P64, P64, P64, i64, i64, MERGE_FN])
+sym_embed = _sig("chb_sym_embed", ctypes.c_int, [i64, P64, P64, P64, P64, P64, P64, P64, i64, P64, P64])
+sym_relative_idx = _sig("chb_sym_relative_idx", ctypes.c_int, [i64, P64, P64, P64, P64, P64, P64])
+amd_order = _sig("chb_amd_order", ctypes.c_int, [i64, P64, P64, P64])
+
+last_error = _sig("chb_last_error", ctypes.c_char_p, [])
+version = _sig("chb_version", ctypes.c_char_p, [])
+
+
+def ptr(a):
+    """int64 pointer to a C-contiguous int64 numpy array (or NULL for None)."""
+    if a is None:
+        return ctypes.cast(None, P64)
+    assert a.dtype == np.int64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(P64)
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = last_error()
+        raise RuntimeError("%s failed (code %d)%s" % (what, rc, (": " + msg.decode()) if msg else ""))
+
+# ---- plan / sweeps (include/chompack_b200.h)
+PPLAN = ctypes.c_void_p
+plan_create = _sig("chb_plan_create", ctypes.c_int,
+                   [i64, i64, P64, P64, P64, P64, P64, P64, P64, P64, P64, ctypes.c_int, ctypes.POINTER(PPLAN)])
+plan_destroy = _sig("chb_plan_destroy", ctypes.c_int, [PPLAN])
+workspace_size = _sig("chb_workspace_size", ctypes.c_int,
+                      [PPLAN, ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)])
+program_info = _sig("chb_program_info", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64])
+cholesky = _sig("chb_cholesky", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
+info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
+
+OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)

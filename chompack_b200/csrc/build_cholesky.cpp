@@ -1,0 +1,203 @@
+// Task program of the multifrontal Cholesky sweep (reference: cholesky.c:3-84).
+//
+// Per supernode k (front F = [blkval panel P, nj x nn, ld nj | update U_k,
+// na x na, ld na]) the reference does
+//   F := [blk, 0] + extend-add(children's U)          (cholesky.c:33-52)
+//   L11 = potrf(F11)                                  (:55)
+//   L21 = F21 * L11^{-T}                              (:61)
+//   U_k = F22 - L21 * L21^T                           (:64-69)
+//   blk21 = L21 * L11^{-1}                            (:72)
+// Here the nn columns are processed in 64-wide column blocks, right-looking:
+// POTRF of the diagonal tile (which also writes M_cc = L_cc^{-1}), TRSM of the
+// tiles below it as a GEMM with M_cc^T, and rank-64 updates of the tiles to
+// the right.  L21 goes to scratch S_k (na x nn), the Schur update U_k -= S S^T
+// is one K = nn GEMM per tile, and the second triangular solve becomes
+// blk21 = S_k * M with M = L11^{-1} assembled block-row by block-row
+// (M(c, j) = -M_cc * sum_{l=j}^{c-1} L(c, l) M(l, j)), so no tile of it has a
+// sequential dependency on its neighbours.
+#include "dag.h"
+
+namespace chb {
+
+int build_cholesky(const chb_plan& P, Program& prog) {
+  const int T = TILE;
+  const int CH = 32;  // front columns per extend-add task
+  const int64_t N = P.nsn;
+  DagBuilder B;
+
+  // workspace: update matrices first (shared layout), then per-front scratch
+  int64_t ws = P.upd_total;
+  std::vector<int64_t> scrS(N, -1), scrM(N, -1);
+  for (int64_t k = 0; k < N; k++) {
+    const FrontDesc& f = P.fronts[k];
+    const int NBc = ceil_div(f.nn, T);
+    if (f.na > 0) {
+      scrS[k] = ws;
+      ws += (int64_t)f.na * f.nn;
+    }
+    if (NBc > 1 || f.na > 0) {
+      scrM[k] = ws;
+      ws += (int64_t)f.nn * f.nn;
+    }
+  }
+  prog.ws_doubles = ws;
+
+  std::vector<int> uc_group(N, -1);
+  for (int64_t k = 0; k < N; k++)
+    if (P.fronts[k].na > 0) uc_group[k] = B.new_group();
+
+  std::vector<int> last_top, last_bot, trsm_top, trsm_prev, trsmb, last_mrow;
+  for (int64_t k = 0; k < N; k++) {
+    const FrontDesc& f = P.fronts[k];
+    const int nn = f.nn, na = f.na, nj = f.nj;
+    const int lv = f.level;
+    const int NBc = ceil_div(nn, T), NBb = ceil_div(na, T);
+    const int64_t blk = f.blk, upd = f.upd, S = scrS[k], M = scrM[k];
+    auto bw = [&](int c) { return std::min(T, nn - c * T); };  // column block width
+    auto bh = [&](int i) { return std::min(T, na - i * T); };  // bottom tile height
+
+    // --- extend-add (cholesky.c:33-52)
+    int asm_group = -1;
+    if (f.chend > f.chbeg || na > 0) {
+      asm_group = B.new_group();
+      for (int j0 = 0; j0 < nj; j0 += CH) {
+        Task t = make_task(T_ASM);
+        t.aux[0] = (int32_t)k;
+        t.aux[1] = j0;
+        t.aux[2] = std::min(nj, j0 + CH);
+        t.aux[3] = na > 0 ? 1 : 0;
+        int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group);
+        for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
+      }
+    }
+
+    last_top.assign((size_t)NBc * NBc, -1);
+    last_bot.assign((size_t)std::max(NBb, 1) * NBc, -1);
+    trsm_top.assign(NBc, -1);
+    trsm_prev.assign(NBc, -1);
+    trsmb.assign(std::max(NBb, 1), -1);
+    last_mrow.assign(NBc, -1);
+    int pot = -1;
+    for (int c = 0; c < NBc; c++) {
+      const int bc = bw(c);
+      const int cT = c * T;
+      // POTRF of the diagonal tile (+ M_cc when anything lies below it)
+      {
+        Task t = make_task(T_POTRF);
+        t.m = t.n = bc;
+        t.a = opnd(B_X, blk + (int64_t)cT * nj + cT, nj);
+        const bool inv = (cT + bc < nj);
+        t.aux[0] = cT;
+        t.aux[1] = inv ? 1 : 0;
+        if (inv) t.c = opnd(B_WS, M + (int64_t)cT * nn + cT, nn);
+        pot = B.add(t, {lv, c, 0, (int)k, 0, 0});
+        if (c == 0) B.wait_group(pot, asm_group);
+        else B.wait_task(pot, last_top[(size_t)c * NBc + c]);
+      }
+      const Operand Mcc = opnd(B_WS, M + (int64_t)cT * nn + cT, nn, OM_TRI_N, 0);
+      // TRSM of the top tiles below the diagonal: P(r,c) := P(r,c) * M_cc^T
+      for (int r = 0; r < NBc; r++) trsm_prev[r] = trsm_top[r];
+      for (int r = c + 1; r < NBc; r++) {
+        const int rT = r * T;
+        Operand pr = opnd(B_X, blk + (int64_t)cT * nj + rT, nj);
+        Task t = gemm(bw(r), bc, bc, 1.0, pr, Mcc, 0.0, pr);
+        int id = B.add(t, {lv, c, 1, (int)k, c, r});
+        B.wait_task(id, pot);
+        if (c > 0) B.wait_task(id, last_top[(size_t)r * NBc + c]);
+        trsm_top[r] = id;
+      }
+      // TRSM of the bottom tiles into S_k
+      for (int i = 0; i < NBb; i++) {
+        const int iT = i * T;
+        Operand pa = opnd(B_X, blk + (int64_t)cT * nj + nn + iT, nj);
+        Operand sc = opnd(B_WS, S + (int64_t)cT * na + iT, na);
+        Task t = gemm(bh(i), bc, bc, 1.0, pa, Mcc, 0.0, sc);
+        int id = B.add(t, {lv, c, 1, (int)k, c, NBc + i});
+        B.wait_task(id, pot);
+        if (c > 0) B.wait_task(id, last_bot[(size_t)i * NBc + c]);
+        trsmb[i] = id;
+      }
+      // block row c of M = L11^{-1} (needed for the second solve)
+      if (na > 0) {
+        for (int j = 0; j < c; j++) {
+          const int jT = j * T;
+          Task t = make_task(T_MROW);
+          t.m = bc;
+          t.n = T;
+          t.k = cT - jT;
+          t.alpha = -1.0;
+          t.a = opnd(B_X, blk + (int64_t)jT * nj + cT, nj);
+          t.b = opnd(B_WS, M + (int64_t)jT * nn + jT, nn, OM_TRI_T, 0);
+          t.c = opnd(B_WS, M + (int64_t)jT * nn + cT, nn);
+          const int64_t moff = M + (int64_t)cT * nn + cT;
+          t.aux[0] = B_WS;
+          t.aux[1] = nn;
+          t.aux[2] = (int32_t)(uint32_t)(moff & 0xffffffffLL);
+          t.aux[3] = (int32_t)(moff >> 32);
+          int id = B.add(t, {lv, c, 3, (int)k, j, 0});
+          B.wait_task(id, pot);
+          B.wait_task(id, trsm_prev[c]);
+          if (c - 1 > j) B.wait_task(id, last_mrow[j]);
+          last_mrow[j] = id;
+        }
+      }
+      // right-looking updates of the tiles right of column block c
+      for (int j = c + 1; j < NBc; j++) {
+        const int jT = j * T;
+        Operand pj = opnd(B_X, blk + (int64_t)cT * nj + jT, nj);
+        for (int r = j; r < NBc; r++) {
+          const int rT = r * T;
+          Operand pr = opnd(B_X, blk + (int64_t)cT * nj + rT, nj);
+          Operand cc = opnd(B_X, blk + (int64_t)jT * nj + rT, nj);
+          Task t = gemm(bw(r), bw(j), bc, -1.0, pr, pj, 1.0, cc, r == j, 0);
+          int id = B.add(t, {lv, c, 2, (int)k, j, r});
+          B.wait_task(id, trsm_top[r]);
+          B.wait_task(id, trsm_top[j]);
+          if (c > 0) B.wait_task(id, last_top[(size_t)r * NBc + j]);
+          last_top[(size_t)r * NBc + j] = id;
+        }
+        for (int i = 0; i < NBb; i++) {
+          const int iT = i * T;
+          Operand sa = opnd(B_WS, S + (int64_t)cT * na + iT, na);
+          Operand cc = opnd(B_X, blk + (int64_t)jT * nj + nn + iT, nj);
+          Task t = gemm(bh(i), bw(j), bc, -1.0, sa, pj, 1.0, cc);
+          int id = B.add(t, {lv, c, 2, (int)k, j, NBc + i});
+          B.wait_task(id, trsmb[i]);
+          B.wait_task(id, trsm_top[j]);
+          if (c > 0) B.wait_task(id, last_bot[(size_t)i * NBc + j]);
+          last_bot[(size_t)i * NBc + j] = id;
+        }
+      }
+    }
+    if (na == 0) continue;
+    // Schur complement U_k -= S_k S_k^T (cholesky.c:64-69)
+    for (int j = 0; j < NBb; j++) {
+      for (int i = j; i < NBb; i++) {
+        Operand sa = opnd(B_WS, S + i * T, na);
+        Operand sb = opnd(B_WS, S + j * T, na);
+        Operand cc = opnd(B_WS, upd + (int64_t)(j * T) * na + i * T, na);
+        Task t = gemm(bh(i), bh(j), nn, -1.0, sa, sb, 1.0, cc, i == j, 0);
+        int id = B.add(t, {lv, NBc, 0, (int)k, j, i}, uc_group[k]);
+        B.wait_task(id, trsmb[i]);
+        B.wait_task(id, trsmb[j]);
+      }
+    }
+    // blk21 = S_k * M  (= L21 L11^{-1}, cholesky.c:72)
+    for (int i = 0; i < NBb; i++) {
+      for (int j = 0; j < NBc; j++) {
+        const int jT = j * T, iT = i * T;
+        Operand sa = opnd(B_WS, S + (int64_t)jT * na + iT, na);
+        Operand mb = opnd(B_WS, M + (int64_t)jT * nn + jT, nn, OM_TRI_T, 0);
+        Operand cc = opnd(B_X, blk + (int64_t)jT * nj + nn + iT, nj);
+        Task t = gemm(bh(i), bw(j), nn - jT, 1.0, sa, mb, 0.0, cc);
+        int id = B.add(t, {lv, NBc, 1, (int)k, j, i});
+        B.wait_task(id, trsmb[i]);
+        B.wait_task(id, pot);
+        if (j < NBc - 1) B.wait_task(id, last_mrow[j]);
+      }
+    }
+  }
+  return B.finish(prog);
+}
+
+}  // namespace chb

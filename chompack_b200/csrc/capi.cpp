@@ -1,0 +1,52 @@
+// C ABI entry points of the numeric sweeps (include/chompack_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "../../include/chompack_b200.h"
+#include "internal.h"
+#include "plan.h"
+
+using namespace chb;
+
+namespace {
+
+int check_plan(chb_plan* plan) {
+  if (!plan) return set_error(-1, "null plan");
+  if (plan->device < 0) return set_error(-1, "plan was created without a device");
+  if (cudaSetDevice(plan->device) != cudaSuccess) return set_error(-3, "cudaSetDevice(%d) failed", plan->device);
+  return 0;
+}
+
+int run_op(chb_plan* plan, int op, int64_t k, int flags, double* const* bases, int nbases, void* work,
+           size_t work_bytes, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  Program* prog = get_program(plan, op, k, flags);
+  if (!prog) return -2;
+  return run_program(plan, prog, work, work_bytes, bases, nbases, (cudaStream_t)stream);
+}
+
+}  // namespace
+
+extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
+  double* bases[1] = {blkval};
+  return run_op(plan, CHB_OP_CHOLESKY, 0, 0, bases, 1, work, work_bytes, stream);
+}
+
+extern "C" int chb_info(chb_plan* plan, void* work, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) {
+    cudaError_t e = cudaGetLastError();
+    return set_error(-100 - (int)e, "stream synchronisation failed: %s", cudaGetErrorString(e));
+  }
+  int ctl[4];
+  if (cudaMemcpy(ctl, work, sizeof(ctl), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(-3, "cannot read the sweep status");
+  if (ctl[1] == DE_TIMEOUT) return set_error(-30, "a task wait timed out (%d CTAs)", ctl[3]);
+  if (ctl[1] != 0) return set_error(-31, "device error %d", ctl[1]);
+  return ctl[2];
+}

@@ -1,0 +1,161 @@
+// Helper for building task programs: tasks are created with provisional ids
+// and a scheduling key, then sorted by key into the final execution order.
+// Waits name either a task (wait until it has run) or a group counter (wait
+// until `target` member tasks have run).  finish() checks that every wait
+// points strictly backwards in the final order, which is what makes the
+// persistent schedule deadlock-free.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "internal.h"
+#include "plan.h"
+
+namespace chb {
+
+struct SchedKey {
+  int32_t level;   // height of the front in the supernodal tree (or sweep phase)
+  int32_t step;    // step of the blocked algorithm inside the front
+  int32_t rank;    // task kind inside a step
+  int32_t front;
+  int32_t j, i;    // tile coordinates
+  bool operator<(const SchedKey& o) const {
+    if (level != o.level) return level < o.level;
+    if (step != o.step) return step < o.step;
+    if (rank != o.rank) return rank < o.rank;
+    if (front != o.front) return front < o.front;
+    if (j != o.j) return j < o.j;
+    return i < o.i;
+  }
+};
+
+struct DagBuilder {
+  struct Wait {
+    int32_t id;      // task id, or group id when is_group
+    int32_t target;
+    bool is_group;
+  };
+  std::vector<Task> tasks;
+  std::vector<SchedKey> keys;
+  std::vector<std::vector<Wait>> waits;
+  std::vector<int32_t> group_of;   // provisional group of each task (-1)
+  std::vector<int32_t> group_size;
+
+  int new_group() {
+    group_size.push_back(0);
+    return (int)group_size.size() - 1;
+  }
+
+  int add(const Task& t, const SchedKey& key, int group = -1) {
+    tasks.push_back(t);
+    keys.push_back(key);
+    waits.emplace_back();
+    group_of.push_back(group);
+    if (group >= 0) group_size[group]++;
+    return (int)tasks.size() - 1;
+  }
+
+  void wait_task(int task, int dep) {
+    if (dep >= 0) waits[task].push_back({dep, 1, false});
+  }
+  // Wait for all members of a group (the group must be complete when the
+  // program is finished).
+  void wait_group(int task, int group) {
+    if (group >= 0) waits[task].push_back({group, -1, true});
+  }
+
+  // Sort into execution order and emit the device program.
+  int finish(Program& prog) {
+    const int nt = (int)tasks.size();
+    std::vector<int> order(nt);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+    std::vector<int> pos(nt);
+    for (int i = 0; i < nt; i++) pos[order[i]] = i;
+    // latest member position of each group
+    std::vector<int> gmax(group_size.size(), -1);
+    for (int t = 0; t < nt; t++)
+      if (group_of[t] >= 0) gmax[group_of[t]] = std::max(gmax[group_of[t]], pos[t]);
+    prog.tasks.resize(nt);
+    prog.waits.clear();
+    for (int i = 0; i < nt; i++) {
+      const int t = order[i];
+      Task tk = tasks[t];
+      tk.wait_off = (int32_t)prog.waits.size();
+      // de-duplicate waits
+      std::vector<int2> w;
+      for (const Wait& wt : waits[t]) {
+        int2 e;
+        if (wt.is_group) {
+          if (group_size[wt.id] == 0) continue;
+          if (gmax[wt.id] >= i)
+            return set_error(-20, "task graph: group wait does not point backwards (task %d)", i);
+          e.x = nt + wt.id;
+          e.y = group_size[wt.id];
+        } else {
+          if (pos[wt.id] >= i)
+            return set_error(-21, "task graph: wait does not point backwards (task %d -> %d)", i, pos[wt.id]);
+          e.x = pos[wt.id];
+          e.y = 1;
+        }
+        bool dup = false;
+        for (const int2& x : w)
+          if (x.x == e.x) { dup = true; break; }
+        if (!dup) w.push_back(e);
+      }
+      if (w.size() > 65535) return set_error(-22, "task graph: too many waits");
+      tk.nwait = (uint16_t)w.size();
+      tk.group = group_of[t] >= 0 ? nt + group_of[t] : -1;
+      prog.waits.insert(prog.waits.end(), w.begin(), w.end());
+      prog.tasks[i] = tk;
+    }
+    prog.ncounters = (int64_t)nt + (int64_t)group_size.size();
+    return 0;
+  }
+};
+
+inline Operand opnd(uint8_t base, int64_t off, int ld, uint8_t mode = OM_N, int diag = 0) {
+  Operand o;
+  std::memset(&o, 0, sizeof(o));
+  o.off = off;
+  o.ld = ld;
+  o.base = base;
+  o.mode = mode;
+  o.diag = diag;
+  return o;
+}
+
+inline Task make_task(uint8_t op) {
+  Task t;
+  std::memset(&t, 0, sizeof(t));
+  t.op = op;
+  t.group = -1;
+  t.alpha = 1.0;
+  t.beta = 0.0;
+  return t;
+}
+
+inline Task gemm(int m, int n, int k, double alpha, const Operand& a, const Operand& b, double beta,
+                 const Operand& c, bool lower = false, int cdiag = 0) {
+  Task t = make_task(T_GEMM);
+  t.m = m;
+  t.n = n;
+  t.k = k;
+  t.alpha = alpha;
+  t.beta = beta;
+  t.a = a;
+  t.b = b;
+  t.c = c;
+  t.cmode = lower ? CM_LOWER : CM_FULL;
+  t.cdiag = cdiag;
+  return t;
+}
+
+inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+}  // namespace chb

@@ -1,0 +1,121 @@
+// Task-graph engine shared by the host planner (plan.cpp) and the device
+// executor (engine.cu).
+//
+// Every numeric sweep is compiled on the host into a list of tile tasks in a
+// topological order.  One persistent kernel executes the list: each CTA
+// claims the next task with an atomic counter, waits (bounded) until the
+// tasks it depends on have signalled, runs it, and signals.  A task only
+// ever waits on tasks that come earlier in the list, so the smallest
+// unfinished claimed task can always run: the schedule cannot deadlock,
+// whatever the number of resident CTAs.
+#pragma once
+#include <cstdint>
+
+#include <vector_types.h>  // int2
+
+namespace chb {
+
+constexpr int TILE = 64;          // tile edge (rows/cols of a C tile)
+constexpr int NTHREADS = 128;     // threads per CTA (4 warps)
+constexpr int KC = 16;            // K chunk staged through shared memory
+constexpr int LDS = TILE + 4;     // padded leading dimension of staged tiles
+constexpr int MAX_BASES = 64;     // base-pointer slots (see Base below)
+
+// Base-pointer slots a task operand refers to.
+enum Base : uint8_t {
+  B_X = 0,      // the cspmatrix values being transformed in place
+  B_WS = 1,     // the double-precision workspace
+  B_L = 2,      // factor values (hessian)
+  B_Y = 3,      // projected-inverse values (hessian)
+  B_RHS = 4,    // dense right-hand sides (trsm)
+  B_U0 = 5      // first of the U matrices (hessian): slot B_U0 + u
+};
+
+// How a GEMM operand is read.  A tile operand maps tile coordinates (r, k),
+// r in [0, 64), k in [0, K), to an element of a column-major matrix with
+// origin `off` and leading dimension `ld`.
+enum OpMode : uint8_t {
+  OM_N = 0,      // X[k*ld + r]
+  OM_T = 1,      // X[r*ld + k]
+  OM_TRI_N = 2,  // lower-triangular X read as OM_N: zero unless r + diag >= k
+  OM_TRI_T = 3,  // lower-triangular X read as OM_T: zero unless k + diag >= r
+  OM_SYM = 4     // symmetric X stored in its lower triangle: element (r+diag, k)
+};
+
+enum CMode : uint8_t {
+  CM_FULL = 0,   // write the whole m x n tile
+  CM_LOWER = 1   // write only entries with r + cdiag >= c (lower triangle)
+};
+
+enum TaskOp : uint8_t {
+  T_GEMM = 0,     // C = alpha * opA * opB^T + beta * C
+  T_POTRF = 1,    // Cholesky of a diagonal tile; optionally its inverse
+  T_ASM = 2,      // extend-add of child update matrices into a front
+  T_MROW = 3,     // C = alpha * M2 * (opA * opB^T); M2 lower-triangular tile
+  T_EXTRACT = 4,  // gather a child's update matrix out of its parent front
+  T_COPY = 5,     // strided copy / scale / zero of a tile
+  T_INV = 6,      // inverse of a lower-triangular diagonal tile
+  T_RPOTRF = 7,   // "reverse" Cholesky: S = L^T L with L lower (diag tile)
+  T_HOUSE = 8,    // Householder reduction of a factored update (one child)
+  T_VEC = 9       // vector ops for the triangular solve sweep
+};
+
+struct Operand {
+  int64_t off;    // element offset from the base pointer
+  int32_t ld;     // leading dimension
+  uint8_t base;   // Base slot
+  uint8_t mode;   // OpMode
+  int16_t pad;
+  int32_t diag;   // diagonal offset for OM_TRI_* / OM_SYM
+  int32_t pad2;   // OM_SYM: column offset of k = 0
+};
+
+struct Task {
+  uint8_t op;       // TaskOp
+  uint8_t cmode;    // CMode (GEMM / MROW)
+  uint16_t nwait;   // number of (counter, target) waits
+  int32_t wait_off; // first wait in the waits array
+  int32_t group;    // extra counter signalled on completion (-1: none)
+  int32_t m, n, k;  // C tile extent and inner dimension
+  int32_t cdiag;    // diagonal offset for CM_LOWER
+  int32_t aux[4];   // op-specific integers (front id, column range, ...)
+  double alpha, beta;
+  Operand a, b, c;
+};
+
+// Per-supernode description used by the gather/scatter tasks.
+struct FrontDesc {
+  int32_t nn, na, nj;   // |N_k|, |A_k|, nn + na
+  int32_t relptr;       // first relative index of this supernode
+  int32_t chbeg, chend; // children are chidx[chbeg:chend]
+  int32_t parent;       // snpar
+  int32_t level;        // height in the supernodal tree
+  int64_t blk;          // blkptr[k]
+  int64_t upd;          // offset (doubles) of the update matrix in the workspace
+  int64_t scr;          // offset of per-front scratch in the workspace
+  int64_t scr2;         // second scratch offset
+};
+
+// Device-side run description (passed by value to the persistent kernel).
+struct RunArgs {
+  const Task* tasks;
+  int32_t ntasks;
+  int32_t pad;
+  const int2* waits;
+  int* counters;          // ntasks task counters, then group counters
+  int* ctl;               // [0] queue head, [1] error code, [2] info, [3] timeouts
+  double* bases[MAX_BASES];  // device base pointers, indexed by Base
+  const FrontDesc* fronts;
+  const int32_t* relidx;
+  const int32_t* chidx;
+  int64_t spin_limit;     // polls before a wait gives up
+};
+
+// Error codes written to ctl[1].
+enum DeviceError : int {
+  DE_NONE = 0,
+  DE_TIMEOUT = 1,
+  DE_BAD_TASK = 2
+};
+
+}  // namespace chb

@@ -1,0 +1,253 @@
+// Plan creation (symbolic upload), program cache and program launch.
+#include "plan.h"
+
+#include <algorithm>
+#include <cstring>
+
+#include "../../include/chompack_b200.h"
+#include "internal.h"
+
+namespace chb {
+
+Program::~Program() {
+  if (d_tasks) cudaFree(d_tasks);
+  if (d_waits) cudaFree(d_waits);
+}
+
+static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+WsLayout ws_layout(const Program& p) {
+  WsLayout L;
+  L.counters_off = 256;
+  L.dbl_off = round_up(L.counters_off + (size_t)p.ncounters * sizeof(int), 256);
+  L.total = L.dbl_off + (size_t)p.ws_doubles * sizeof(double);
+  return L;
+}
+
+#define CUDA_TRY(x)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (x);                                                                    \
+    if (e_ != cudaSuccess) return set_error(-100 - (int)e_, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+static int upload_program(Program& prog) {
+  if (!prog.tasks.empty()) {
+    CUDA_TRY(cudaMalloc(&prog.d_tasks, prog.tasks.size() * sizeof(Task)));
+    CUDA_TRY(cudaMemcpy(prog.d_tasks, prog.tasks.data(), prog.tasks.size() * sizeof(Task), cudaMemcpyHostToDevice));
+  }
+  if (!prog.waits.empty()) {
+    CUDA_TRY(cudaMalloc(&prog.d_waits, prog.waits.size() * sizeof(int2)));
+    CUDA_TRY(cudaMemcpy(prog.d_waits, prog.waits.data(), prog.waits.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+// Builds the host side of a program only (no device upload); used by the
+// introspection entry points, which must work without a GPU.
+static Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
+  ProgKey key{op, k, flags};
+  auto it = plan->progs.find(key);
+  if (it != plan->progs.end()) return it->second.get();
+  std::unique_ptr<Program> prog(new Program());
+  int rc;
+  switch (op) {
+    case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
+    default: rc = set_error(-2, "operation %d is not available", op); break;
+  }
+  if (rc != 0) return nullptr;
+  Program* p = prog.get();
+  plan->progs[key] = std::move(prog);
+  return p;
+}
+
+Program* get_program(chb_plan* plan, int op, int64_t k, int flags) {
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return nullptr;
+  if (!p->tasks.empty() && !p->d_tasks) {
+    if (cudaSetDevice(plan->device) != cudaSuccess) {
+      set_error(-3, "cudaSetDevice(%d) failed", plan->device);
+      return nullptr;
+    }
+    if (upload_program(*p) != 0) return nullptr;
+  }
+  return p;
+}
+
+int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
+                cudaStream_t stream) {
+  WsLayout L = ws_layout(*prog);
+  if (work_bytes < L.total || (L.total > 0 && !work))
+    return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, L.total);
+  if (((uintptr_t)work) % 256 != 0) return set_error(-5, "workspace must be 256-byte aligned");
+  char* w = (char*)work;
+  CUDA_TRY(cudaMemsetAsync(w, 0, L.dbl_off, stream));
+  if (prog->tasks.empty()) return 0;
+  RunArgs ra;
+  std::memset(&ra, 0, sizeof(ra));
+  ra.tasks = prog->d_tasks;
+  ra.ntasks = (int32_t)prog->tasks.size();
+  ra.waits = prog->d_waits;
+  ra.ctl = (int*)w;
+  ra.counters = (int*)(w + L.counters_off);
+  for (int i = 0; i < nbases && i < MAX_BASES; i++) ra.bases[i] = bases[i];
+  ra.bases[B_WS] = (double*)(w + L.dbl_off);
+  ra.fronts = plan->d_fronts;
+  ra.relidx = plan->d_relidx;
+  ra.chidx = plan->d_chidx;
+  ra.spin_limit = 40000000LL;  // about 10 s of polling at the longest back-off
+  int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
+  CUDA_TRY(engine_launch(ra, grid, stream));
+  return 0;
+}
+
+}  // namespace chb
+
+using namespace chb;
+
+extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, const int64_t* snpar,
+                               const int64_t* relptr, const int64_t* relidx, const int64_t* chptr,
+                               const int64_t* chidx, const int64_t* blkptr, const int64_t* snode, const int64_t* p,
+                               int device, chb_plan** out) {
+  clear_error();
+  if (!out) return set_error(-1, "null output pointer");
+  *out = nullptr;
+  if (n < 0 || nsn < 0) return set_error(-1, "negative size");
+  std::unique_ptr<chb_plan> P(new chb_plan());
+  P->device = device;
+  P->n = n;
+  P->nsn = nsn;
+  P->fronts.resize(nsn);
+  P->snpar.resize(nsn);
+  P->level.assign(nsn, 0);
+  P->snptr.assign(snptr, snptr + nsn + 1);
+  P->snode.assign(snode, snode + n);
+  P->perm.assign(p, p + n);
+  const int64_t nrel = relptr[nsn];
+  P->relidx.resize(nrel);
+  for (int64_t i = 0; i < nrel; i++) {
+    if (relidx[i] < 0 || relidx[i] > INT32_MAX) return set_error(-6, "relidx out of range");
+    P->relidx[i] = (int32_t)relidx[i];
+  }
+  P->chidx.resize(chptr[nsn]);
+  for (int64_t i = 0; i < chptr[nsn]; i++) P->chidx[i] = (int32_t)chidx[i];
+  int64_t upd = 0;
+  for (int64_t k = 0; k < nsn; k++) {
+    FrontDesc& f = P->fronts[k];
+    std::memset(&f, 0, sizeof(f));
+    int64_t nn = snptr[k + 1] - snptr[k];
+    int64_t na = relptr[k + 1] - relptr[k];
+    if (nn <= 0 || na < 0 || nn + na > INT32_MAX / 2) return set_error(-7, "invalid supernode %lld", (long long)k);
+    if (blkptr[k + 1] - blkptr[k] != nn * (nn + na)) return set_error(-8, "blkptr inconsistent at %lld", (long long)k);
+    f.nn = (int32_t)nn;
+    f.na = (int32_t)na;
+    f.nj = (int32_t)(nn + na);
+    f.relptr = (int32_t)relptr[k];
+    f.chbeg = (int32_t)chptr[k];
+    f.chend = (int32_t)chptr[k + 1];
+    f.parent = (int32_t)snpar[k];
+    f.blk = blkptr[k];
+    f.upd = upd;
+    upd += na * na;
+    P->snpar[k] = (int32_t)snpar[k];
+    if (snpar[k] < k || snpar[k] >= nsn) return set_error(-9, "snpar must point to a later supernode or itself");
+    if ((snpar[k] == k) != (na == 0)) return set_error(-10, "root / separator mismatch at %lld", (long long)k);
+    for (int64_t i = 0; i < na; i++) {
+      int64_t r = relidx[relptr[k] + i];
+      if (snpar[k] != k) {
+        int64_t njp = (snptr[snpar[k] + 1] - snptr[snpar[k]]) + (relptr[snpar[k] + 1] - relptr[snpar[k]]);
+        if (r >= njp || (i > 0 && r <= relidx[relptr[k] + i - 1]))
+          return set_error(-11, "relidx of supernode %lld not increasing / in range", (long long)k);
+      }
+    }
+  }
+  P->upd_total = upd;
+  P->blk_total = blkptr[nsn];
+  // heights (children precede parents)
+  int maxlv = 0;
+  for (int64_t k = 0; k < nsn; k++) {
+    if (snpar[k] != k) P->level[snpar[k]] = std::max(P->level[snpar[k]], P->level[k] + 1);
+  }
+  for (int64_t k = 0; k < nsn; k++) {
+    P->fronts[k].level = P->level[k];
+    maxlv = std::max(maxlv, P->level[k]);
+  }
+  P->nlevels = nsn ? maxlv + 1 : 0;
+
+  // device upload (skipped with device < 0: host-only plan for introspection)
+  if (device >= 0) {
+    CUDA_TRY(cudaSetDevice(device));
+    if (nsn > 0) {
+      CUDA_TRY(cudaMalloc(&P->d_fronts, nsn * sizeof(FrontDesc)));
+      CUDA_TRY(cudaMemcpy(P->d_fronts, P->fronts.data(), nsn * sizeof(FrontDesc), cudaMemcpyHostToDevice));
+    }
+    if (nrel > 0) {
+      CUDA_TRY(cudaMalloc(&P->d_relidx, nrel * sizeof(int32_t)));
+      CUDA_TRY(cudaMemcpy(P->d_relidx, P->relidx.data(), nrel * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+    if (!P->chidx.empty()) {
+      CUDA_TRY(cudaMalloc(&P->d_chidx, P->chidx.size() * sizeof(int32_t)));
+      CUDA_TRY(cudaMemcpy(P->d_chidx, P->chidx.data(), P->chidx.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    }
+    if (n > 0) {
+      CUDA_TRY(cudaMalloc(&P->d_perm, n * sizeof(int64_t)));
+      CUDA_TRY(cudaMemcpy(P->d_perm, p, n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    }
+    int per_sm = 0, nsm = 0;
+    if (engine_occupancy(&per_sm) != 0 || per_sm <= 0) return set_error(-12, "engine kernel cannot be resident");
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    P->grid = per_sm * nsm;
+  }
+  *out = P.release();
+  return 0;
+}
+
+extern "C" int chb_plan_destroy(chb_plan* plan) {
+  if (!plan) return 0;
+  if (plan->device >= 0) cudaSetDevice(plan->device);
+  plan->progs.clear();
+  if (plan->d_fronts) cudaFree(plan->d_fronts);
+  if (plan->d_relidx) cudaFree(plan->d_relidx);
+  if (plan->d_chidx) cudaFree(plan->d_chidx);
+  if (plan->d_perm) cudaFree(plan->d_perm);
+  delete plan;
+  return 0;
+}
+
+extern "C" int chb_workspace_size(const chb_plan* plan_c, int op, int64_t k, int flags, size_t* bytes) {
+  clear_error();
+  chb_plan* plan = const_cast<chb_plan*>(plan_c);
+  if (!plan || !bytes) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  *bytes = ws_layout(*p).total;
+  return 0;
+}
+
+extern "C" int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, int64_t* info) {
+  clear_error();
+  if (!plan || !info) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  WsLayout L = ws_layout(*p);
+  info[0] = (int64_t)p->tasks.size();
+  info[1] = (int64_t)p->waits.size();
+  info[2] = p->ncounters;
+  info[3] = p->ws_doubles;
+  info[4] = (int64_t)L.total;
+  info[5] = (int64_t)L.dbl_off;
+  info[6] = plan->upd_total;
+  info[7] = (int64_t)sizeof(Task);
+  return 0;
+}
+
+extern "C" int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits,
+                                  void* fronts) {
+  clear_error();
+  if (!plan) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  if (tasks) std::memcpy(tasks, p->tasks.data(), p->tasks.size() * sizeof(Task));
+  if (waits) std::memcpy(waits, p->waits.data(), p->waits.size() * sizeof(int2));
+  if (fronts) std::memcpy(fronts, plan->fronts.data(), plan->fronts.size() * sizeof(FrontDesc));
+  return 0;
+}

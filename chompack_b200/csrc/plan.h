@@ -1,0 +1,85 @@
+// Host-side plan: uploaded symbolic data, workspace layout and the compiled
+// task programs of each sweep.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "engine.h"
+
+struct chb_plan;
+
+namespace chb {
+
+struct Program {
+  std::vector<Task> tasks;
+  std::vector<int2> waits;
+  int64_t ncounters = 0;   // tasks + groups
+  int64_t ws_doubles = 0;  // doubles of workspace (update matrices + scratch)
+  Task* d_tasks = nullptr;
+  int2* d_waits = nullptr;
+  ~Program();
+};
+
+// Byte layout of a caller workspace for one program:
+//   [0, 256)                 control words (queue head, error, info, ...)
+//   [256, counters_end)      task / group counters (int32)
+//   [dbl_off, ...)           doubles: update matrices, then program scratch
+struct WsLayout {
+  size_t counters_off;
+  size_t dbl_off;
+  size_t total;
+};
+WsLayout ws_layout(const Program& p);
+
+// Key of a program in the plan's cache.
+struct ProgKey {
+  int op;
+  int64_t k;
+  int flags;
+  bool operator<(const ProgKey& o) const {
+    if (op != o.op) return op < o.op;
+    if (k != o.k) return k < o.k;
+    return flags < o.flags;
+  }
+};
+
+}  // namespace chb
+
+struct chb_plan {
+  int device = 0;
+  int64_t n = 0, nsn = 0;
+  std::vector<chb::FrontDesc> fronts;  // host copy (upd = offset of U_k)
+  std::vector<int32_t> relidx, chidx, snpar, level;
+  std::vector<int64_t> snptr, snode, perm;
+  int64_t blk_total = 0;
+  int64_t upd_total = 0;   // sum of na^2
+  int nlevels = 0;
+  chb::FrontDesc* d_fronts = nullptr;
+  int32_t* d_relidx = nullptr;
+  int32_t* d_chidx = nullptr;
+  int64_t* d_perm = nullptr;    // p (trsm row gather)
+  int grid = 0;                 // persistent grid size
+  std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;
+};
+
+namespace chb {
+// Build (or fetch) the program of an operation.  Returns nullptr and sets
+// the error text on failure.
+Program* get_program(chb_plan* plan, int op, int64_t k, int flags);
+
+// Launch a program.  bases: MAX_BASES device pointers (unused slots null).
+int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
+                cudaStream_t stream);
+
+// Device entry points implemented in engine.cu.
+size_t engine_smem_bytes();
+cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream);
+int engine_occupancy(int* blocks_per_sm);
+
+// Program builders (one per sweep), in build_*.cpp.
+int build_cholesky(const chb_plan& P, Program& prog);
+}  // namespace chb

@@ -1,0 +1,70 @@
+"""Device plan of a symbolic factorisation: the symbolic arrays uploaded once
+(chb_plan_create), the compiled task programs of each sweep, and the device
+workspaces they run in (allocated through torch's caching allocator and
+reused across calls)."""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+__all__ = ["Plan"]
+
+
+def _i64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+
+
+class Plan(object):
+    """Uploaded symbolic factorisation.  device=None picks the current CUDA
+    device; device=-1 builds a host-only plan (introspection only)."""
+
+    def __init__(self, symb, device=None):
+        if device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("chompack_b200 sweeps need a CUDA device (no CPU fallback)")
+            device = torch.cuda.current_device()
+        self.device = int(device)
+        self.symb = symb
+        arrs = [_i64(getattr(symb, a)) for a in ("snptr", "snpar", "relptr", "relidx", "chptr", "chidx",
+                                                 "blkptr", "snode", "p")]
+        self._keep = arrs
+        h = N.PPLAN()
+        if self.device >= 0:
+            with torch.cuda.device(self.device):
+                rc = N.plan_create(symb.n, symb.Nsn, *[N.ptr(a) for a in arrs], self.device, ctypes.byref(h))
+        else:
+            rc = N.plan_create(symb.n, symb.Nsn, *[N.ptr(a) for a in arrs], self.device, ctypes.byref(h))
+        N.check(rc, "plan_create")
+        self.handle = h
+        self._ws = {}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            N.plan_destroy(h)
+            self.handle = None
+
+    def workspace_bytes(self, op, k=0, flags=0):
+        sz = ctypes.c_size_t()
+        N.check(N.workspace_size(self.handle, op, int(k), int(flags), ctypes.byref(sz)), "workspace_size")
+        return int(sz.value)
+
+    def workspace(self, op, k=0, flags=0, slot=0):
+        """Device workspace for an operation (cached; 256-byte aligned)."""
+        nbytes = self.workspace_bytes(op, k, flags)
+        key = (slot,)
+        buf = self._ws.get(key)
+        if buf is None or buf.numel() < nbytes + 256:
+            buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=torch.device("cuda", self.device))
+            self._ws[key] = buf
+        base = buf.data_ptr()
+        aligned = (base + 255) // 256 * 256
+        return aligned, nbytes
+
+    def program_info(self, op, k=0, flags=0):
+        info = (ctypes.c_int64 * 8)()
+        N.check(N.program_info(self.handle, op, int(k), int(flags), info), "program_info")
+        keys = ("tasks", "waits", "counters", "ws_doubles", "ws_bytes", "dbl_off", "upd_doubles", "task_bytes")
+        return dict(zip(keys, list(info)))

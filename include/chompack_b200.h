@@ -1,0 +1,160 @@
+/*
+ * chompack_b200 — C ABI of the B200 (sm_100a) multifrontal sweeps over a
+ * supernodal clique tree.
+ *
+ * The boundary replaces the reference's CPython extension `chompack.cbase`
+ * (src/C/cbase.c) and the plain-C kernels it wraps (src/C/chompack.h:63-231).
+ * Every entry point takes plain pointers and sizes: int64 index arrays in the
+ * reference's `symbolic` layout on the host, float64 `blkval` buffers in the
+ * reference's block layout on the device, and a CUDA stream as `void*`.
+ *
+ * Return codes: 0 success; > 0 a LAPACK-style `info` from a device
+ * factorisation (the reference raises ArithmeticError on it, cbase.c:281);
+ * < 0 an argument, consistency or CUDA error (see chb_last_error()).
+ */
+#ifndef CHOMPACK_B200_H
+#define CHOMPACK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Host symbolic analysis (reference: src/python/symbolic.py).               */
+/* Each function restates the named reference function over int64 arrays.   */
+/* ------------------------------------------------------------------------ */
+
+/* Merge decision callback: merge_fn(|J_parent|, |J_k|, |N_parent|, |N_k|)
+ * returns non-zero to merge supernode k into its parent (symbolic.py:527). */
+typedef int (*chb_merge_fn)(int64_t cp, int64_t ck, int64_t np, int64_t nk);
+
+/* etree(A) — symbolic.py:49-72. cp/ri: CCS of the symmetric pattern. */
+int chb_sym_etree(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* parent);
+/* post_order(parent) — symbolic.py:26-47. */
+int chb_sym_post_order(int64_t n, const int64_t* parent, int64_t* post);
+/* counts(A, parent, post) — symbolic.py:95-131. */
+int chb_sym_counts(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* parent,
+                   const int64_t* post, int64_t* colcount);
+/* supernodes(par, post, colcount) incl. pothen_sun — symbolic.py:133-244. */
+int chb_sym_supernodes(int64_t n, const int64_t* par, const int64_t* post, const int64_t* colcount,
+                       int64_t* snode, int64_t* snptr, int64_t* snpar, int64_t* nsn);
+/* amalgamate(...) with merge_size_fill(tsize, tfill) or merge_fn —
+ * symbolic.py:246-326, :486-496. */
+int chb_sym_amalgamate(int64_t n, int64_t* colcount, int64_t* snode, int64_t* snptr, int64_t* snpar,
+                       const int64_t* snpost_in, int64_t* snpost_out, int64_t* nsn, int64_t tsize,
+                       int64_t tfill, chb_merge_fn merge_fn);
+/* embed(A, ...) — symbolic.py:328-384 (rowidx == NULL: only colptr). */
+int chb_sym_embed(int64_t n, const int64_t* cp, const int64_t* ri, const int64_t* colcount,
+                  const int64_t* snode, const int64_t* snptr, const int64_t* snpar, const int64_t* snpost,
+                  int64_t nsn, int64_t* colptr, int64_t* rowidx);
+/* relative_idx(colptr, rowidx, snptr, snpar) — symbolic.py:386-411. */
+int chb_sym_relative_idx(int64_t nsn, const int64_t* colptr, const int64_t* rowidx, const int64_t* snptr,
+                         const int64_t* snpar, int64_t* relptr, int64_t* relidx);
+/* Approximate minimum degree ordering (stands in for cvxopt.amd.order,
+ * called by symbolic.py:541-542). cp/ri: CCS of the symmetric pattern
+ * (diagonal entries allowed); perm[n] receives the elimination order. */
+int chb_amd_order(int64_t n, const int64_t* cp, const int64_t* ri, int64_t* perm);
+
+/* ------------------------------------------------------------------------ */
+/* Device plan: the symbolic arrays a sweep reads, uploaded once.            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct chb_plan chb_plan;
+
+/* Upload a symbolic factorisation (the attributes cbase.c:229-246 and
+ * :1021-1042 read from `symb`) and build the level schedules.  All arrays are
+ * host int64 in the reference's layout; snpost must be range(nsn) (the
+ * reference renumbers supernodes in postorder, symbolic.py:564-575).  The plan
+ * is bound to `device`; device < 0 gives a host-only plan that supports the
+ * introspection calls only. */
+int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, const int64_t* snpar,
+                    const int64_t* relptr, const int64_t* relidx, const int64_t* chptr,
+                    const int64_t* chidx, const int64_t* blkptr, const int64_t* snode, const int64_t* p,
+                    int device, chb_plan** plan);
+int chb_plan_destroy(chb_plan* plan);
+
+/* Operation codes for workspace queries. */
+enum chb_op {
+  CHB_OP_CHOLESKY = 0,
+  CHB_OP_LLT = 1,
+  CHB_OP_PROJECTED_INVERSE = 2,
+  CHB_OP_COMPLETION = 3,
+  CHB_OP_HESSIAN = 4,
+  CHB_OP_TRSM = 5,
+  CHB_OP_DOT = 6
+};
+
+/* Device workspace (bytes) an operation needs; `k` is nrhs for CHB_OP_TRSM,
+ * the number of U matrices for CHB_OP_HESSIAN and factored_updates for
+ * CHB_OP_COMPLETION (ignored otherwise); `flags` is the hessian adj/inv
+ * selector (adj | inv << 1 | factored_updates << 2), else 0.  This replaces
+ * the per-call malloc of fws/upd/upd_size sized from symb.memory
+ * (cbase.c:249-258, :1037-1039).  The caller owns the workspace, which must
+ * be 256-byte aligned. */
+int chb_workspace_size(const chb_plan* plan, int op, int64_t k, int flags, size_t* bytes);
+
+/* Introspection of a compiled sweep (works on a host-only plan, device < 0):
+ * info[0..7] = tasks, waits, counters, workspace doubles, workspace bytes,
+ * byte offset of the doubles, doubles of update matrices, sizeof(task).
+ * chb_program_export copies the task list, the (counter, target) waits and
+ * the per-supernode descriptors into caller buffers of those sizes. */
+int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
+int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits, void* fronts);
+
+/* ------------------------------------------------------------------------ */
+/* Numeric sweeps.  All pointers are device pointers; calls are asynchronous */
+/* on `stream` except that chb_info() synchronises to read the status.       */
+/* ------------------------------------------------------------------------ */
+
+/* cholesky — cholesky.c:3-84 (wrapper cbase.c:187-284).  In place on blkval. */
+int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream);
+
+/* llt — llt.c:3-60 (wrapper cbase.c:298-390).  In place on blkval. */
+int chb_llt(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream);
+
+/* projected_inverse — projected_inverse.c:3-75 (wrapper cbase.c:404-500). */
+int chb_projected_inverse(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream);
+
+/* completion — completion.c:3-120 + update_factor.c:3-108 (wrapper
+ * cbase.c:521-621).  factored_updates as in the reference (default 1). */
+int chb_completion(chb_plan* plan, double* blkval, int factored_updates, void* work, size_t work_bytes,
+                   void* stream);
+
+/* hessian — hessian.c:349-374 (_Y2K :3, _M2T :114, _scale :216; wrapper
+ * cbase.c:675-857).  ublkval: host array of nu device pointers, each a U
+ * blkval updated in place.  adj/inv as hessian.c; the reference's adj=None
+ * (full Hessian) is two calls with adj toggled (cbase.c:833-841). */
+int chb_hessian(chb_plan* plan, const double* lblkval, const double* yblkval, double* const* ublkval,
+                int64_t nu, int adj, int inv, int factored_updates, void* work, size_t work_bytes,
+                void* stream);
+
+/* trsm — trsm.c:3-139 (wrapper cbase.c:965-1077).  B := alpha*L^{-1}B
+ * (trans 'N') or alpha*L^{-T}B (trans 'T'); B is n x nrhs column-major with
+ * leading dimension ldB, rows in the original (unpermuted) order. */
+int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
+             int64_t ldB, void* work, size_t work_bytes, void* stream);
+
+/* dot — dot.c:3-23 (wrapper cbase.c:106-174).  Writes <X,Y> to result (one
+ * device double). */
+int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
+            size_t work_bytes, void* stream);
+
+/* Synchronise `stream` and return the status of the last sweep run with this
+ * workspace: 0, or the 1-based failing column of the first failing front
+ * (LAPACK info convention), or < 0 on a device-side consistency error. */
+int chb_info(chb_plan* plan, void* work, void* stream);
+
+/* Text of the last host-side error on this thread. */
+const char* chb_last_error(void);
+
+/* Build/version string (compute capability the kernels were built for). */
+const char* chb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHOMPACK_B200_H */

@@ -1,0 +1,56 @@
+"""Shared helpers for the parity tests: problem construction (the shared
+seeded value recipe of chompack_b200.grids, AMD ordering, merge rule) and
+block-wise comparison against the oracle.
+
+Tolerance of the FP64 parity checks (stated once, used everywhere):
+    |x - x_ref| <= RTOL * max(|x_ref|, FLOOR * max|block_ref|)
+with RTOL = 1e-12 and FLOOR = 1e-3, over the lower trapezoid of each
+supernode block (the only part the reference defines, symbolic.py:1087-1094);
+the floor covers entries that are the result of near cancellation.
+"""
+import numpy as np
+
+import chompack_b200 as cp
+from chompack_b200 import grids
+
+RTOL = 1e-12
+FLOOR = 1e-3
+
+
+def problem(kind, *args, merge=None, seed=0, order="amd"):
+    if kind == "grid2d":
+        A = grids.grid2d(*args, seed=seed)
+    elif kind == "grid3d":
+        A = grids.grid3d(*args, seed=seed)
+    elif kind == "grid2d_extra":
+        A = grids.grid2d_extra(*args, seed=seed)
+    elif kind == "random":
+        A = grids.random_lower(*args, seed=seed)
+    else:
+        raise ValueError(kind)
+    p = cp.amd.order(A) if order == "amd" else None
+    s = cp.symbolic(A, p=p, merge_function=cp.merge_size_fill(*merge) if merge else None)
+    return A, s
+
+
+def block_errors(symb, x, ref):
+    """Worst scaled error over all supernode blocks (lower trapezoid)."""
+    x = np.asarray(x)
+    ref = np.asarray(ref)
+    worst = 0.0
+    for k in range(symb.Nsn):
+        nn = int(symb.snptr[k + 1] - symb.snptr[k])
+        nj = int(symb.sncolptr[k + 1] - symb.sncolptr[k])
+        b = slice(int(symb.blkptr[k]), int(symb.blkptr[k + 1]))
+        xm = x[b].reshape((nj, nn), order="F")
+        rm = ref[b].reshape((nj, nn), order="F")
+        mask = np.tril(np.ones((nj, nn), dtype=bool))
+        rv = rm[mask]
+        scale = np.maximum(np.abs(rv), FLOOR * max(np.abs(rv).max(), 1e-300))
+        worst = max(worst, float((np.abs(xm[mask] - rv) / scale).max()))
+    return worst
+
+
+def assert_blocks_close(symb, x, ref, rtol=RTOL):
+    e = block_errors(symb, x, ref)
+    assert e <= rtol, "scaled block error %.3e exceeds %.1e" % (e, rtol)

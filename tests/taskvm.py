@@ -1,0 +1,210 @@
+"""CPU interpreter of the device task programs (test infrastructure).
+
+The native planner compiles every sweep into a task list (the same bytes the
+persistent GPU kernel executes).  This module decodes that list through the
+library's introspection API and executes it with numpy, either in list order
+or in a random order that only respects the recorded waits.  Running random
+topological orders against the reference results checks, without a GPU, that
+the planner's operands are right and that its dependency lists are complete.
+It is a checker of the planner, never a way to compute a result in the
+product.
+"""
+import ctypes
+
+import numpy as np
+
+from chompack_b200 import _native as N
+
+OPERAND = np.dtype([("off", "<i8"), ("ld", "<i4"), ("base", "u1"), ("mode", "u1"), ("pad", "<i2"),
+                    ("diag", "<i4"), ("pad2", "<i4")])
+TASK = np.dtype({
+    "names": ["op", "cmode", "nwait", "wait_off", "group", "m", "n", "k", "cdiag", "aux", "alpha", "beta",
+              "a", "b", "c"],
+    "formats": ["u1", "u1", "<u2", "<i4", "<i4", "<i4", "<i4", "<i4", "<i4", ("<i4", 4), "<f8", "<f8",
+                OPERAND, OPERAND, OPERAND],
+    "offsets": [0, 1, 2, 4, 8, 12, 16, 20, 24, 28, 48, 56, 64, 88, 112],
+    "itemsize": 136,
+})
+FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4"), ("chbeg", "<i4"),
+                  ("chend", "<i4"), ("parent", "<i4"), ("level", "<i4"), ("blk", "<i8"), ("upd", "<i8"),
+                  ("scr", "<i8"), ("scr2", "<i8")])
+
+OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
+T_GEMM, T_POTRF, T_ASM, T_MROW = 0, 1, 2, 3
+B_X, B_WS = 0, 1
+
+N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_int64)]
+N.lib.chb_program_export.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+
+
+class Program(object):
+    def __init__(self, plan_handle, op, k=0, flags=0, nsn=0):
+        info = (ctypes.c_int64 * 8)()
+        N.check(N.lib.chb_program_info(plan_handle, op, k, flags, info), "program_info")
+        self.ntasks, self.nwaits, self.ncounters, self.ws_doubles = info[0], info[1], info[2], info[3]
+        assert info[7] == TASK.itemsize, "Task layout mismatch (%d bytes)" % info[7]
+        self.upd_total = info[6]
+        self.tasks = np.zeros(self.ntasks, dtype=TASK)
+        self.waits = np.zeros((self.nwaits, 2), dtype=np.int32)
+        self.fronts = np.zeros(nsn, dtype=FRONT)
+        N.check(N.lib.chb_program_export(plan_handle, op, k, flags, self.tasks.ctypes.data,
+                                         self.waits.ctypes.data, self.fronts.ctypes.data), "program_export")
+
+
+def _operand(buf, o, rows, K):
+    r = np.arange(rows)[:, None]
+    k = np.arange(K)[None, :]
+    mode = int(o["mode"])
+    off, ld, d = int(o["off"]), int(o["ld"]), int(o["diag"])
+    if mode == OM_N:
+        return buf[off + k * ld + r]
+    if mode == OM_T:
+        return buf[off + r * ld + k]
+    if mode == OM_TRI_N:
+        v = buf[off + np.minimum(k * ld + r, buf.size - 1 - off)]
+        return np.where(r + d >= k, v, 0.0)
+    if mode == OM_TRI_T:
+        v = buf[off + np.minimum(r * ld + k, buf.size - 1 - off)]
+        return np.where(k + d >= r, v, 0.0)
+    gr, gc = r + d, k + int(o["pad2"])
+    idx = np.where(gr >= gc, gc * ld + gr, gr * ld + gc)
+    return buf[off + idx]
+
+
+def _store(buf, o, m, n, val, lower, cdiag, beta):
+    r = np.arange(m)[:, None]
+    c = np.arange(n)[None, :]
+    idx = int(o["off"]) + c * int(o["ld"]) + r
+    mask = np.ones((m, n), dtype=bool) if not lower else (r + cdiag >= c)
+    old = buf[idx]
+    new = val + (beta * old if beta != 0.0 else 0.0)
+    buf[idx[mask]] = new[mask]
+
+
+class VM(object):
+    """Executes a Program on numpy buffers.  bases: dict slot -> 1-D array."""
+
+    def __init__(self, prog, bases, relidx, chidx):
+        self.p = prog
+        self.bases = bases
+        self.relidx = np.asarray(relidx)
+        self.chidx = np.asarray(chidx)
+        self.info = 0
+
+    def run_task(self, t):
+        op = int(t["op"])
+        if op == T_GEMM:
+            m, n, K = int(t["m"]), int(t["n"]), int(t["k"])
+            A = _operand(self.bases[int(t["a"]["base"])], t["a"], m, K)
+            Bm = _operand(self.bases[int(t["b"]["base"])], t["b"], n, K)
+            _store(self.bases[int(t["c"]["base"])], t["c"], m, n, float(t["alpha"]) * (A @ Bm.T),
+                   int(t["cmode"]) == 1, int(t["cdiag"]), float(t["beta"]))
+        elif op == T_MROW:
+            m, n, K = int(t["m"]), int(t["n"]), int(t["k"])
+            A = _operand(self.bases[int(t["a"]["base"])], t["a"], m, K)
+            Bm = _operand(self.bases[int(t["b"]["base"])], t["b"], n, K)
+            aux = t["aux"]
+            moff = (int(aux[2]) & 0xffffffff) | (int(aux[3]) << 32)
+            buf = self.bases[int(aux[0])]
+            r = np.arange(m)[:, None]
+            k = np.arange(m)[None, :]
+            M2 = np.where(r >= k, buf[moff + k * int(aux[1]) + r], 0.0)
+            _store(self.bases[int(t["c"]["base"])], t["c"], m, n, float(t["alpha"]) * (M2 @ (A @ Bm.T)),
+                   False, 0, 0.0)
+        elif op == T_POTRF:
+            b = int(t["m"])
+            X = self.bases[int(t["a"]["base"])]
+            off, ld = int(t["a"]["off"]), int(t["a"]["ld"])
+            r = np.arange(b)[:, None]
+            c = np.arange(b)[None, :]
+            tile = X[off + c * ld + r]
+            S = np.tril(tile) + np.tril(tile, -1).T
+            try:
+                L = np.linalg.cholesky(S)
+            except np.linalg.LinAlgError:
+                if self.info == 0:
+                    self.info = int(t["aux"][0]) + 1
+                L = np.nan_to_num(np.tril(tile))
+            idx = off + c * ld + r
+            low = r >= c
+            X[idx[low]] = L[low]
+            if int(t["aux"][1]):
+                M = np.linalg.inv(L)
+                _store(self.bases[int(t["c"]["base"])], t["c"], b, b, np.tril(M), False, 0, 0.0)
+        elif op == T_ASM:
+            self._asm(t)
+        else:
+            raise NotImplementedError("task op %d" % op)
+
+    def _asm(self, t):
+        f = self.p.fronts[int(t["aux"][0])]
+        j0, j1 = int(t["aux"][1]), int(t["aux"][2])
+        nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
+        X, WS = self.bases[B_X], self.bases[B_WS]
+        blk, upd = int(f["blk"]), int(f["upd"])
+        if int(t["aux"][3]) & 1:
+            for j in range(max(j0, nn), j1):
+                jj = j - nn
+                WS[upd + jj * na + jj: upd + jj * na + na] = 0.0
+        for l in range(int(f["chend"]) - 1, int(f["chbeg"]) - 1, -1):
+            ch = self.p.fronts[self.chidx[l]]
+            Nc = int(ch["na"])
+            r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+            Uc = WS[int(ch["upd"]): int(ch["upd"]) + Nc * Nc].reshape((Nc, Nc), order="F")
+            for q in range(Nc):
+                col = int(r[q])
+                if not (j0 <= col < j1):
+                    continue
+                rows = r[q:]
+                v = Uc[q:, q]
+                if col < nn:
+                    X[blk + col * nj + rows] += v
+                else:
+                    WS[upd + (col - nn) * na + (rows - nn)] += v
+
+    def run(self, order="list", seed=0):
+        tasks = self.p.tasks
+        nt = len(tasks)
+        if order == "list":
+            seq = range(nt)
+        else:
+            seq = self._random_order(seed)
+        for i in seq:
+            self.run_task(tasks[i])
+        return self.info
+
+    def _random_order(self, seed):
+        """A random execution order allowed by the waits alone."""
+        rng = np.random.default_rng(seed)
+        tasks, waits = self.p.tasks, self.p.waits
+        nt = len(tasks)
+        counters = np.zeros(self.p.ncounters, dtype=np.int64)
+        # waiters per counter
+        need = np.zeros(nt, dtype=np.int64)
+        watchers = {}
+        for i in range(nt):
+            w0, nw = int(tasks[i]["wait_off"]), int(tasks[i]["nwait"])
+            need[i] = nw
+            for (cid, target) in waits[w0:w0 + nw]:
+                watchers.setdefault(int(cid), []).append((i, int(target)))
+        ready = [i for i in range(nt) if need[i] == 0]
+        order = []
+        while ready:
+            j = int(rng.integers(len(ready)))
+            i = ready[j]
+            ready[j] = ready[-1]
+            ready.pop()
+            order.append(i)
+            for cid in (i, int(tasks[i]["group"])):
+                if cid < 0:
+                    continue
+                counters[cid] += 1
+                for (w, target) in watchers.get(cid, ()):
+                    if counters[cid] == target:
+                        need[w] -= 1
+                        if need[w] == 0:
+                            ready.append(w)
+        assert len(order) == nt, "task graph has unsatisfiable waits"
+        return order
