@@ -69,5 +69,6 @@ workspace_size = _sig("chb_workspace_size", ctypes.c_int,
 program_info = _sig("chb_program_info", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64])
 cholesky = _sig("chb_cholesky", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
+set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 
 OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)

@@ -21,7 +21,7 @@ namespace chb {
 
 int build_cholesky(const chb_plan& P, Program& prog) {
   const int T = TILE;
-  const int CH = 32;  // front columns per extend-add task
+  const int CH = 64;  // at most this many front columns per extend-add task
   const int64_t N = P.nsn;
   DagBuilder B;
 
@@ -56,18 +56,33 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     auto bw = [&](int c) { return std::min(T, nn - c * T); };  // column block width
     auto bh = [&](int i) { return std::min(T, na - i * T); };  // bottom tile height
 
-    // --- extend-add (cholesky.c:33-52)
+    // --- extend-add (cholesky.c:33-52), split into column chunks of about
+    // equal work (children's update entries landing in the chunk)
     int asm_group = -1;
     if (f.chend > f.chbeg || na > 0) {
       asm_group = B.new_group();
-      for (int j0 = 0; j0 < nj; j0 += CH) {
+      std::vector<double> colwork(nj, 0.0);
+      for (int l = f.chbeg; l < f.chend; l++) {
+        const FrontDesc& ch = P.fronts[P.chidx[l]];
+        for (int q = 0; q < ch.na; q++) colwork[P.relidx[ch.relptr + q]] += ch.na - q;
+      }
+      for (int j = nn; j < nj; j++) colwork[j] += nj - j;  // zeroing of U_k
+      double total = 0.0;
+      for (double w : colwork) total += w;
+      const double target = std::max(8192.0, total / 64.0);
+      int j0 = 0;
+      while (j0 < nj) {
+        int j1 = j0;
+        double w = 0.0;
+        while (j1 < nj && (j1 - j0 < 8 || w < target) && j1 - j0 < CH) w += colwork[j1++];
         Task t = make_task(T_ASM);
         t.aux[0] = (int32_t)k;
         t.aux[1] = j0;
-        t.aux[2] = std::min(nj, j0 + CH);
+        t.aux[2] = j1;
         t.aux[3] = na > 0 ? 1 : 0;
-        int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group);
+        int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group, 3.0 + w / 2000.0);
         for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
+        j0 = j1;
       }
     }
 
@@ -197,7 +212,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       }
     }
   }
-  return B.finish(prog);
+  return B.finish(prog, P.grid > 0 ? P.grid : 296);
 }
 
 }  // namespace chb

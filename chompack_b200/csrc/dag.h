@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -45,15 +46,17 @@ struct DagBuilder {
   std::vector<std::vector<Wait>> waits;
   std::vector<int32_t> group_of;   // provisional group of each task (-1)
   std::vector<int32_t> group_size;
+  std::vector<double> cost;        // estimated duration (microseconds)
 
   int new_group() {
     group_size.push_back(0);
     return (int)group_size.size() - 1;
   }
 
-  int add(const Task& t, const SchedKey& key, int group = -1) {
+  int add(const Task& t, const SchedKey& key, int group = -1, double est_us = -1.0) {
     tasks.push_back(t);
     keys.push_back(key);
+    cost.push_back(est_us >= 0 ? est_us : estimate(t));
     waits.emplace_back();
     group_of.push_back(group);
     if (group >= 0) group_size[group]++;
@@ -69,12 +72,104 @@ struct DagBuilder {
     if (group >= 0) waits[task].push_back({group, -1, true});
   }
 
+  // Rough duration model of a task on one CTA (microseconds); only the
+  // relative sizes matter for the priority order.
+  static double estimate(const Task& t) {
+    switch (t.op) {
+      case T_GEMM:
+      case T_MROW:
+        return 3.0 + 4.5 * ((double)t.m * t.n * t.k) / (64.0 * 64.0 * 64.0) + (t.op == T_MROW ? 5.0 : 0.0);
+      case T_POTRF:
+        return 4.0 + 0.5 * t.m;
+      default:
+        return 4.0;
+    }
+  }
+
   // Sort into execution order and emit the device program.
-  int finish(Program& prog) {
+  //
+  // The order is the start order of a simulated list schedule on `slots`
+  // virtual CTAs: whenever a slot is free it starts the ready task with the
+  // largest upward rank (longest estimated path from the task to the end of
+  // the sweep).  A task starts only after everything it waits on has
+  // finished, so ordering by simulated start time is topological, and the
+  // device's CTAs, which claim tasks in list order, follow a schedule that
+  // keeps the critical path moving while ready work fills the machine.
+  int finish(Program& prog, int slots = 296) {
     const int nt = (int)tasks.size();
+    const int ng = (int)group_size.size();
+    std::vector<std::vector<int>> members(ng);
+    for (int t = 0; t < nt; t++)
+      if (group_of[t] >= 0) members[group_of[t]].push_back(t);
+    std::vector<double> rank(nt, 0.0);
+    // creation order is topological (every wait names an earlier task)
+    for (int t = nt - 1; t >= 0; t--) {
+      rank[t] += cost[t];
+      for (const Wait& wt : waits[t]) {
+        if (wt.is_group) {
+          for (int u : members[wt.id])
+            if (u < t) rank[u] = std::max(rank[u], rank[t]);
+        } else if (wt.id < t) {
+          rank[wt.id] = std::max(rank[wt.id], rank[t]);
+        }
+      }
+    }
+    // waiters of each task / group, and unmet wait counts
+    std::vector<std::vector<int>> task_waiters(nt), group_waiters(ng);
+    std::vector<int> unmet(nt, 0);
+    for (int t = 0; t < nt; t++) {
+      for (const Wait& wt : waits[t]) {
+        if (wt.is_group) {
+          if (group_size[wt.id] == 0) continue;
+          group_waiters[wt.id].push_back(t);
+        } else {
+          task_waiters[wt.id].push_back(t);
+        }
+        unmet[t]++;
+      }
+    }
+    std::vector<int> group_left(group_size.begin(), group_size.end());
+    std::vector<double> start(nt, 0.0);
+    {
+      auto by_rank = [&](int a, int b) { return rank[a] < rank[b] || (rank[a] == rank[b] && b < a); };
+      std::priority_queue<int, std::vector<int>, decltype(by_rank)> ready(by_rank);
+      typedef std::pair<double, int> Ev;
+      std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
+      for (int t = 0; t < nt; t++)
+        if (unmet[t] == 0) ready.push(t);
+      int free_slots = std::max(slots, 1);
+      double now = 0.0;
+      int done = 0;
+      auto release = [&](int w) {
+        if (--unmet[w] == 0) ready.push(w);
+      };
+      while (done < nt) {
+        while (free_slots > 0 && !ready.empty()) {
+          int t = ready.top();
+          ready.pop();
+          start[t] = now;
+          running.push({now + std::max(cost[t], 1e-3), t});
+          free_slots--;
+        }
+        if (running.empty()) return set_error(-23, "task graph: unsatisfiable waits");
+        Ev e = running.top();
+        running.pop();
+        now = e.first;
+        free_slots++;
+        done++;
+        const int t = e.second;
+        for (int w : task_waiters[t]) release(w);
+        if (group_of[t] >= 0 && --group_left[group_of[t]] == 0)
+          for (int w : group_waiters[group_of[t]]) release(w);
+      }
+    }
     std::vector<int> order(nt);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      if (start[a] != start[b]) return start[a] < start[b];
+      if (rank[a] != rank[b]) return rank[a] > rank[b];
+      return keys[a] < keys[b];
+    });
     std::vector<int> pos(nt);
     for (int i = 0; i < nt; i++) pos[order[i]] = i;
     // latest member position of each group

@@ -31,170 +31,280 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
 
 __device__ __forceinline__ int ld_volatile(const int* p) { return *((const volatile int*)p); }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned sm_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
+
 // ------------------------------------------------------------- operands
 struct SmemLayout {
   double* A;   // [TILE][LDS]: A(r, k) stored at A[k*LDS + r]
   double* B;   // [TILE][LDS]
 };
 
-__device__ __forceinline__ const double* base_ptr(const RunArgs& ra, uint8_t b) { return ra.bases[b]; }
+constexpr int PER_THREAD = (TILE * KC) / NTHREADS;  // staged elements per thread
 
 // Element (r, k) of an operand, already known to be inside [0,rows) x [0,K).
-__device__ __forceinline__ double op_elem(const double* X, const Operand& o, int r, int k) {
-  switch (o.mode) {
-    case OM_N:
-      return __ldcg(X + (int64_t)k * o.ld + r);
-    case OM_T:
-      return __ldcg(X + (int64_t)r * o.ld + k);
-    case OM_TRI_N:
-      return (r + o.diag >= k) ? __ldcg(X + (int64_t)k * o.ld + r) : 0.0;
-    case OM_TRI_T:
-      return (k + o.diag >= r) ? __ldcg(X + (int64_t)r * o.ld + k) : 0.0;
-    default: {  // OM_SYM: element (r + diag, k + pad2) of a symmetric matrix
-      int gr = r + o.diag, gc = k + o.pad2;
-      return (gr >= gc) ? __ldcg(X + (int64_t)gc * o.ld + gr) : __ldcg(X + (int64_t)gr * o.ld + gc);
-    }
+template <int MODE>
+__device__ __forceinline__ double op_elem(const double* __restrict__ X, int ld, int diag, int koff, int r, int k) {
+  if (MODE == OM_N) return __ldcg(X + (int64_t)k * ld + r);
+  if (MODE == OM_T) return __ldcg(X + (int64_t)r * ld + k);
+  if (MODE == OM_TRI_N) return (r + diag >= k) ? __ldcg(X + (int64_t)k * ld + r) : 0.0;
+  if (MODE == OM_TRI_T) return (k + diag >= r) ? __ldcg(X + (int64_t)r * ld + k) : 0.0;
+  // OM_SYM: element (r + diag, k + koff) of a symmetric matrix stored lower
+  int gr = r + diag, gc = k + koff;
+  return (gr >= gc) ? __ldcg(X + (int64_t)gc * ld + gr) : __ldcg(X + (int64_t)gr * ld + gc);
+}
+
+// Coordinates of the s-th staged element of this thread.  Operands read
+// along k (OM_T, OM_TRI_T) give consecutive threads consecutive k so that
+// global reads stay coalesced; the others give consecutive threads
+// consecutive rows.
+template <int MODE>
+__device__ __forceinline__ void stage_coord(int s, int& r, int& kk) {
+  const int idx = threadIdx.x + s * NTHREADS;
+  if (MODE == OM_T || MODE == OM_TRI_T) {
+    kk = idx % KC;
+    r = idx / KC;
+  } else {
+    r = idx % TILE;
+    kk = idx / TILE;
   }
 }
 
-// Stage opX(r, k0 + kk) for r < 64, kk < KC into S[kk*LDS + r] (zero padded).
-__device__ __forceinline__ void stage(const RunArgs& ra, const Operand& o, int rows, int k0, int K, double* S) {
-  const double* X = base_ptr(ra, o.base) + o.off;
-  const bool kfast = (o.mode == OM_T || o.mode == OM_TRI_T);
-#pragma unroll 4
-  for (int s = 0; s < (TILE * KC) / NTHREADS; s++) {
-    int idx = threadIdx.x + s * NTHREADS;
+template <int MODE>
+__device__ __forceinline__ void load_chunk_t(const double* __restrict__ X, int ld, int diag, int koff, int rows,
+                                             int k0, int K, double (&v)[PER_THREAD]) {
+#pragma unroll
+  for (int s = 0; s < PER_THREAD; s++) {
     int r, kk;
-    if (kfast) {
-      kk = idx % KC;
-      r = idx / KC;
-    } else {
-      r = idx % TILE;
-      kk = idx / TILE;
-    }
-    int k = k0 + kk;
-    double v = 0.0;
-    if (r < rows && k < K) v = op_elem(X, o, r, k);
-    S[kk * LDS + r] = v;
+    stage_coord<MODE>(s, r, kk);
+    const int k = k0 + kk;
+    v[s] = (r < rows && k < K) ? op_elem<MODE>(X, ld, diag, koff, r, k) : 0.0;
   }
 }
 
-__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(c[0]), "+d"(c[1])
-               : "d"(a), "d"(b));
+template <int MODE>
+__device__ __forceinline__ void store_chunk_t(double* S, const double (&v)[PER_THREAD]) {
+#pragma unroll
+  for (int s = 0; s < PER_THREAD; s++) {
+    int r, kk;
+    stage_coord<MODE>(s, r, kk);
+    S[kk * LDS + r] = v[s];
+  }
+}
+
+// Operand held in registers for the duration of a task.
+struct Opnd {
+  const double* X;
+  int ld, diag, koff, mode;
+};
+
+__device__ __forceinline__ Opnd make_opnd(const RunArgs& ra, const Operand& o) {
+  Opnd p;
+  p.X = ra.bases[o.base] + o.off;
+  p.ld = o.ld;
+  p.diag = o.diag;
+  p.koff = o.pad2;
+  p.mode = o.mode;
+  return p;
+}
+
+__device__ __forceinline__ void load_chunk(const Opnd& o, int rows, int k0, int K, double (&v)[PER_THREAD]) {
+  switch (o.mode) {
+    case OM_N: load_chunk_t<OM_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+    case OM_T: load_chunk_t<OM_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+    case OM_TRI_N: load_chunk_t<OM_TRI_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+    case OM_TRI_T: load_chunk_t<OM_TRI_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+    default: load_chunk_t<OM_SYM>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+  }
+}
+
+__device__ __forceinline__ void store_chunk(int mode, double* S, const double (&v)[PER_THREAD]) {
+  if (mode == OM_T || mode == OM_TRI_T) store_chunk_t<OM_T>(S, v);
+  else store_chunk_t<OM_N>(S, v);
+}
+
+// Double-precision tensor-core MMA, m16n8k4 (sm_90+):
+//   A 16x4 row-major: a0 = A(g, q), a1 = A(g + 8, q)
+//   B 4x8 col-major:  b0 = B(q, g)
+//   C 16x8:           c0,c1 = C(g, 2q + {0,1}), c2,c3 = C(g + 8, 2q + {0,1})
+// with g = lane / 4, q = lane % 4.  A warp owns a 32x32 C sub-tile: two m16
+// rows x four n8 columns.
+__device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, double b) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a0), "d"(a1), "d"(b));
+}
+
+// Accumulator layout: acc[i][j][h] with i in 0..1 (m16 tile), j in 0..3 (n8
+// tile), h in 0..3 (c0..c3).
+typedef double Acc[2][4][4];
+
+// Tile coordinates of acc[i][j][h] inside the 64x64 C tile.
+__device__ __forceinline__ void acc_coord(int i, int j, int h, int& r, int& c) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  r = (warp >> 1) * 32 + 16 * i + g + ((h & 2) ? 8 : 0);
+  c = (warp & 1) * 32 + 8 * j + 2 * q + (h & 1);
 }
 
 // acc += A(:, 0:kn) * B(:, 0:kn)^T from staged tiles (kn multiple of 4).
-__device__ __forceinline__ void mma_block(const double* sA, const double* sB, int kn, double (&acc)[4][4][2]) {
+__device__ __forceinline__ void mma_block(const double* sA, const double* sB, int kn, Acc& acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int r0 = (warp >> 1) * 32 + g, c0 = (warp & 1) * 32 + g;
+#pragma unroll 4
   for (int kk = 0; kk < kn; kk += 4) {
-    double a[4], b[4];
+    double a[2][2], b[4];
+    const double* ak = sA + (kk + q) * LDS + r0;
+    const double* bk = sB + (kk + q) * LDS + c0;
 #pragma unroll
-    for (int i = 0; i < 4; i++) a[i] = sA[(kk + q) * LDS + r0 + 8 * i];
+    for (int i = 0; i < 2; i++) {
+      a[i][0] = ak[16 * i];
+      a[i][1] = ak[16 * i + 8];
+    }
 #pragma unroll
-    for (int j = 0; j < 4; j++) b[j] = sB[(kk + q) * LDS + c0 + 8 * j];
+    for (int j = 0; j < 4; j++) b[j] = bk[8 * j];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 2; i++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) dmma(acc[i][j], a[i], b[j]);
+      for (int j = 0; j < 4; j++) dmma16(acc[i][j], a[i][0], a[i][1], b[j]);
   }
 }
 
-__device__ __forceinline__ void zero_acc(double (&acc)[4][4][2]) {
+__device__ __forceinline__ void zero_acc(Acc& acc) {
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 4; h++) acc[i][j][h] = 0.0;
 }
 
-// acc = opA * opB^T over the full K range.
-__device__ void gemm_acc(const RunArgs& ra, const Task& t, const SmemLayout& sm, double (&acc)[4][4][2]) {
+// acc = opA * opB^T over K, with the next K chunk's global loads in flight
+// while the current chunk is multiplied.
+__device__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm, Acc& acc) {
   zero_acc(acc);
-  for (int k0 = 0; k0 < t.k; k0 += KC) {
-    stage(ra, t.a, t.m, k0, t.k, sm.A);
-    stage(ra, t.b, t.n, k0, t.k, sm.B);
+  double va[PER_THREAD], vb[PER_THREAD];
+  if (K > 0) {
+    load_chunk(A, m, 0, K, va);
+    load_chunk(B, n, 0, K, vb);
+  }
+  for (int k0 = 0; k0 < K; k0 += KC) {
+    store_chunk(A.mode, sm.A, va);
+    store_chunk(B.mode, sm.B, vb);
     __syncthreads();
-    int kn = min(KC, t.k - k0);
+    if (k0 + KC < K) {
+      load_chunk(A, m, k0 + KC, K, va);
+      load_chunk(B, n, k0 + KC, K, vb);
+    }
+    int kn = min(KC, K - k0);
     kn = (kn + 3) & ~3;
     mma_block(sm.A, sm.B, kn, acc);
     __syncthreads();
   }
 }
 
-// C = alpha*acc + beta*C (masked to m x n and, for CM_LOWER, to the lower
-// triangle).
-__device__ void store_acc(const RunArgs& ra, const Task& t, const Operand& co, double alpha, double beta,
-                          const double (&acc)[4][4][2]) {
-  double* C = ra.bases[co.base] + co.off;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, q = lane & 3;
-  const int r0 = (warp >> 1) * 32 + g;
+// C = alpha*acc + beta*C (masked to m x n and, for lower, to r + cdiag >= c).
+// All old values are fetched before the first store so that the loads are
+// in flight together (the compiler cannot reorder them across stores to C).
+__device__ void store_acc(double* __restrict__ C, int ldc, int m, int n, bool lower, int cdiag, double alpha,
+                          double beta, const Acc& acc) {
+  double old[2][4][4];
+  if (beta != 0.0) {
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    int r = r0 + 8 * i;
-    if (r >= t.m) continue;
+    for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+      for (int j = 0; j < 4; j++)
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        int c = (warp & 1) * 32 + 8 * j + 2 * q + h;
-        if (c >= t.n) continue;
-        if (t.cmode == CM_LOWER && r + t.cdiag < c) continue;
-        double* p = C + (int64_t)c * co.ld + r;
-        double v = alpha * acc[i][j][h];
-        if (beta != 0.0) v += beta * __ldcg(p);
-        *p = v;
-      }
-    }
+        for (int h = 0; h < 4; h++) {
+          int r, c;
+          acc_coord(i, j, h, r, c);
+          const bool ok = r < m && c < n && !(lower && r + cdiag < c);
+          old[i][j][h] = ok ? __ldcg(C + (int64_t)c * ldc + r) : 0.0;
+        }
   }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        int r, c;
+        acc_coord(i, j, h, r, c);
+        if (r >= m || c >= n) continue;
+        if (lower && r + cdiag < c) continue;
+        double v = alpha * acc[i][j][h];
+        if (beta != 0.0) v += beta * old[i][j][h];
+        C[(int64_t)c * ldc + r] = v;
+      }
 }
 
 // ------------------------------------------------------------------ GEMM
 __device__ void run_gemm(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
-  double acc[4][4][2];
-  gemm_acc(ra, t, sm, acc);
-  store_acc(ra, t, t.c, t.alpha, t.beta, acc);
+  const Opnd A = make_opnd(ra, t.a), B = make_opnd(ra, t.b);
+  double* C = ra.bases[t.c.base] + t.c.off;
+  const int ldc = t.c.ld, m = t.m, n = t.n, K = t.k, cdiag = t.cdiag;
+  const bool lower = t.cmode == CM_LOWER;
+  const double alpha = t.alpha, beta = t.beta;
+  Acc acc;
+  gemm_acc(A, B, m, n, K, sm, acc);
+  store_acc(C, ldc, m, n, lower, cdiag, alpha, beta, acc);
 }
 
 // C = alpha * M2 * (opA * opB^T), M2 = lower-triangular m x m tile (operand
 // `c` of the task holds C; M2 is described by aux: base aux[0], ld aux[1],
 // offset (aux[2] | aux[3] << 32)).
 __device__ void run_mrow(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
-  double acc[4][4][2];
-  gemm_acc(ra, t, sm, acc);
-  // T = acc (m x n) into sm.B as B-stage layout: sB[k*LDS + n] = T(k, n)
-  {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane >> 2, q = lane & 3;
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          int r = (warp >> 1) * 32 + 8 * i + g;
-          int c = (warp & 1) * 32 + 8 * j + 2 * q + h;
-          sm.B[r * LDS + c] = acc[i][j][h];
-        }
-  }
-  // sA[k*LDS + r] = M2(r, k) (lower triangle, zero padded)
+  const Opnd A = make_opnd(ra, t.a), B = make_opnd(ra, t.b);
+  double* C = ra.bases[t.c.base] + t.c.off;
+  const int ldc = t.c.ld, m = t.m, n = t.n, K = t.k;
+  const double alpha = t.alpha;
   const int64_t moff = (int64_t)(uint32_t)t.aux[2] | ((int64_t)t.aux[3] << 32);
-  const double* M2 = ra.bases[t.aux[0]] + moff;
+  const double* __restrict__ M2 = ra.bases[t.aux[0]] + moff;
   const int ldm = t.aux[1];
-  for (int idx = threadIdx.x; idx < TILE * TILE; idx += NTHREADS) {
-    int r = idx % TILE, k = idx / TILE;
-    double v = 0.0;
-    if (r < t.m && k < t.m && r >= k) v = __ldcg(M2 + (int64_t)k * ldm + r);
-    sm.A[k * LDS + r] = v;
+  Acc acc;
+  gemm_acc(A, B, m, n, K, sm, acc);
+  // T = acc (m x n) into sm.B in B-stage layout: sB[k*LDS + n] = T(k, n)
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        int r, c;
+        acc_coord(i, j, h, r, c);
+        sm.B[r * LDS + c] = acc[i][j][h];
+      }
+  // sA[k*LDS + r] = M2(r, k) (lower triangle, zero padded), 32 loads in
+  // flight per thread
+  {
+    double v[TILE * TILE / NTHREADS];
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = threadIdx.x + s2 * NTHREADS;
+      const int r = idx % TILE, k = idx / TILE;
+      v[s2] = (r < m && k < m && r >= k) ? __ldcg(M2 + (int64_t)k * ldm + r) : 0.0;
+    }
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = threadIdx.x + s2 * NTHREADS;
+      sm.A[(idx / TILE) * LDS + idx % TILE] = v[s2];
+    }
   }
   __syncthreads();
   zero_acc(acc);
-  mma_block(sm.A, sm.B, (t.m + 3) & ~3, acc);
+  mma_block(sm.A, sm.B, (m + 3) & ~3, acc);
   __syncthreads();
-  store_acc(ra, t, t.c, t.alpha, 0.0, acc);
+  store_acc(C, ldc, m, n, false, 0, alpha, 0.0, acc);
 }
 
 // ----------------------------------------------------------------- POTRF
@@ -202,65 +312,227 @@ __device__ void run_mrow(const RunArgs& ra, const Task& t, const SmemLayout& sm)
 // written back); if aux[1] != 0 also writes M = L^{-1} (full b x b with
 // zeros above the diagonal) to operand c.  A non-positive pivot records the
 // LAPACK-style info aux[0] + j + 1 in ctl[2] (first writer wins).
+//
+// The tile is padded to 64 x 64 with an identity block (which factors and
+// inverts to itself and does not couple to the leading b x b part), then
+// processed in four 16-column blocks J:
+//   (a) warp 0 factors the 16x16 diagonal block in registers (lane i holds
+//       row i, right-looking, pivots and multipliers broadcast by shuffles)
+//       and inverts it (lane c holds column c of Minv_JJ);
+//   (b) panel below: L(r, J) = A(r, J) Minv_JJ^T            (DMMA)
+//   (c) trailing lower triangle: A(r, c) -= L(r, J) L(c, J)^T (DMMA)
+// then the inverse of the whole tile block row by block row:
+//   M(I, :I) = -Minv_II (L(I, :I) M(:I, :I))                (DMMA)
+constexpr int POTRF_LD = TILE + 1;
+constexpr int POTRF_SMEM_DOUBLES = 2 * TILE * POTRF_LD + TILE + 16 * TILE;
+
+// Phase timing for development builds (-DCHB_PROFILE_POTRF); compiled out
+// otherwise.
+#ifdef CHB_PROFILE_POTRF
+__device__ unsigned long long g_potrf_phase[8];
+#define POTRF_STAMP(i)                                                    \
+  do {                                                                    \
+    long long now_ = clock64();                                           \
+    if (threadIdx.x == 0) atomicAdd(&g_potrf_phase[i], now_ - stamp_);    \
+    stamp_ = now_;                                                        \
+  } while (0)
+#else
+#define POTRF_STAMP(i) \
+  do {                 \
+  } while (0)
+#endif
+
+// acc += A(16 x K) B(K x 8) with A(r, k) = pa[r + k*lda] and
+// B(k, n) = pb[k*ksb + n*nsb] in shared memory (K a multiple of 4).
+__device__ __forceinline__ void warp_mma_16x8(double (&acc)[4], const double* pa, int lda, const double* pb,
+                                              int ksb, int nsb, int K, bool negate) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const double sgn = negate ? -1.0 : 1.0;
+#pragma unroll 4
+  for (int k = 0; k < K; k += 4) {
+    const double a0 = sgn * pa[g + (k + q) * lda];
+    const double a1 = sgn * pa[g + 8 + (k + q) * lda];
+    const double b0 = pb[(k + q) * ksb + g * nsb];
+    dmma16(acc, a0, a1, b0);
+  }
+}
+
 __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
   const int b = t.m;
-  const int LD = TILE + 1;
-  double* sL = smem;            // [col][row], ld 65
-  double* sM = smem + TILE * LD;
-  double* X = ra.bases[t.a.base] + t.a.off;
+  const int LD = POTRF_LD;
+  double* sL = smem;               // [col][row], lower; upper part zero
+  double* sM = sL + TILE * LD;     // inverse, upper part zero
+  double* rdiag = sM + TILE * LD;  // 1 / L(j,j)
+  double* sT = rdiag + TILE;       // [16 x 64] scratch, T(r, c) at sT[r + 16 c]
+  double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
   const int lda = t.a.ld;
-  for (int idx = threadIdx.x; idx < b * b; idx += NTHREADS) {
-    int r = idx % b, c = idx / b;
-    sL[c * LD + r] = (r >= c) ? __ldcg(X + (int64_t)c * lda + r) : 0.0;
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j = 0; j < b; j++) {
-    __syncthreads();  // trailing update of column j-1 complete
-    double d = sL[j * LD + j];
-    bool bad = !(d > 0.0);
-    double piv = sqrt(bad ? 1.0 : d);
-    double inv = 1.0 / piv;
-    if (bad && threadIdx.x == 0) atomicCAS(&ra.ctl[2], 0, t.aux[0] + j + 1);
-    for (int i = j + 1 + threadIdx.x; i < b; i += NTHREADS) sL[j * LD + i] *= inv;
-    __syncthreads();  // column j scaled; nobody reads sL(j,j) below
-    if (threadIdx.x == 0) sL[j * LD + j] = piv;
-    for (int l = j + 1 + warp; l < b; l += NTHREADS / 32) {
-      double ljl = sL[j * LD + l];
-      for (int i = l + lane; i < b; i += 32) sL[l * LD + i] -= sL[j * LD + i] * ljl;
+  const int info_base = t.aux[0];
+  const bool want_inv = t.aux[1] != 0;
+  double* __restrict__ Mout = want_inv ? ra.bases[t.c.base] + t.c.off : nullptr;
+  const int ldm = t.c.ld;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, q = lane & 3;
+#ifdef CHB_PROFILE_POTRF
+  long long stamp_ = clock64();
+#endif
+  {
+    double v[TILE * TILE / NTHREADS];
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = tid + s2 * NTHREADS;
+      const int r = idx % TILE, c = idx / TILE;
+      v[s2] = (r < b && c < b && r >= c) ? __ldcg(X + (int64_t)c * lda + r) : (r == c ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = tid + s2 * NTHREADS;
+      sL[(idx / TILE) * LD + idx % TILE] = (idx % TILE >= idx / TILE) ? v[s2] : 0.0;
+      sM[(idx / TILE) * LD + idx % TILE] = 0.0;
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < b * b; idx += NTHREADS) {
-    int r = idx % b, c = idx / b;
-    if (r >= c) X[(int64_t)c * lda + r] = sL[c * LD + r];
-  }
-  if (t.aux[1]) {
-    // column c of M = L^{-1}:  M(c,c) = 1/L(c,c);
-    // M(i,c) = -(sum_{l=c}^{i-1} L(i,l) M(l,c)) / L(i,i)
-    for (int c = threadIdx.x; c < b; c += NTHREADS) {
-      sM[c * LD + c] = 1.0 / sL[c * LD + c];
-      for (int i = c + 1; i < b; i++) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int l = c;
-        for (; l + 3 < i; l += 4) {
-          s0 += sL[l * LD + i] * sM[c * LD + l];
-          s1 += sL[(l + 1) * LD + i] * sM[c * LD + l + 1];
-          s2 += sL[(l + 2) * LD + i] * sM[c * LD + l + 2];
-          s3 += sL[(l + 3) * LD + i] * sM[c * LD + l + 3];
+  POTRF_STAMP(0);
+#pragma unroll 1
+  for (int J = 0; J < 4; J++) {
+    const int j0 = 16 * J, j1 = j0 + 16;
+    if (warp == 0) {
+      // (a) factor the 16x16 diagonal block in registers: lane i < 16 row i
+      const int il = lane & 15;
+      double a[16];
+#pragma unroll
+      for (int c = 0; c < 16; c++) a[c] = sL[(j0 + c) * LD + j0 + il];
+#pragma unroll
+      for (int jj = 0; jj < 16; jj++) {
+        const double d = __shfl_sync(0xffffffffu, a[jj], jj);
+        const bool bad = !(d > 0.0);
+        if (bad && lane == 0 && j0 + jj < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + jj + 1);
+        const double x = bad ? 1.0 : d;
+        const double rs = rsqrt(x);
+        a[jj] = (il == jj) ? x * rs : ((il > jj) ? a[jj] * rs : a[jj]);
+        if (lane == jj) rdiag[j0 + jj] = rs;
+#pragma unroll
+        for (int kk = jj + 1; kk < 16; kk++) {
+          const double lkj = __shfl_sync(0xffffffffu, a[jj], kk);
+          if (il >= kk) a[kk] -= a[jj] * lkj;
         }
-        for (; l < i; l++) s0 += sL[l * LD + i] * sM[c * LD + l];
-        sM[c * LD + i] = -((s0 + s1) + (s2 + s3)) / sL[i * LD + i];
       }
+      if (lane < 16) {
+#pragma unroll
+        for (int c = 0; c < 16; c++)
+          if (c <= il) sL[(j0 + c) * LD + j0 + il] = a[c];
+      }
+      __syncwarp();
+      POTRF_STAMP(1);
+      // inverse of the block: lane c < 16 holds column c,
+      // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c)
+      double m[16];
+#pragma unroll
+      for (int r = 0; r < 16; r++) {
+        double sacc = 0.0;
+#pragma unroll
+        for (int l = 0; l < r; l++) sacc += sL[(j0 + l) * LD + j0 + r] * m[l];
+        const double rd = rdiag[j0 + r];
+        m[r] = (r == il) ? rd : ((r > il) ? -rd * sacc : 0.0);
+      }
+      if (lane < 16) {
+#pragma unroll
+        for (int r = 0; r < 16; r++)
+          if (r >= il) sM[(j0 + il) * LD + j0 + r] = m[r];
+      }
+      POTRF_STAMP(2);
     }
     __syncthreads();
-    double* M = ra.bases[t.c.base] + t.c.off;
-    const int ldm = t.c.ld;
-    for (int idx = threadIdx.x; idx < b * b; idx += NTHREADS) {
-      int r = idx % b, c = idx / b;
-      M[(int64_t)c * ldm + r] = (r >= c) ? sM[c * LD + r] : 0.0;
+    POTRF_STAMP(3);
+    const int prow = TILE - j1;  // rows below the block: 48, 32, 16, 0
+    if (prow > 0) {
+      // (b) panel: X(r, n) = sum_k A(r, k) Minv(n, k), 16x8 tiles; at most
+      // six tiles, so warp w owns tiles w and w + 4
+      const int ntiles = (prow / 16) * 2;
+      double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
+      const int t0 = warp, t1 = warp + NTHREADS / 32;
+      if (t0 < ntiles)
+        warp_mma_16x8(acc0, sL + j0 * LD + j1 + 16 * (t0 >> 1), LD, sM + j0 * LD + j0 + 8 * (t0 & 1), LD, 1, 16,
+                      false);
+      if (t1 < ntiles)
+        warp_mma_16x8(acc1, sL + j0 * LD + j1 + 16 * (t1 >> 1), LD, sM + j0 * LD + j0 + 8 * (t1 & 1), LD, 1, 16,
+                      false);
+      __syncthreads();
+      if (t0 < ntiles) {
+        const int r0 = j1 + 16 * (t0 >> 1) + g, c0 = j0 + 8 * (t0 & 1) + 2 * q;
+        sL[c0 * LD + r0] = acc0[0];
+        sL[(c0 + 1) * LD + r0] = acc0[1];
+        sL[c0 * LD + r0 + 8] = acc0[2];
+        sL[(c0 + 1) * LD + r0 + 8] = acc0[3];
+      }
+      if (t1 < ntiles) {
+        const int r0 = j1 + 16 * (t1 >> 1) + g, c0 = j0 + 8 * (t1 & 1) + 2 * q;
+        sL[c0 * LD + r0] = acc1[0];
+        sL[(c0 + 1) * LD + r0] = acc1[1];
+        sL[c0 * LD + r0 + 8] = acc1[2];
+        sL[(c0 + 1) * LD + r0 + 8] = acc1[3];
+      }
+      __syncthreads();
+      // (c) trailing: C(r, c) -= sum_k L(r, k) L(c, k) on the lower triangle
+      const int nti = prow / 16, ntj = prow / 8;
+      for (int tt = warp; tt < nti * ntj; tt += NTHREADS / 32) {
+        const int ti = tt / ntj, tj = tt % ntj;
+        if (8 * tj > 16 * ti + 15) continue;  // tile entirely above the diagonal
+        const int r0 = j1 + 16 * ti + g, c0 = j1 + 8 * tj + 2 * q;
+        double ac[4] = {sL[c0 * LD + r0], sL[(c0 + 1) * LD + r0], sL[c0 * LD + r0 + 8], sL[(c0 + 1) * LD + r0 + 8]};
+        warp_mma_16x8(ac, sL + j0 * LD + j1 + 16 * ti, LD, sL + j0 * LD + j1 + 8 * tj, LD, 1, 16, true);
+        if (r0 >= c0) sL[c0 * LD + r0] = ac[0];
+        if (r0 >= c0 + 1) sL[(c0 + 1) * LD + r0] = ac[1];
+        if (r0 + 8 >= c0) sL[c0 * LD + r0 + 8] = ac[2];
+        if (r0 + 8 >= c0 + 1) sL[(c0 + 1) * LD + r0 + 8] = ac[3];
+      }
+      __syncthreads();
     }
+    POTRF_STAMP(4);
   }
+#pragma unroll 8
+  for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+    const int idx = tid + s2 * NTHREADS;
+    const int r = idx % TILE, c = idx / TILE;
+    if (r < b && c < b && r >= c) X[(int64_t)c * lda + r] = sL[c * LD + r];
+  }
+  POTRF_STAMP(5);
+  if (!want_inv) return;
+  // full inverse, block row by block row (M's diagonal blocks are in place)
+#pragma unroll 1
+  for (int I = 1; I < 4; I++) {
+    const int i0 = 16 * I;
+    const int ntj = i0 / 8;
+    // T(r, c) = sum_{l < i0} L(i0 + r, l) M(l, c), c < i0
+    for (int tj = warp; tj < ntj; tj += NTHREADS / 32) {
+      double ac[4] = {0.0, 0.0, 0.0, 0.0};
+      warp_mma_16x8(ac, sL + i0, LD, sM + (8 * tj) * LD, 1, LD, i0, false);
+      const int c0 = 8 * tj + 2 * q;
+      sT[g + 16 * c0] = ac[0];
+      sT[g + 16 * (c0 + 1)] = ac[1];
+      sT[g + 8 + 16 * c0] = ac[2];
+      sT[g + 8 + 16 * (c0 + 1)] = ac[3];
+    }
+    __syncthreads();
+    // M(i0 + r, c) = -sum_k Minv_II(r, k) T(k, c)
+    for (int tj = warp; tj < ntj; tj += NTHREADS / 32) {
+      double ac[4] = {0.0, 0.0, 0.0, 0.0};
+      warp_mma_16x8(ac, sM + i0 * LD + i0, LD, sT + 16 * (8 * tj), 1, 16, 16, true);
+      const int c0 = 8 * tj + 2 * q, r0 = i0 + g;
+      sM[c0 * LD + r0] = ac[0];
+      sM[(c0 + 1) * LD + r0] = ac[1];
+      sM[c0 * LD + r0 + 8] = ac[2];
+      sM[(c0 + 1) * LD + r0 + 8] = ac[3];
+    }
+    __syncthreads();
+  }
+  POTRF_STAMP(6);
+#pragma unroll 8
+  for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+    const int idx = tid + s2 * NTHREADS;
+    const int r = idx % TILE, cc = idx / TILE;
+    if (r < b && cc < b) Mout[(int64_t)cc * ldm + r] = sM[cc * LD + r];
+  }
+  POTRF_STAMP(7);
 }
 
 // ------------------------------------------------------------ assembly
@@ -270,38 +542,53 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
 //   * for each child, last to first (the order the reference pops its update
 //     stack, cholesky.c:41-52), add U_child(i, q) into F(r[i], r[q]) for the
 //     child columns q whose relative index r[q] lies in the range.
-// F(i, j) is blkval (front panel, ld nj) for j < nn, else U_k (ld na).
+// F(i, j) is blkval (front panel, ld nj) for j < nn, else U_k (ld na).  One
+// warp per child column; children are applied one after the other.
 __device__ void run_asm(const RunArgs& ra, const Task& t) {
   const FrontDesc f = ra.fronts[t.aux[0]];
   const int j0 = t.aux[1], j1 = t.aux[2];
-  double* P = ra.bases[B_X] + f.blk;
-  double* Uk = ra.bases[B_WS] + f.upd;
-  if (t.aux[3] & 1) {
-    for (int j = max(j0, f.nn); j < j1; j++) {
-      int jj = j - f.nn;
-      for (int i = jj + threadIdx.x; i < f.na; i += NTHREADS) Uk[(int64_t)jj * f.na + i] = 0.0;
+  const bool zero_u = (t.aux[3] & 1) != 0;
+  double* __restrict__ P = ra.bases[B_X] + f.blk;
+  double* __restrict__ Uk = ra.bases[B_WS] + f.upd;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (zero_u) {
+    for (int j = max(j0, f.nn) + warp; j < j1; j += NTHREADS / 32) {
+      const int jj = j - f.nn;
+      for (int i = jj + lane; i < f.na; i += 32) Uk[(int64_t)jj * f.na + i] = 0.0;
     }
   }
   __syncthreads();
   for (int l = f.chend - 1; l >= f.chbeg; l--) {
     const FrontDesc ch = ra.fronts[ra.chidx[l]];
     const int N = ch.na;
-    const int32_t* r = ra.relidx + ch.relptr;
-    const double* Uc = ra.bases[B_WS] + ch.upd;
+    const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+    const double* __restrict__ Uc = ra.bases[B_WS] + ch.upd;
     // child columns with r[q] in [j0, j1): r is strictly increasing
     int lo = 0, hi = N;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (r[mid] < j0) lo = mid + 1; else hi = mid; }
-    int q0 = lo;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < j0) lo = mid + 1; else hi = mid; }
+    const int q0 = lo;
     hi = N;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (r[mid] < j1) lo = mid + 1; else hi = mid; }
-    int q1 = lo;
-    for (int q = q0; q < q1; q++) {
-      const int col = r[q];
-      for (int i = q + threadIdx.x; i < N; i += NTHREADS) {
-        const int row = r[i];
-        double v = __ldcg(Uc + (int64_t)q * N + i);
-        if (col < f.nn) P[(int64_t)col * f.nj + row] += v;
-        else Uk[(int64_t)(col - f.nn) * f.na + (row - f.nn)] += v;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < j1) lo = mid + 1; else hi = mid; }
+    const int q1 = lo;
+    for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
+      const int col = __ldg(r + q);
+      double* __restrict__ dst =
+          (col < f.nn) ? P + (int64_t)col * f.nj : Uk + (int64_t)(col - f.nn) * f.na - f.nn;
+      const double* __restrict__ src = Uc + (int64_t)q * N;
+      for (int i0 = q; i0 < N; i0 += 4 * 32) {
+        int ri[4];
+        double u[4], d[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int i = i0 + lane + 32 * e;
+          ri[e] = (i < N) ? __ldg(r + i) : -1;
+          u[e] = (i < N) ? __ldcg(src + i) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++) d[e] = (ri[e] >= 0) ? __ldcg(dst + ri[e]) : 0.0;
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+          if (ri[e] >= 0) dst[ri[e]] = d[e] + u[e];
       }
     }
     __syncthreads();
@@ -309,23 +596,31 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
 }
 
 // ---------------------------------------------------------------- kernel
-__global__ void __launch_bounds__(NTHREADS, 3) engine_kernel(RunArgs ra) {
+__global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   extern __shared__ double smem[];
   __shared__ int s_task;
   __shared__ int s_abort;
+  __shared__ __align__(16) Task s_t;
   SmemLayout sm{smem, smem + TILE * LDS};
   for (;;) {
     if (threadIdx.x == 0) s_task = atomicAdd(&ra.ctl[0], 1);
     __syncthreads();
     const int ti = s_task;
     if (ti >= ra.ntasks) break;
-    const Task& t = ra.tasks[ti];
+    {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(ra.tasks + ti);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_t);
+      for (int w = threadIdx.x; w < (int)(sizeof(Task) / 4); w += NTHREADS) dst[w] = __ldg(src + w);
+    }
+    __syncthreads();
+    const Task& t = s_t;
     if (threadIdx.x == 0) {
+      if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
       int abort = 0;
       for (int w = 0; w < t.nwait && !abort; w++) {
         const int2 wt = ra.waits[t.wait_off + w];
         int64_t spins = 0;
-        unsigned ns = 32;
+        unsigned ns = 16;
         while (ld_acquire(ra.counters + wt.x) < wt.y) {
           if (++spins > ra.spin_limit) {
             atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
@@ -335,11 +630,12 @@ __global__ void __launch_bounds__(NTHREADS, 3) engine_kernel(RunArgs ra) {
           }
           if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
           __nanosleep(ns);
-          if (ns < 256) ns <<= 1;
+          if (ns < 128) ns <<= 1;
         }
       }
       if (!abort && ld_volatile(&ra.ctl[1]) != 0) abort = 1;
       s_abort = abort;
+      if (ra.trace) ra.trace[4 * (int64_t)ti + 1] = global_ns();
     }
     __syncthreads();
     if (s_abort) break;
@@ -354,6 +650,10 @@ __global__ void __launch_bounds__(NTHREADS, 3) engine_kernel(RunArgs ra) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+      if (ra.trace) {
+        ra.trace[4 * (int64_t)ti + 2] = global_ns();
+        ra.trace[4 * (int64_t)ti + 3] = (unsigned long long)sm_id() | ((unsigned long long)t.op << 32);
+      }
       __threadfence();
       red_release_add(ra.counters + ti, 1);
       if (t.group >= 0) red_release_add(ra.counters + t.group, 1);
@@ -361,7 +661,10 @@ __global__ void __launch_bounds__(NTHREADS, 3) engine_kernel(RunArgs ra) {
   }
 }
 
-size_t engine_smem_bytes() { return (size_t)2 * TILE * LDS * sizeof(double); }
+size_t engine_smem_bytes() {
+  const size_t gemm = (size_t)2 * TILE * LDS;
+  return (gemm > (size_t)POTRF_SMEM_DOUBLES ? gemm : (size_t)POTRF_SMEM_DOUBLES) * sizeof(double);
+}
 
 // The dynamic shared-memory attribute must have been raised on the current
 // device by engine_occupancy() (done when a plan is created).

@@ -109,6 +109,7 @@ struct RunArgs {
   const int32_t* relidx;
   const int32_t* chidx;
   int64_t spin_limit;     // polls before a wait gives up
+  unsigned long long* trace;  // optional: 4 words per task (claim, start, end, sm | op << 32)
 };
 
 // Error codes written to ctl[1].

@@ -95,6 +95,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.relidx = plan->d_relidx;
   ra.chidx = plan->d_chidx;
   ra.spin_limit = 40000000LL;  // about 10 s of polling at the longest back-off
+  ra.trace = (plan->trace && plan->trace_cap >= (int64_t)prog->tasks.size()) ? plan->trace : nullptr;
   int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
   CUDA_TRY(engine_launch(ra, grid, stream));
   return 0;
@@ -249,5 +250,13 @@ extern "C" int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, 
   if (tasks) std::memcpy(tasks, p->tasks.data(), p->tasks.size() * sizeof(Task));
   if (waits) std::memcpy(waits, p->waits.data(), p->waits.size() * sizeof(int2));
   if (fronts) std::memcpy(fronts, plan->fronts.data(), plan->fronts.size() * sizeof(FrontDesc));
+  return 0;
+}
+
+extern "C" int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks) {
+  clear_error();
+  if (!plan) return set_error(-1, "null plan");
+  plan->trace = (unsigned long long*)buffer;
+  plan->trace_cap = buffer ? capacity_tasks : 0;
   return 0;
 }

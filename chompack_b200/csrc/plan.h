@@ -63,6 +63,8 @@ struct chb_plan {
   int32_t* d_chidx = nullptr;
   int64_t* d_perm = nullptr;    // p (trsm row gather)
   int grid = 0;                 // persistent grid size
+  unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
+  int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;
 };
 

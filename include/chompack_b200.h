@@ -142,6 +142,12 @@ int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const doubl
 int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
             size_t work_bytes, void* stream);
 
+/* Profiling: when `buffer` (device memory, 32 bytes per task) is set, the
+ * next sweeps whose task count fits `capacity_tasks` record per task the
+ * global-timer ns at claim, start (dependencies met) and end, and the SM id
+ * | task kind << 32.  Pass NULL to switch tracing off. */
+int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
+
 /* Synchronise `stream` and return the status of the last sweep run with this
  * workspace: 0, or the 1-based failing column of the first failing front
  * (LAPACK info convention), or < 0 on a device-side consistency error. */
