@@ -58,6 +58,20 @@ def cholesky(X):
         raise ArithmeticError("factorization failed")
 
 
+def projected_inverse(L):
+    """Supernodal multifrontal projected inverse Y = P(L^{-T} L^{-1}), in place
+    (cbase.c:393-500).  On exit L holds Y and L.is_factor is False."""
+    if L.is_factor is not True:
+        raise ValueError("X must be a cspmatrix")
+    v = _values(L)
+    plan = L.symb.plan(v.device.index)
+    info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
+                           lambda ws, nb, s: N.projected_inverse(plan.handle, v.data_ptr(), ws, nb, s))
+    L.is_factor = False
+    if info:
+        raise ArithmeticError("partial inverse failed")
+
+
 def _missing(name):
     def f(*args, **kwargs):
         raise NotImplementedError("%s is not available in this build" % name)
@@ -66,7 +80,6 @@ def _missing(name):
 
 
 llt = _missing("llt")
-projected_inverse = _missing("projected_inverse")
 completion = _missing("completion")
 hessian = _missing("hessian")
 trsm = _missing("trsm")

@@ -80,6 +80,8 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         t.aux[1] = j0;
         t.aux[2] = j1;
         t.aux[3] = na > 0 ? 1 : 0;
+        t.a = opnd(B_X, blk, nj);
+        t.c = opnd(B_WS, upd, std::max(na, 1));
         int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group, 3.0 + w / 2000.0);
         for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
         j0 = j1;

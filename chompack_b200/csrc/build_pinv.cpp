@@ -1,0 +1,211 @@
+// Task program of the projected-inverse sweep Y = P(X^{-1}) from the factor
+// (reference: projected_inverse.c:3-75), run in reverse postorder (parents
+// before children).
+//
+// Per supernode k, with L = L_kk (diagonal block of the factor), W = the
+// stored off-diagonal block (L_{Ak,Nk} L_kk^{-1}) and V_k = the update the
+// parent extracted for k (na x na, in the update buffer of k):
+//   M   = L^{-1}                             (dtrtri, :33)
+//   Y11 = M^T M                              (dsyrk, :42)
+//   S21 = -V_k W                             (dsymm, :53)
+//   Y11 = Y11 - S21^T W                      (dgemm, :57)
+//   U_c = F[r_c, r_c] for every child c      (:62-71)
+//   blk = [Y11 (lower, upper zeroed); S21]   (:36-38, :73)
+// M is built tile-wise: inverses of the 64x64 diagonal tiles (independent)
+// and the block rows below them (M(c, j) = -M_cc sum_l L(c, l) M(l, j)).
+// Y11 and S21 live in scratch until every reader of the factor block is done,
+// then are copied back into blkval.
+#include "dag.h"
+
+namespace chb {
+
+int build_projected_inverse(const chb_plan& P, Program& prog) {
+  const int T = TILE;
+  const int CH = 16;  // child columns per extract task
+  const int64_t N = P.nsn;
+  DagBuilder B;
+
+  int64_t ws = P.upd_total;
+  std::vector<int64_t> scrM(N), scrY(N), scrS(N, -1);
+  for (int64_t k = 0; k < N; k++) {
+    const FrontDesc& f = P.fronts[k];
+    scrM[k] = ws;
+    ws += (int64_t)f.nn * f.nn;
+    scrY[k] = ws;
+    ws += (int64_t)f.nn * f.nn;
+    if (f.na > 0) {
+      scrS[k] = ws;
+      ws += (int64_t)f.na * f.nn;
+    }
+  }
+  prog.ws_doubles = ws;
+
+  // group: the parent's extract tasks that produce V_k (k non-root)
+  std::vector<int> vready(N, -1);
+  for (int64_t k = 0; k < N; k++)
+    if (P.fronts[k].na > 0) vready[k] = B.new_group();
+
+  const int maxlv = P.nlevels;
+  std::vector<int> inv, last_mrow;
+  for (int64_t k = N - 1; k >= 0; k--) {
+    const FrontDesc& f = P.fronts[k];
+    const int nn = f.nn, na = f.na, nj = f.nj;
+    const int lv = maxlv - f.level;  // roots first
+    const int NBc = ceil_div(nn, T), NBb = ceil_div(na, T);
+    const int64_t blk = f.blk, upd = f.upd, M = scrM[k], Y = scrY[k], S = scrS[k];
+    auto bw = [&](int c) { return std::min(T, nn - c * T); };
+    auto bh = [&](int i) { return std::min(T, na - i * T); };
+
+    // M = L^{-1}: diagonal tiles
+    inv.assign(NBc, -1);
+    for (int c = 0; c < NBc; c++) {
+      const int cT = c * T;
+      Task t = make_task(T_POTRF);
+      t.m = t.n = bw(c);
+      t.a = opnd(B_X, blk + (int64_t)cT * nj + cT, nj);
+      t.c = opnd(B_WS, M + (int64_t)cT * nn + cT, nn);
+      t.aux[0] = cT;
+      t.aux[1] = 1;
+      t.aux[2] = 1;  // invert only
+      inv[c] = B.add(t, {lv, 0, 0, (int)k, c, 0});
+    }
+    // block rows of M below the diagonal tiles
+    last_mrow.assign(NBc, -1);
+    for (int c = 1; c < NBc; c++) {
+      const int cT = c * T;
+      for (int j = 0; j < c; j++) {
+        const int jT = j * T;
+        Task t = make_task(T_MROW);
+        t.m = bw(c);
+        t.n = T;
+        t.k = cT - jT;
+        t.alpha = -1.0;
+        t.a = opnd(B_X, blk + (int64_t)jT * nj + cT, nj);
+        t.b = opnd(B_WS, M + (int64_t)jT * nn + jT, nn, OM_TRI_T, 0);
+        t.c = opnd(B_WS, M + (int64_t)jT * nn + cT, nn);
+        const int64_t moff = M + (int64_t)cT * nn + cT;
+        t.aux[0] = B_WS;
+        t.aux[1] = nn;
+        t.aux[2] = (int32_t)(uint32_t)(moff & 0xffffffffLL);
+        t.aux[3] = (int32_t)(moff >> 32);
+        int id = B.add(t, {lv, 1, c, (int)k, j, 0});
+        B.wait_task(id, inv[c]);
+        B.wait_task(id, inv[j]);
+        if (c - 1 > j) B.wait_task(id, last_mrow[j]);
+        last_mrow[j] = id;
+      }
+    }
+    // Y11 = M^T M (lower tiles)
+    std::vector<int> y11(NBc * NBc, -1);
+    for (int i = 0; i < NBc; i++) {
+      for (int j = 0; j <= i; j++) {
+        const int iT = i * T, jT = j * T;
+        Operand a = opnd(B_WS, M + (int64_t)iT * nn + iT, nn, OM_TRI_T, 0);
+        Operand b = opnd(B_WS, M + (int64_t)jT * nn + iT, nn, i == j ? OM_TRI_T : OM_T, 0);
+        Operand c = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
+        Task t = gemm(bw(i), bw(j), nn - iT, 1.0, a, b, 0.0, c, i == j, 0);
+        int id = B.add(t, {lv, 2, 0, (int)k, j, i});
+        B.wait_task(id, inv[i]);
+        B.wait_task(id, inv[j]);
+        if (i < NBc - 1) B.wait_task(id, last_mrow[i]);
+        if (j < NBc - 1) B.wait_task(id, last_mrow[j]);
+        y11[i * NBc + j] = id;
+      }
+    }
+    const int yfinal = B.new_group();
+    const int sgroup = na > 0 ? B.new_group() : -1;
+    if (na > 0) {
+      // S21 = -V_k W
+      for (int i = 0; i < NBb; i++) {
+        for (int j = 0; j < NBc; j++) {
+          const int iT = i * T, jT = j * T;
+          Operand a = opnd(B_WS, upd, na, OM_SYM, iT);
+          Operand b = opnd(B_X, blk + (int64_t)jT * nj + nn, nj, OM_T, 0);
+          Operand c = opnd(B_WS, S + (int64_t)jT * na + iT, na);
+          Task t = gemm(bh(i), bw(j), na, -1.0, a, b, 0.0, c);
+          int id = B.add(t, {lv, 3, 0, (int)k, j, i}, sgroup);
+          B.wait_group(id, vready[k]);
+        }
+      }
+      // Y11 -= S21^T W
+      for (int i = 0; i < NBc; i++) {
+        for (int j = 0; j <= i; j++) {
+          const int iT = i * T, jT = j * T;
+          Operand a = opnd(B_WS, S + (int64_t)iT * na, na, OM_T, 0);
+          Operand b = opnd(B_X, blk + (int64_t)jT * nj + nn, nj, OM_T, 0);
+          Operand c = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
+          Task t = gemm(bw(i), bw(j), na, -1.0, a, b, 1.0, c, i == j, 0);
+          int id = B.add(t, {lv, 4, 0, (int)k, j, i}, yfinal);
+          B.wait_task(id, y11[i * NBc + j]);
+          B.wait_group(id, sgroup);
+        }
+      }
+    } else {
+      // root: Y11 = M^T M is final; mark it with a copy-free group via the
+      // tile tasks themselves
+      for (int i = 0; i < NBc; i++)
+        for (int j = 0; j <= i; j++) {
+          B.group_of[y11[i * NBc + j]] = yfinal;
+          B.group_size[yfinal]++;
+        }
+    }
+    // children's updates
+    for (int l = f.chbeg; l < f.chend; l++) {
+      const int c = P.chidx[l];
+      const int Nc = P.fronts[c].na;
+      for (int q0 = 0; q0 < Nc; q0 += CH) {
+        Task t = make_task(T_EXTRACT);
+        t.aux[0] = c;
+        t.aux[1] = q0;
+        t.aux[2] = std::min(Nc, q0 + CH);
+        t.a = opnd(B_WS, Y, nn);
+        t.b = opnd(B_WS, na > 0 ? S : 0, std::max(na, 1));
+        t.c = opnd(B_WS, upd, std::max(na, 1));
+        int id = B.add(t, {lv, 5, 0, (int)k, c, q0}, vready[c], 3.0 + (double)(Nc - q0) * CH / 2000.0);
+        B.wait_group(id, yfinal);
+        B.wait_group(id, sgroup);
+      }
+    }
+    // copy back into blkval (all readers of the factor block are done once
+    // the final Y11 tiles are: they wait on every M tile and S21 tile)
+    for (int i = 0; i < NBc; i++) {
+      for (int j = 0; j <= i; j++) {
+        const int iT = i * T, jT = j * T;
+        Task t = make_task(T_COPY);
+        t.m = bw(i);
+        t.n = bw(j);
+        t.a = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + iT, nj);
+        t.aux[0] = (i == j) ? 3 : 0;
+        int id = B.add(t, {lv, 6, 0, (int)k, j, i});
+        B.wait_group(id, yfinal);
+      }
+      // strict upper tiles of the diagonal block are zeroed too
+      for (int j = i + 1; j < NBc; j++) {
+        const int iT = i * T, jT = j * T;
+        Task t = make_task(T_COPY);
+        t.m = bw(i);
+        t.n = bw(j);
+        t.aux[0] = 4;  // zeros
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + iT, nj);
+        int id = B.add(t, {lv, 6, 1, (int)k, j, i});
+        B.wait_group(id, yfinal);
+      }
+    }
+    for (int i = 0; i < NBb; i++) {
+      for (int j = 0; j < NBc; j++) {
+        const int iT = i * T, jT = j * T;
+        Task t = make_task(T_COPY);
+        t.m = bh(i);
+        t.n = bw(j);
+        t.a = opnd(B_WS, S + (int64_t)jT * na + iT, na);
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + nn + iT, nj);
+        int id = B.add(t, {lv, 6, 2, (int)k, j, i});
+        B.wait_group(id, yfinal);
+      }
+    }
+  }
+  return B.finish(prog, P.grid > 0 ? P.grid : 296);
+}
+
+}  // namespace chb

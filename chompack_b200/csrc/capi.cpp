@@ -35,6 +35,11 @@ extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t w
   return run_op(plan, CHB_OP_CHOLESKY, 0, 0, bases, 1, work, work_bytes, stream);
 }
 
+extern "C" int chb_projected_inverse(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
+  double* bases[1] = {blkval};
+  return run_op(plan, CHB_OP_PROJECTED_INVERSE, 0, 0, bases, 1, work, work_bytes, stream);
+}
+
 extern "C" int chb_info(chb_plan* plan, void* work, void* stream) {
   clear_error();
   int rc = check_plan(plan);

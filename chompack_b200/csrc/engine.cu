@@ -368,6 +368,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
   const int lda = t.a.ld;
   const int info_base = t.aux[0];
   const bool want_inv = t.aux[1] != 0;
+  const bool factor = t.aux[2] == 0;  // aux[2] != 0: the tile already holds L; invert only
   double* __restrict__ Mout = want_inv ? ra.bases[t.c.base] + t.c.off : nullptr;
   const int ldm = t.c.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -395,9 +396,20 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
 #pragma unroll 1
   for (int J = 0; J < 4; J++) {
     const int j0 = 16 * J, j1 = j0 + 16;
+    if (warp == 0 && !factor) {
+      // invert-only: reciprocals of the diagonal (a zero pivot is singular)
+      const int il = lane & 15;
+      const double d = sL[(j0 + il) * LD + j0 + il];
+      if (lane < 16) {
+        if (d == 0.0 && j0 + il < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + il + 1);
+        rdiag[j0 + il] = 1.0 / (d == 0.0 ? 1.0 : d);
+      }
+      __syncwarp();
+    }
     if (warp == 0) {
       // (a) factor the 16x16 diagonal block in registers: lane i < 16 row i
       const int il = lane & 15;
+      if (factor) {
       double a[16];
 #pragma unroll
       for (int c = 0; c < 16; c++) a[c] = sL[(j0 + c) * LD + j0 + il];
@@ -420,6 +432,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
 #pragma unroll
         for (int c = 0; c < 16; c++)
           if (c <= il) sL[(j0 + c) * LD + j0 + il] = a[c];
+      }
       }
       __syncwarp();
       POTRF_STAMP(1);
@@ -444,7 +457,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
     __syncthreads();
     POTRF_STAMP(3);
     const int prow = TILE - j1;  // rows below the block: 48, 32, 16, 0
-    if (prow > 0) {
+    if (factor && prow > 0) {
       // (b) panel: X(r, n) = sum_k A(r, k) Minv(n, k), 16x8 tiles; at most
       // six tiles, so warp w owns tiles w and w + 4
       const int ntiles = (prow / 16) * 2;
@@ -489,11 +502,13 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
     }
     POTRF_STAMP(4);
   }
+  if (factor) {
 #pragma unroll 8
-  for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
-    const int idx = tid + s2 * NTHREADS;
-    const int r = idx % TILE, c = idx / TILE;
-    if (r < b && c < b && r >= c) X[(int64_t)c * lda + r] = sL[c * LD + r];
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = tid + s2 * NTHREADS;
+      const int r = idx % TILE, c = idx / TILE;
+      if (r < b && c < b && r >= c) X[(int64_t)c * lda + r] = sL[c * LD + r];
+    }
   }
   POTRF_STAMP(5);
   if (!want_inv) return;
@@ -542,19 +557,22 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
 //   * for each child, last to first (the order the reference pops its update
 //     stack, cholesky.c:41-52), add U_child(i, q) into F(r[i], r[q]) for the
 //     child columns q whose relative index r[q] lies in the range.
-// F(i, j) is blkval (front panel, ld nj) for j < nn, else U_k (ld na).  One
-// warp per child column; children are applied one after the other.
+// F(i, j) is the front panel (operand a: nj rows, ld a.ld) for j < nn, else
+// the update block U_k (operand c, ld c.ld).  One warp per child column;
+// children are applied one after the other.
 __device__ void run_asm(const RunArgs& ra, const Task& t) {
   const FrontDesc f = ra.fronts[t.aux[0]];
   const int j0 = t.aux[1], j1 = t.aux[2];
   const bool zero_u = (t.aux[3] & 1) != 0;
-  double* __restrict__ P = ra.bases[B_X] + f.blk;
-  double* __restrict__ Uk = ra.bases[B_WS] + f.upd;
+  double* __restrict__ P = ra.bases[t.a.base] + t.a.off;
+  const int ldp = t.a.ld;
+  double* __restrict__ Uk = ra.bases[t.c.base] + t.c.off;
+  const int ldu = t.c.ld;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (zero_u) {
     for (int j = max(j0, f.nn) + warp; j < j1; j += NTHREADS / 32) {
       const int jj = j - f.nn;
-      for (int i = jj + lane; i < f.na; i += 32) Uk[(int64_t)jj * f.na + i] = 0.0;
+      for (int i = jj + lane; i < f.na; i += 32) Uk[(int64_t)jj * ldu + i] = 0.0;
     }
   }
   __syncthreads();
@@ -573,7 +591,7 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
     for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
       const int col = __ldg(r + q);
       double* __restrict__ dst =
-          (col < f.nn) ? P + (int64_t)col * f.nj : Uk + (int64_t)(col - f.nn) * f.na - f.nn;
+          (col < f.nn) ? P + (int64_t)col * ldp : Uk + (int64_t)(col - f.nn) * ldu - f.nn;
       const double* __restrict__ src = Uc + (int64_t)q * N;
       for (int i0 = q; i0 < N; i0 += 4 * 32) {
         int ri[4];
@@ -592,6 +610,76 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
       }
     }
     __syncthreads();
+  }
+}
+
+// Gather of a child's update matrix out of its parent's front
+// (projected_inverse.c:62-71, completion.c:61-66): for child c = aux[0] and
+// child columns q in [aux[1], aux[2]), U_c(i, q) = F(r[i], r[q]) for i >= q,
+// where F(row, col) (col <= row) is read from
+//   operand a (rows < nn, ld a.ld) when row < nn,
+//   operand b (rows >= nn, row nn at offset 0, ld b.ld) when col < nn <= row,
+//   operand c (update block, ld c.ld) when col >= nn.
+__device__ void run_extract(const RunArgs& ra, const Task& t) {
+  const FrontDesc ch = ra.fronts[t.aux[0]];
+  const FrontDesc f = ra.fronts[ch.parent];
+  const int q0 = t.aux[1], q1 = t.aux[2];
+  const int N = ch.na, nn = f.nn;
+  const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+  const double* __restrict__ F11 = ra.bases[t.a.base] + t.a.off;
+  const double* __restrict__ F21 = ra.bases[t.b.base] + t.b.off;
+  const double* __restrict__ F22 = ra.bases[t.c.base] + t.c.off;
+  const int ld11 = t.a.ld, ld21 = t.b.ld, ld22 = t.c.ld;
+  double* __restrict__ Uc = ra.bases[B_WS] + ch.upd;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
+    const int col = __ldg(r + q);
+    for (int i0 = q; i0 < N; i0 += 4 * 32) {
+      double v[4];
+      int idx[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int i = i0 + lane + 32 * e;
+        idx[e] = i;
+        const int row = (i < N) ? __ldg(r + i) : 0;
+        const double* src;
+        if (col >= nn) src = F22 + (int64_t)(col - nn) * ld22 + (row - nn);
+        else if (row >= nn) src = F21 + (int64_t)col * ld21 + (row - nn);
+        else src = F11 + (int64_t)col * ld11 + row;
+        v[e] = (i < N) ? __ldcg(src) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++)
+        if (idx[e] < N) Uc[(int64_t)q * N + idx[e]] = v[e];
+    }
+  }
+}
+
+// Tile copy C = alpha * A (m x n).  aux[0] bit 0: copy only the lower
+// triangle (r >= c); bit 1: write zeros above the diagonal; bit 2: write
+// zeros everywhere (A is not read).
+__device__ void run_copy(const RunArgs& ra, const Task& t) {
+  const double* __restrict__ A = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+  const int lda = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n;
+  const bool lower = (t.aux[0] & 1) != 0, zup = (t.aux[0] & 2) != 0, zall = (t.aux[0] & 4) != 0;
+  const double alpha = t.alpha;
+  for (int base = 0; base < m * n; base += 8 * NTHREADS) {
+    double v[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int idx = base + threadIdx.x + e * NTHREADS;
+      const int r = idx % m, c = idx / m;
+      v[e] = (!zall && idx < m * n && (!lower || r >= c)) ? __ldcg(A + (int64_t)c * lda + r) : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int idx = base + threadIdx.x + e * NTHREADS;
+      const int r = idx % m, c = idx / m;
+      if (idx >= m * n) continue;
+      if (r >= c || !lower) C[(int64_t)c * ldc + r] = alpha * v[e];
+      else if (zup) C[(int64_t)c * ldc + r] = 0.0;
+    }
   }
 }
 
@@ -644,6 +732,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem); break;
       case T_ASM: run_asm(ra, t); break;
+      case T_EXTRACT: run_extract(ra, t); break;
+      case T_COPY: run_copy(ra, t); break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;

@@ -52,6 +52,7 @@ static Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags)
   int rc;
   switch (op) {
     case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
+    case CHB_OP_PROJECTED_INVERSE: rc = build_projected_inverse(*plan, *prog); break;
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;

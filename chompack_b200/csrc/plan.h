@@ -84,4 +84,5 @@ int engine_occupancy(int* blocks_per_sm);
 
 // Program builders (one per sweep), in build_*.cpp.
 int build_cholesky(const chb_plan& P, Program& prog);
+int build_projected_inverse(const chb_plan& P, Program& prog);
 }  // namespace chb

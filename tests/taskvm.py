@@ -30,7 +30,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
                   ("scr", "<i8"), ("scr2", "<i8")])
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
-T_GEMM, T_POTRF, T_ASM, T_MROW = 0, 1, 2, 3
+T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
 B_X, B_WS = 0, 1
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
@@ -120,21 +120,44 @@ class VM(object):
             r = np.arange(b)[:, None]
             c = np.arange(b)[None, :]
             tile = X[off + c * ld + r]
-            S = np.tril(tile) + np.tril(tile, -1).T
-            try:
-                L = np.linalg.cholesky(S)
-            except np.linalg.LinAlgError:
-                if self.info == 0:
+            if int(t["aux"][2]):
+                L = np.tril(tile)
+                if np.any(np.diag(L) == 0.0) and self.info == 0:
                     self.info = int(t["aux"][0]) + 1
-                L = np.nan_to_num(np.tril(tile))
-            idx = off + c * ld + r
-            low = r >= c
-            X[idx[low]] = L[low]
+            else:
+                S = np.tril(tile) + np.tril(tile, -1).T
+                try:
+                    L = np.linalg.cholesky(S)
+                except np.linalg.LinAlgError:
+                    if self.info == 0:
+                        self.info = int(t["aux"][0]) + 1
+                    L = np.nan_to_num(np.tril(tile))
+                idx = off + c * ld + r
+                low = r >= c
+                X[idx[low]] = L[low]
             if int(t["aux"][1]):
                 M = np.linalg.inv(L)
                 _store(self.bases[int(t["c"]["base"])], t["c"], b, b, np.tril(M), False, 0, 0.0)
         elif op == T_ASM:
             self._asm(t)
+        elif op == T_EXTRACT:
+            self._extract(t)
+        elif op == T_COPY:
+            m, n = int(t["m"]), int(t["n"])
+            fl = int(t["aux"][0])
+            r = np.arange(m)[:, None]
+            c = np.arange(n)[None, :]
+            C = self.bases[int(t["c"]["base"])]
+            cidx = int(t["c"]["off"]) + c * int(t["c"]["ld"]) + r
+            if fl & 4:
+                C[cidx] = 0.0
+            else:
+                A = self.bases[int(t["a"]["base"])]
+                v = float(t["alpha"]) * A[int(t["a"]["off"]) + c * int(t["a"]["ld"]) + r]
+                low = (r >= c) | (not (fl & 1))
+                C[cidx[low]] = v[low]
+                if fl & 2:
+                    C[cidx[~low]] = 0.0
         else:
             raise NotImplementedError("task op %d" % op)
 
@@ -142,12 +165,13 @@ class VM(object):
         f = self.p.fronts[int(t["aux"][0])]
         j0, j1 = int(t["aux"][1]), int(t["aux"][2])
         nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
-        X, WS = self.bases[B_X], self.bases[B_WS]
-        blk, upd = int(f["blk"]), int(f["upd"])
+        WS = self.bases[B_WS]
+        Pb, Pof, ldp = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
+        Ub, Uof, ldu = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
         if int(t["aux"][3]) & 1:
             for j in range(max(j0, nn), j1):
                 jj = j - nn
-                WS[upd + jj * na + jj: upd + jj * na + na] = 0.0
+                Ub[Uof + jj * ldu + jj: Uof + jj * ldu + na] = 0.0
         for l in range(int(f["chend"]) - 1, int(f["chbeg"]) - 1, -1):
             ch = self.p.fronts[self.chidx[l]]
             Nc = int(ch["na"])
@@ -160,9 +184,35 @@ class VM(object):
                 rows = r[q:]
                 v = Uc[q:, q]
                 if col < nn:
-                    X[blk + col * nj + rows] += v
+                    Pb[Pof + col * ldp + rows] += v
                 else:
-                    WS[upd + (col - nn) * na + (rows - nn)] += v
+                    Ub[Uof + (col - nn) * ldu + (rows - nn)] += v
+
+    def _extract(self, t):
+        ch = self.p.fronts[int(t["aux"][0])]
+        f = self.p.fronts[int(ch["parent"])]
+        q0, q1 = int(t["aux"][1]), int(t["aux"][2])
+        Nc, nn = int(ch["na"]), int(f["nn"])
+        r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+        A = (self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"]))
+        Bb = (self.bases[int(t["b"]["base"])], int(t["b"]["off"]), int(t["b"]["ld"]))
+        C = (self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
+        WS = self.bases[B_WS]
+        up = int(ch["upd"])
+        for q in range(q0, q1):
+            col = int(r[q])
+            for i in range(q, Nc):
+                row = int(r[i])
+                if col >= nn:
+                    buf, off, ld = C
+                    v = buf[off + (col - nn) * ld + row - nn]
+                elif row >= nn:
+                    buf, off, ld = Bb
+                    v = buf[off + col * ld + row - nn]
+                else:
+                    buf, off, ld = A
+                    v = buf[off + col * ld + row]
+                WS[up + q * Nc + i] = v
 
     def run(self, order="list", seed=0):
         tasks = self.p.tasks
