@@ -44,7 +44,7 @@ static int upload_program(Program& prog) {
 
 // Builds the host side of a program only (no device upload); used by the
 // introspection entry points, which must work without a GPU.
-static Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
+Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   ProgKey key{op, k, flags};
   auto it = plan->progs.find(key);
   if (it != plan->progs.end()) return it->second.get();

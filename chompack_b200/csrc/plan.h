@@ -72,6 +72,8 @@ namespace chb {
 // Build (or fetch) the program of an operation.  Returns nullptr and sets
 // the error text on failure.
 Program* get_program(chb_plan* plan, int op, int64_t k, int flags);
+// Host side only (no device upload).
+Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags);
 
 // Launch a program.  bases: MAX_BASES device pointers (unused slots null).
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,

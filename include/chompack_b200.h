@@ -148,6 +148,22 @@ int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, vo
  * | task kind << 32.  Pass NULL to switch tracing off. */
 int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
 
+/* Allocation-free Cholesky.  No counterpart in the reference: an addition for
+ * callers that cannot call cudaMalloc when they factor (code running under
+ * CUDA graph capture, frameworks whose device memory all comes from their own
+ * pool, processes that must not grow their device footprint after start-up).
+ * Same result as chb_cholesky, but all device scratch comes from one static
+ * __device__ array of CHB_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU which
+ * loads this library holds until the process exits; problems that need more
+ * are rejected with error -40 and a message giving the size.  The plan may be
+ * host-only (device < 0).  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current: make that
+ * first call before any stream capture.  The call is synchronous and returns
+ * the status like chb_info.  Every call shares the one array, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialise them. */
+#define CHB_NOALLOC_SCRATCH_BYTES (32u << 20)
+int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream);
+
 /* Synchronise `stream` and return the status of the last sweep run with this
  * workspace: 0, or the 1-based failing column of the first failing front
  * (LAPACK info convention), or < 0 on a device-side consistency error. */
