@@ -69,6 +69,9 @@ workspace_size = _sig("chb_workspace_size", ctypes.c_int,
 program_info = _sig("chb_program_info", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64])
 cholesky = _sig("chb_cholesky", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 projected_inverse = _sig("chb_projected_inverse", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
+llt = _sig("chb_llt", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
+trsm = _sig("chb_trsm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
+dot = _sig("chb_dot", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
 set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 

@@ -72,6 +72,91 @@ def projected_inverse(L):
         raise ArithmeticError("partial inverse failed")
 
 
+def llt(L):
+    """Supernodal multifrontal Cholesky product X = L L^T, in place
+    (cbase.c:287-390).  On exit L holds X and L.is_factor is False."""
+    if L.is_factor is not True:
+        raise ValueError("X must be a cspmatrix")
+    v = _values(L)
+    plan = L.symb.plan(v.device.index)
+    _run_and_status(plan, N.OP_LLT, lambda ws, nb, s: N.llt(plan.handle, v.data_ptr(), ws, nb, s))
+    L.is_factor = False
+
+
+def trsm(L, B, alpha=1.0, trans='N', nrhs=None, offsetB=0, ldB=None):
+    """Triangular solve with a cspmatrix factor (cbase.c:944-1077):
+    B := alpha L^{-1} B (trans 'N') or alpha L^{-T} B (trans 'T'), in place.
+
+    B holds the right-hand sides column by column (column-major), rows in
+    the original order: a CUDA float64 tensor whose element (i, j) is at
+    storage offset i + j*ld (a 1-D tensor, or a 2-D tensor with stride(0) ==
+    1), or a Fortran-ordered numpy array (copied to the GPU and back)."""
+    if L.is_factor is not True:
+        raise ValueError("L must be a cspmatrix factor")
+    if trans not in ('N', 'T'):
+        raise ValueError("trans must be 'N' or 'T'")
+    v = _values(L, "L")
+    dev = v.device
+    host = None
+    if isinstance(B, torch.Tensor):
+        if B.device != dev or B.dtype != torch.float64:
+            raise ValueError("B must be a float64 tensor on the device of L")
+        if B.dim() == 1:
+            rows, cols, ld0 = B.shape[0], 1, B.shape[0]
+        elif B.stride(0) == 1:
+            rows, cols, ld0 = B.shape[0], B.shape[1], B.stride(1)
+        else:
+            raise ValueError("B must be column-major (stride(0) == 1)")
+        Bt = B
+    else:
+        import numpy as np
+        host = np.asarray(B)
+        if host.dtype != np.float64:
+            raise ValueError("B must be float64")
+        if host.ndim == 1:
+            rows, cols, ld0 = host.shape[0], 1, host.shape[0]
+        else:
+            if not host.flags["F_CONTIGUOUS"]:
+                raise ValueError("B must be column-major (Fortran order)")
+            rows, cols, ld0 = host.shape[0], host.shape[1], host.shape[0]
+        Bt = torch.from_numpy(host.reshape(-1, order="F")).to(dev)
+    if nrhs is None:
+        nrhs = cols
+    if ldB is None:
+        ldB = ld0 if host is None else rows
+    plan = L.symb.plan(dev.index)
+    flags = 1 if trans == 'T' else 0
+    ptr = Bt.data_ptr() + 8 * int(offsetB)
+    _run_and_status(plan, N.OP_TRSM,
+                    lambda ws, nb, s: N.trsm(plan.handle, trans.encode(), int(nrhs), float(alpha), v.data_ptr(), ptr,
+                                             int(ldB), ws, nb, s), k=int(nrhs), flags=flags)
+    if host is not None:
+        out = Bt.cpu().numpy()
+        host.reshape(-1, order="F")[:] = out if host.ndim == 1 else out
+        if host.ndim > 1:
+            host[:, :] = out.reshape(host.shape, order="F")
+
+
+def dot(X, Y):
+    """Trace inner product <X, Y> of two chordal matrices on the same
+    symbolic factorisation (cbase.c:106-174); None if the factorisations
+    differ, as in the reference."""
+    if X.is_factor is not False:
+        raise ValueError("X must be a cspmatrix")
+    if Y.is_factor is not False:
+        raise ValueError("Y must be a cspmatrix")
+    if X.symb is not Y.symb:
+        return None
+    x = _values(X)
+    y = _values(Y, "Y")
+    plan = X.symb.plan(x.device.index)
+    ws, nb = plan.workspace(N.OP_DOT)
+    out = torch.empty(1, dtype=torch.float64, device=x.device)
+    s = _stream(x.device)
+    _check(N.dot(plan.handle, x.data_ptr(), y.data_ptr(), out.data_ptr(), ws, nb, s), "dot")
+    return float(out.item())
+
+
 def _missing(name):
     def f(*args, **kwargs):
         raise NotImplementedError("%s is not available in this build" % name)
@@ -79,8 +164,5 @@ def _missing(name):
     return f
 
 
-llt = _missing("llt")
 completion = _missing("completion")
 hessian = _missing("hessian")
-trsm = _missing("trsm")
-dot = _missing("dot")

@@ -19,13 +19,13 @@ int check_plan(chb_plan* plan) {
 }
 
 int run_op(chb_plan* plan, int op, int64_t k, int flags, double* const* bases, int nbases, void* work,
-           size_t work_bytes, void* stream) {
+           size_t work_bytes, void* stream, int64_t ldb = 0, double alpha = 1.0) {
   clear_error();
   int rc = check_plan(plan);
   if (rc) return rc;
   Program* prog = get_program(plan, op, k, flags);
   if (!prog) return -2;
-  return run_program(plan, prog, work, work_bytes, bases, nbases, (cudaStream_t)stream);
+  return run_program(plan, prog, work, work_bytes, bases, nbases, (cudaStream_t)stream, ldb, alpha);
 }
 
 }  // namespace
@@ -38,6 +38,33 @@ extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t w
 extern "C" int chb_projected_inverse(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
   double* bases[1] = {blkval};
   return run_op(plan, CHB_OP_PROJECTED_INVERSE, 0, 0, bases, 1, work, work_bytes, stream);
+}
+
+extern "C" int chb_llt(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
+  double* bases[1] = {blkval};
+  return run_op(plan, CHB_OP_LLT, 0, 0, bases, 1, work, work_bytes, stream);
+}
+
+extern "C" int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
+                        int64_t ldB, void* work, size_t work_bytes, void* stream) {
+  if (trans != 'N' && trans != 'T') return set_error(-1, "trans must be 'N' or 'T'");
+  if (nrhs < 0 || (plan && ldB < plan->n)) return set_error(-1, "invalid nrhs or ldB");
+  double* bases[B_RHS + 1] = {const_cast<double*>(blkval), nullptr, nullptr, nullptr, B};
+  return run_op(plan, CHB_OP_TRSM, nrhs, trans == 'T' ? 1 : 0, bases, B_RHS + 1, work, work_bytes, stream, ldB,
+                alpha);
+}
+
+extern "C" int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
+                       size_t work_bytes, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  const size_t need = 256 + (size_t)(plan->nsn + 1) * sizeof(double);
+  if (work_bytes < need || !work) return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, need);
+  double* partial = (double*)((char*)work + 256);
+  cudaError_t e = dot_launch(x, y, plan->d_fronts, (int)plan->nsn, partial, result, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(-100 - (int)e, "dot launch failed: %s", cudaGetErrorString(e));
+  return 0;
 }
 
 extern "C" int chb_info(chb_plan* plan, void* work, void* stream) {

@@ -1,0 +1,65 @@
+// Trace inner product <X, Y> of two chordal matrices on the same pattern
+// (reference: dot.c:3-23): sum over the lower trapezoid of every supernode
+// block, off-diagonal entries counted twice.  One CTA per supernode block
+// writes a partial sum; a single CTA adds the partials in a fixed order, so
+// the result is deterministic.
+#include <cuda_runtime.h>
+
+#include "engine.h"
+
+namespace chb {
+
+namespace {
+constexpr int DOT_THREADS = 256;
+
+__device__ double block_sum(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = DOT_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+__global__ void __launch_bounds__(DOT_THREADS) dot_blocks(const double* __restrict__ x, const double* __restrict__ y,
+                                                          const FrontDesc* __restrict__ fronts, int nsn,
+                                                          double* __restrict__ partial) {
+  __shared__ double sh[DOT_THREADS];
+  for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
+    const FrontDesc f = fronts[k];
+    const int64_t total = (int64_t)f.nj * f.nn;
+    double acc = 0.0;
+    for (int64_t idx = threadIdx.x; idx < total; idx += DOT_THREADS) {
+      const int r = (int)(idx % f.nj), c = (int)(idx / f.nj);
+      if (r < c) continue;
+      const double p = x[f.blk + idx] * y[f.blk + idx];
+      acc += (r == c) ? p : 2.0 * p;
+    }
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[k] = s;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(DOT_THREADS) dot_final(const double* __restrict__ partial, int n,
+                                                         double* __restrict__ out) {
+  __shared__ double sh[DOT_THREADS];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += DOT_THREADS) acc += partial[i];
+  const double s = block_sum(acc, sh);
+  if (threadIdx.x == 0) *out = s;
+}
+}  // namespace
+
+cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
+                       double* out, cudaStream_t stream) {
+  if (nsn > 0) {
+    int grid = nsn < 4096 ? nsn : 4096;
+    dot_blocks<<<grid, DOT_THREADS, 0, stream>>>(x, y, fronts, nsn, partial);
+  }
+  dot_final<<<1, DOT_THREADS, 0, stream>>>(partial, nsn, out);
+  return cudaGetLastError();
+}
+
+}  // namespace chb

@@ -683,6 +683,83 @@ __device__ void run_copy(const RunArgs& ra, const Task& t) {
   }
 }
 
+// ------------------------------------------------------- solve vectors
+// Vector operations of the triangular solve sweep (T_VEC, sub-operation
+// aux[0], nrhs = t.n right-hand sides).  Bp / x_k live at operand a or c
+// with leading dimension n; the per-front vector updates u_k (na x nrhs,
+// ld na) start at WS + b.off + vpos[k] * nrhs.
+__device__ void run_vec(const RunArgs& ra, const Task& t) {
+  const int mode = t.aux[0], nrhs = t.n;
+  if (mode == VEC_GATHER || mode == VEC_SCATTER) {
+    const int r0 = t.aux[1], r1 = t.aux[2];
+    double* __restrict__ Bp = ra.bases[t.c.base] + t.c.off;
+    const int ldp = t.c.ld;
+    double* __restrict__ Bu = ra.bases[B_RHS];
+    const int64_t ldb = ra.ldb;
+    const int rows = r1 - r0;
+    for (int base = 0; base < rows * nrhs; base += 4 * NTHREADS) {
+      double v[4];
+      int64_t src[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int i = r0 + idx % max(rows, 1), j = idx / max(rows, 1);
+        src[e] = (idx < rows * nrhs) ? __ldg(ra.perm + i) + (int64_t)j * ldb : -1;
+        if (mode == VEC_GATHER) v[e] = (src[e] >= 0) ? ra.alpha * __ldcg(Bu + src[e]) : 0.0;
+        else v[e] = (src[e] >= 0) ? __ldcg(Bp + i + (int64_t)j * ldp) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int i = r0 + idx % max(rows, 1), j = idx / max(rows, 1);
+        if (src[e] < 0) continue;
+        if (mode == VEC_GATHER) Bp[i + (int64_t)j * ldp] = v[e];
+        else Bu[src[e]] = v[e];
+      }
+    }
+    return;
+  }
+  double* __restrict__ WS = ra.bases[B_WS];
+  const int64_t vbase = t.b.off;
+  if (mode == VEC_ASM) {
+    const FrontDesc f = ra.fronts[t.aux[1]];
+    double* __restrict__ xk = ra.bases[t.a.base] + t.a.off;
+    const int ldx = t.a.ld;
+    double* __restrict__ uk = ra.bases[t.c.base] + t.c.off;
+    for (int idx = threadIdx.x; idx < f.na * nrhs; idx += NTHREADS) uk[idx] = 0.0;
+    __syncthreads();
+    for (int l = f.chend - 1; l >= f.chbeg; l--) {
+      const FrontDesc ch = ra.fronts[ra.chidx[l]];
+      const int Nc = ch.na;
+      const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+      const double* __restrict__ uc = WS + vbase + ch.vpos * nrhs;
+      for (int idx = threadIdx.x; idx < Nc * nrhs; idx += NTHREADS) {
+        const int i = idx % Nc, j = idx / Nc;
+        const int row = __ldg(r + i);
+        const double v = __ldcg(uc + idx);
+        if (row < f.nn) xk[row + (int64_t)j * ldx] += v;
+        else uk[(row - f.nn) + (int64_t)j * f.na] += v;
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  // VEC_EXTRACT for child aux1 of the front p described by operands a, c
+  const FrontDesc ch = ra.fronts[t.aux[1]];
+  const FrontDesc f = ra.fronts[ch.parent];
+  const double* __restrict__ xp = ra.bases[t.a.base] + t.a.off;
+  const int ldx = t.a.ld;
+  const double* __restrict__ up = ra.bases[t.c.base] + t.c.off;
+  const int Nc = ch.na;
+  const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+  double* __restrict__ uc = WS + vbase + ch.vpos * nrhs;
+  for (int idx = threadIdx.x; idx < Nc * nrhs; idx += NTHREADS) {
+    const int i = idx % Nc, j = idx / Nc;
+    const int row = __ldg(r + i);
+    uc[idx] = (row < f.nn) ? __ldcg(xp + row + (int64_t)j * ldx) : __ldcg(up + (row - f.nn) + (int64_t)j * f.na);
+  }
+}
+
 // ---------------------------------------------------------------- kernel
 __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   extern __shared__ double smem[];
@@ -734,6 +811,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_ASM: run_asm(ra, t); break;
       case T_EXTRACT: run_extract(ra, t); break;
       case T_COPY: run_copy(ra, t); break;
+      case T_VEC: run_vec(ra, t); break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;

@@ -92,8 +92,8 @@ struct FrontDesc {
   int32_t level;        // height in the supernodal tree
   int64_t blk;          // blkptr[k]
   int64_t upd;          // offset (doubles) of the update matrix in the workspace
-  int64_t scr;          // offset of per-front scratch in the workspace
-  int64_t scr2;         // second scratch offset
+  int64_t col0;         // snptr[k]: first (reordered) column of the supernode
+  int64_t vpos;         // sum of na over the preceding supernodes (vector updates)
 };
 
 // Device-side run description (passed by value to the persistent kernel).
@@ -109,7 +109,18 @@ struct RunArgs {
   const int32_t* relidx;
   const int32_t* chidx;
   int64_t spin_limit;     // polls before a wait gives up
+  const int64_t* perm;    // p (trsm gather/scatter)
+  int64_t ldb;            // leading dimension of the right-hand sides (trsm)
+  double alpha;           // scale applied by the trsm gather
   unsigned long long* trace;  // optional: 4 words per task (claim, start, end, sm | op << 32)
+};
+
+// Sub-operations of T_VEC (triangular solve sweep).
+enum VecOp : int {
+  VEC_GATHER = 0,   // Bp[i, :] = alpha * B[p[i], :] for i in [aux1, aux2)
+  VEC_SCATTER = 1,  // B[p[i], :] = Bp[i, :]
+  VEC_ASM = 2,      // front aux1: zero u_k, add the children's updates into x_k / u_k
+  VEC_EXTRACT = 3   // child aux1: u_c = [x_p; u_p](r_c)
 };
 
 // Error codes written to ctl[1].

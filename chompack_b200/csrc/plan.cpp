@@ -53,6 +53,8 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   switch (op) {
     case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
     case CHB_OP_PROJECTED_INVERSE: rc = build_projected_inverse(*plan, *prog); break;
+    case CHB_OP_LLT: rc = build_llt(*plan, *prog); break;
+    case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, flags != 0); break;
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;
@@ -75,7 +77,7 @@ Program* get_program(chb_plan* plan, int op, int64_t k, int flags) {
 }
 
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
-                cudaStream_t stream) {
+                cudaStream_t stream, int64_t run_ldb, double run_alpha) {
   WsLayout L = ws_layout(*prog);
   if (work_bytes < L.total || (L.total > 0 && !work))
     return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, L.total);
@@ -97,6 +99,9 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.chidx = plan->d_chidx;
   ra.spin_limit = 40000000LL;  // about 10 s of polling at the longest back-off
   ra.trace = (plan->trace && plan->trace_cap >= (int64_t)prog->tasks.size()) ? plan->trace : nullptr;
+  ra.perm = plan->d_perm;
+  ra.ldb = run_ldb;
+  ra.alpha = run_alpha;
   int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
   CUDA_TRY(engine_launch(ra, grid, stream));
   return 0;
@@ -132,7 +137,7 @@ extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, con
   }
   P->chidx.resize(chptr[nsn]);
   for (int64_t i = 0; i < chptr[nsn]; i++) P->chidx[i] = (int32_t)chidx[i];
-  int64_t upd = 0;
+  int64_t upd = 0, vpos = 0;
   for (int64_t k = 0; k < nsn; k++) {
     FrontDesc& f = P->fronts[k];
     std::memset(&f, 0, sizeof(f));
@@ -149,7 +154,10 @@ extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, con
     f.parent = (int32_t)snpar[k];
     f.blk = blkptr[k];
     f.upd = upd;
+    f.col0 = snptr[k];
+    f.vpos = vpos;
     upd += na * na;
+    vpos += na;
     P->snpar[k] = (int32_t)snpar[k];
     if (snpar[k] < k || snpar[k] >= nsn) return set_error(-9, "snpar must point to a later supernode or itself");
     if ((snpar[k] == k) != (na == 0)) return set_error(-10, "root / separator mismatch at %lld", (long long)k);
@@ -219,6 +227,10 @@ extern "C" int chb_workspace_size(const chb_plan* plan_c, int op, int64_t k, int
   clear_error();
   chb_plan* plan = const_cast<chb_plan*>(plan_c);
   if (!plan || !bytes) return set_error(-1, "null argument");
+  if (op == CHB_OP_DOT) {  // per-supernode partial sums
+    *bytes = 256 + (size_t)(plan->nsn + 1) * sizeof(double);
+    return 0;
+  }
   Program* p = build_host_program(plan, op, k, flags);
   if (!p) return -2;
   *bytes = ws_layout(*p).total;

@@ -77,14 +77,18 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags);
 
 // Launch a program.  bases: MAX_BASES device pointers (unused slots null).
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
-                cudaStream_t stream);
+                cudaStream_t stream, int64_t run_ldb = 0, double run_alpha = 1.0);
 
 // Device entry points implemented in engine.cu.
 size_t engine_smem_bytes();
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream);
 int engine_occupancy(int* blocks_per_sm);
+cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
+                       double* out, cudaStream_t stream);
 
 // Program builders (one per sweep), in build_*.cpp.
 int build_cholesky(const chb_plan& P, Program& prog);
 int build_projected_inverse(const chb_plan& P, Program& prog);
+int build_llt(const chb_plan& P, Program& prog);
+int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans);
 }  // namespace chb

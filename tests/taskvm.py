@@ -27,11 +27,12 @@ TASK = np.dtype({
 })
 FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4"), ("chbeg", "<i4"),
                   ("chend", "<i4"), ("parent", "<i4"), ("level", "<i4"), ("blk", "<i8"), ("upd", "<i8"),
-                  ("scr", "<i8"), ("scr2", "<i8")])
+                  ("col0", "<i8"), ("vpos", "<i8")])
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-B_X, B_WS = 0, 1
+T_VEC = 9
+B_X, B_WS, B_RHS = 0, 1, 4
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
                                    ctypes.POINTER(ctypes.c_int64)]
@@ -86,11 +87,14 @@ def _store(buf, o, m, n, val, lower, cdiag, beta):
 class VM(object):
     """Executes a Program on numpy buffers.  bases: dict slot -> 1-D array."""
 
-    def __init__(self, prog, bases, relidx, chidx):
+    def __init__(self, prog, bases, relidx, chidx, perm=None, ldb=0, alpha=1.0):
         self.p = prog
         self.bases = bases
         self.relidx = np.asarray(relidx)
         self.chidx = np.asarray(chidx)
+        self.perm = None if perm is None else np.asarray(perm)
+        self.ldb = ldb
+        self.alpha = alpha
         self.info = 0
 
     def run_task(self, t):
@@ -142,6 +146,8 @@ class VM(object):
             self._asm(t)
         elif op == T_EXTRACT:
             self._extract(t)
+        elif op == T_VEC:
+            self._vec(t)
         elif op == T_COPY:
             m, n = int(t["m"]), int(t["n"])
             fl = int(t["aux"][0])
@@ -187,6 +193,49 @@ class VM(object):
                     Pb[Pof + col * ldp + rows] += v
                 else:
                     Ub[Uof + (col - nn) * ldu + (rows - nn)] += v
+
+    def _vec(self, t):
+        mode, nrhs = int(t["aux"][0]), int(t["n"])
+        WS = self.bases[B_WS]
+        if mode in (0, 1):
+            r0, r1 = int(t["aux"][1]), int(t["aux"][2])
+            Bp, off, ld = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
+            Bu = self.bases[B_RHS]
+            for j in range(nrhs):
+                src = self.perm[r0:r1] + j * self.ldb
+                if mode == 0:
+                    Bp[off + np.arange(r0, r1) + j * ld] = self.alpha * Bu[src]
+                else:
+                    Bu[src] = Bp[off + np.arange(r0, r1) + j * ld]
+            return
+        vbase = int(t["b"]["off"])
+        xb, xo, ldx = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
+        ub, uo = self.bases[int(t["c"]["base"])], int(t["c"]["off"])
+        if mode == 2:
+            f = self.p.fronts[int(t["aux"][1])]
+            nn, na = int(f["nn"]), int(f["na"])
+            ub[uo: uo + na * nrhs] = 0.0
+            for l in range(int(f["chend"]) - 1, int(f["chbeg"]) - 1, -1):
+                ch = self.p.fronts[self.chidx[l]]
+                Nc = int(ch["na"])
+                r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+                uc = WS[vbase + int(ch["vpos"]) * nrhs: vbase + int(ch["vpos"]) * nrhs + Nc * nrhs].reshape((Nc, nrhs), order="F")
+                for j in range(nrhs):
+                    top = r < nn
+                    xb[xo + r[top] + j * ldx] += uc[top, j]
+                    ub[uo + (r[~top] - nn) + j * na] += uc[~top, j]
+            return
+        ch = self.p.fronts[int(t["aux"][1])]
+        f = self.p.fronts[int(ch["parent"])]
+        nn, na, Nc = int(f["nn"]), int(f["na"]), int(ch["na"])
+        r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+        base = vbase + int(ch["vpos"]) * nrhs
+        for j in range(nrhs):
+            top = r < nn
+            vals = np.empty(Nc)
+            vals[top] = xb[xo + r[top] + j * ldx]
+            vals[~top] = ub[uo + (r[~top] - nn) + j * na]
+            WS[base + j * Nc: base + (j + 1) * Nc] = vals
 
     def _extract(self, t):
         ch = self.p.fronts[int(t["aux"][0])]
