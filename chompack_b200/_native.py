@@ -70,9 +70,13 @@ program_info = _sig("chb_program_info", ctypes.c_int, [PPLAN, ctypes.c_int, i64,
 cholesky = _sig("chb_cholesky", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 projected_inverse = _sig("chb_projected_inverse", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 llt = _sig("chb_llt", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
+completion = _sig("chb_completion", ctypes.c_int, [PPLAN, vp, ctypes.c_int, vp, ctypes.c_size_t, vp])
+hessian = _sig("chb_hessian", ctypes.c_int, [PPLAN, vp, vp, ctypes.POINTER(vp), i64, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, vp, ctypes.c_size_t, vp])
 trsm = _sig("chb_trsm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
 dot = _sig("chb_dot", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
 set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 
 OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)
+HESSIAN_MAX_U = 59   # U matrices per chb_hessian call (base slots 5..63)

@@ -9,6 +9,8 @@ cspmatrix's CUDA float64 tensor, transformed in place.  Calls are
 synchronous like the reference's (they read the device status to raise
 ArithmeticError); the `*_async` variants in `chompack_b200.engine` skip that.
 """
+import ctypes
+
 import torch
 
 from . import _native as N
@@ -157,12 +159,66 @@ def dot(X, Y):
     return float(out.item())
 
 
-def _missing(name):
-    def f(*args, **kwargs):
-        raise NotImplementedError("%s is not available in this build" % name)
-    f.__name__ = name
-    return f
+def completion(X, factored_updates=True):
+    """Maximum-determinant positive definite completion (cbase.c:521-620):
+    on exit X holds, in place, the Cholesky factor L of the inverse of the
+    max-det positive definite completion of X (so L L^T has projected
+    inverse X); X.is_factor becomes True.  factored_updates selects the
+    update_factor form of the update matrices (the same L up to rounding)."""
+    if X.is_factor is not False:
+        raise ValueError("X must be a cspmatrix")
+    v = _values(X)
+    plan = X.symb.plan(v.device.index)
+    fu = 1 if factored_updates is True else 0
+    info = _run_and_status(plan, N.OP_COMPLETION,
+                           lambda ws, nb, s: N.completion(plan.handle, v.data_ptr(), fu, ws, nb, s), k=fu)
+    X.is_factor = True
+    if info:
+        raise ArithmeticError("completion failed")
 
 
-completion = _missing("completion")
-hessian = _missing("hessian")
+def hessian(L, Y, U, adj=False, inv=False, factored_updates=True):
+    """Hessian factors of the log-det barrier (cbase.c:675-857), applied in
+    place to U (a cspmatrix or a list of them, all on L's symbolic
+    factorisation):
+
+        adj=False, inv=False:  U := G(U)          adj=True,  inv=False: U := G^adj(U)
+        adj=False, inv=True:   U := G^{-1}(U)     adj=True,  inv=True:  U := (G^adj)^{-1}(U)
+        adj=None:              U := H(U) = G^adj(G(U))  (inv=True: the inverse)
+
+    L is the Cholesky factor, Y the projected inverse (L.symb's)."""
+    symb = L.symb
+    Us = U if isinstance(U, list) else [U]
+    if Y.symb is not symb or any(u.symb is not symb for u in Us):
+        raise ValueError("symbolic factorizations must be the same")
+    if L.is_factor is False:
+        raise ValueError("L must be a cspmatrix factor")
+    if Y.is_factor is True:
+        raise ValueError("Y must be a cspmatrix")
+    inv_i = 1 if inv is True else 0
+    if adj is True:
+        adj_i = 1
+    elif adj is None:
+        adj_i = inv_i
+    else:
+        adj_i = 0
+    fu = 1 if factored_updates is True else 0
+    lv = _values(L, "L")
+    yv = _values(Y, "Y")
+    uv = [_values(u, "U") for u in Us]
+    if not Us:
+        return
+    plan = symb.plan(lv.device.index)
+    passes = [adj_i, 1 ^ adj_i] if adj is None else [adj_i]
+    info = 0
+    for a in passes:
+        for c0 in range(0, len(uv), N.HESSIAN_MAX_U):
+            chunk = uv[c0:c0 + N.HESSIAN_MAX_U]
+            arr = (ctypes.c_void_p * len(chunk))(*[u.data_ptr() for u in chunk])
+            flags = a | inv_i << 1 | fu << 2
+            info |= _run_and_status(
+                plan, N.OP_HESSIAN,
+                lambda ws, nb, s: N.hessian(plan.handle, lv.data_ptr(), yv.data_ptr(), arr, len(chunk), a, inv_i,
+                                            fu, ws, nb, s), k=len(chunk), flags=flags)
+    if info:
+        raise ArithmeticError("hessian failed")

@@ -45,6 +45,26 @@ extern "C" int chb_llt(chb_plan* plan, double* blkval, void* work, size_t work_b
   return run_op(plan, CHB_OP_LLT, 0, 0, bases, 1, work, work_bytes, stream);
 }
 
+extern "C" int chb_completion(chb_plan* plan, double* blkval, int factored_updates, void* work, size_t work_bytes,
+                              void* stream) {
+  double* bases[1] = {blkval};
+  return run_op(plan, CHB_OP_COMPLETION, factored_updates ? 1 : 0, 0, bases, 1, work, work_bytes, stream);
+}
+
+extern "C" int chb_hessian(chb_plan* plan, const double* lblkval, const double* yblkval, double* const* ublkval,
+                           int64_t nu, int adj, int inv, int factored_updates, void* work, size_t work_bytes,
+                           void* stream) {
+  if (nu < 1 || nu > MAX_BASES - B_U0)
+    return set_error(-1, "hessian: between 1 and %d U matrices per call, %lld given", MAX_BASES - B_U0, (long long)nu);
+  if (!ublkval) return set_error(-1, "hessian: null U array");
+  double* bases[MAX_BASES] = {};
+  bases[B_L] = const_cast<double*>(lblkval);
+  bases[B_Y] = const_cast<double*>(yblkval);
+  for (int64_t u = 0; u < nu; u++) bases[B_U0 + u] = ublkval[u];
+  const int flags = (adj ? 1 : 0) | (inv ? 2 : 0) | (factored_updates ? 4 : 0);
+  return run_op(plan, CHB_OP_HESSIAN, nu, flags, bases, (int)(B_U0 + nu), work, work_bytes, stream);
+}
+
 extern "C" int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
                         int64_t ldB, void* work, size_t work_bytes, void* stream) {
   if (trans != 'N' && trans != 'T') return set_error(-1, "trans must be 'N' or 'T'");

@@ -580,7 +580,7 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
     const FrontDesc ch = ra.fronts[ra.chidx[l]];
     const int N = ch.na;
     const int32_t* __restrict__ r = ra.relidx + ch.relptr;
-    const double* __restrict__ Uc = ra.bases[B_WS] + ch.upd;
+    const double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
     // child columns with r[q] in [j0, j1): r is strictly increasing
     int lo = 0, hi = N;
     while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < j0) lo = mid + 1; else hi = mid; }
@@ -630,7 +630,7 @@ __device__ void run_extract(const RunArgs& ra, const Task& t) {
   const double* __restrict__ F21 = ra.bases[t.b.base] + t.b.off;
   const double* __restrict__ F22 = ra.bases[t.c.base] + t.c.off;
   const int ld11 = t.a.ld, ld21 = t.b.ld, ld22 = t.c.ld;
-  double* __restrict__ Uc = ra.bases[B_WS] + ch.upd;
+  double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
     const int col = __ldg(r + q);
@@ -657,8 +657,56 @@ __device__ void run_extract(const RunArgs& ra, const Task& t) {
 
 // Tile copy C = alpha * A (m x n).  aux[0] bit 0: copy only the lower
 // triangle (r >= c); bit 1: write zeros above the diagonal; bit 2: write
-// zeros everywhere (A is not read).
+// zeros everywhere (A is not read).  Bit 3: anti-transpose inside an
+// aux[1] x aux[1] matrix: operands a and c are the matrices' origins and the
+// tile has origin (aux[2], aux[3]) in C; C(i, j) = A(n-1-j, n-1-i) for the
+// lower entries i >= j (with J the order reversal, C = J A^T J).  Bit 4:
+// transpose, C(r, c) = A(c, r); bit 5 with it: only entries above the
+// diagonal of the tile (r < c), used to symmetrise a diagonal block.
 __device__ void run_copy(const RunArgs& ra, const Task& t) {
+  if (t.aux[0] & 16) {
+    const double* __restrict__ A = ra.bases[t.a.base] + t.a.off;
+    double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+    const int lda = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n;
+    const bool upper = (t.aux[0] & 32) != 0;
+    for (int base = 0; base < m * n; base += 8 * NTHREADS) {
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int r = idx % m, c = idx / m;
+        v[e] = (idx < m * n && (!upper || r < c)) ? __ldcg(A + (int64_t)r * lda + c) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int r = idx % m, c = idx / m;
+        if (idx < m * n && (!upper || r < c)) C[(int64_t)c * ldc + r] = t.alpha * v[e];
+      }
+    }
+    return;
+  }
+  if (t.aux[0] & 8) {
+    const double* __restrict__ A = ra.bases[t.a.base] + t.a.off;
+    double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+    const int lda = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n, nn = t.aux[1], i0 = t.aux[2], j0 = t.aux[3];
+    for (int base = 0; base < m * n; base += 8 * NTHREADS) {
+      double v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int gi = i0 + idx % m, gj = j0 + idx / m;
+        v[e] = (idx < m * n && gi >= gj) ? __ldcg(A + (int64_t)(nn - 1 - gi) * lda + (nn - 1 - gj)) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int idx = base + threadIdx.x + e * NTHREADS;
+        const int gi = i0 + idx % m, gj = j0 + idx / m;
+        if (idx < m * n && gi >= gj) C[(int64_t)gj * ldc + gi] = v[e];
+      }
+    }
+    return;
+  }
   const double* __restrict__ A = ra.bases[t.a.base] + t.a.off;
   double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
   const int lda = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n;
@@ -680,6 +728,149 @@ __device__ void run_copy(const RunArgs& ra, const Task& t) {
       if (r >= c || !lower) C[(int64_t)c * ldc + r] = alpha * v[e];
       else if (zup) C[(int64_t)c * ldc + r] = 0.0;
     }
+  }
+}
+
+// ------------------------------------------------------ update_factor
+__device__ __forceinline__ double block_reduce_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int w = 0; w < NTHREADS / 32; w++) s += red[w];
+  return s;
+}
+
+// Factored update of child c = aux[0] (update_factor.c:3-108): with the
+// parent's front F = [F11, F21^T; F21, L_k] where V_k = L_k^T L_k, computes
+// the lower-triangular U_c with U_c^T U_c = F[r, r] (r the child's relative
+// indices), by the reference's steps: U_c(:, :N1) = F[r, r[:N1]]; the
+// columns r[N1:] of L_k are reduced to lower-triangular form by Householder
+// reflections, last column first (LAPACK dlarfg/dlarfx conventions: beta =
+// -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta, v = x/(alpha -
+// beta)); L21 solves L22^T L21 = F[r[N1:], r[:N1]]; then U_c(:N1, :N1) is the
+// "reverse" Cholesky of F[r[:N1], r[:N1]] - L21^T L21.  One CTA; the
+// Householder scratch (na x N2) is at WS + (aux[1] | aux[2] << 32).
+// Operands: a = F11 (ld nj), b = F21 (row nn at offset 0, ld nj), c = L_k.
+__device__ void run_house(const RunArgs& ra, const Task& t, double* smem) {
+  const FrontDesc ch = ra.fronts[t.aux[0]];
+  const FrontDesc f = ra.fronts[ch.parent];
+  const int N = ch.na, nn = f.nn, na = f.na;
+  const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+  const double* __restrict__ F11 = ra.bases[t.a.base] + t.a.off;
+  const double* __restrict__ F21 = ra.bases[t.b.base] + t.b.off;
+  const double* __restrict__ F22 = ra.bases[t.c.base] + t.c.off;
+  const int ld11 = t.a.ld, ld21 = t.b.ld, ld22 = t.c.ld;
+  double* __restrict__ u = ra.bases[B_WS] + t.off2 + ch.upd;
+  const int64_t hoff = (int64_t)(uint32_t)t.aux[1] | ((int64_t)t.aux[2] << 32);
+  double* __restrict__ C = ra.bases[B_WS] + hoff;
+  double* red = smem;          // reduction scratch
+  double* sc = smem + 32;      // broadcast scalars
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // N1 = number of relative indices < nn (r is increasing)
+  int lo = 0, hi = N;
+  while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < nn) lo = mid + 1; else hi = mid; }
+  const int N1 = lo, N2 = N - N1;
+  // leading N1 columns: u(i, j) = F(r[i], r[j]), i >= j
+  for (int64_t idx = tid; idx < (int64_t)N * N1; idx += NTHREADS) {
+    const int i = (int)(idx % N), j = (int)(idx / N);
+    if (i < j) continue;
+    const int ri = __ldg(r + i), rj = __ldg(r + j);
+    u[(int64_t)j * N + i] = (ri < nn) ? __ldcg(F11 + (int64_t)rj * ld11 + ri) : __ldcg(F21 + (int64_t)rj * ld21 + (ri - nn));
+  }
+  if (N2 > 0) {
+    // C(:, j) = L_k(:, r[N1 + j] - nn), rows from the diagonal down
+    for (int64_t idx = tid; idx < (int64_t)na * N2; idx += NTHREADS) {
+      const int ii = (int)(idx % na), j = (int)(idx / na);
+      const int jj = __ldg(r + N1 + j) - nn;
+      if (ii >= jj) C[(int64_t)j * na + ii] = __ldcg(F22 + (int64_t)jj * ld22 + ii);
+    }
+    __syncthreads();
+    for (int j = 0; j < N2; j++) {
+      const int jj = __ldg(r + N - 1 - j) - nn;
+      const int ii = (na - jj) - (j + 1);  // entries to annihilate
+      if (ii == 0) continue;
+      const int col = N2 - 1 - j, prow = na - 1 - j, r0 = prow - ii;  // x = C[r0:prow, col]
+      double* cc = C + (int64_t)col * na;
+      double part = 0.0;
+      for (int q = r0 + tid; q < prow; q += NTHREADS) part += cc[q] * cc[q];
+      const double xnorm2 = block_reduce_sum(part, red);
+      const double alpha = cc[prow];
+      if (xnorm2 == 0.0) {  // tau = 0: the reflection is the identity
+        __syncthreads();
+        continue;
+      }
+      const double beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+      const double tau = (beta - alpha) / beta;
+      const double scal = 1.0 / (alpha - beta);
+      __syncthreads();
+      for (int q = r0 + tid; q < prow; q += NTHREADS) cc[q] *= scal;
+      if (tid == 0) cc[prow] = beta;
+      __syncthreads();
+      // H = I - tau v v^T with v = [x; 1] applied to columns 0..col-1, rows r0..prow
+      for (int q2 = warp; q2 < col; q2 += NTHREADS / 32) {
+        double* cq = C + (int64_t)q2 * na;
+        double w = 0.0;
+        for (int q = r0 + lane; q <= prow; q += 32) w += ((q == prow) ? 1.0 : cc[q]) * cq[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        w *= tau;
+        for (int q = r0 + lane; q <= prow; q += 32) cq[q] -= ((q == prow) ? 1.0 : cc[q]) * w;
+      }
+      __syncthreads();
+    }
+    // L22 = last N2 rows of C (lower) into u(N1:, N1:)
+    for (int64_t idx = tid; idx < (int64_t)N2 * N2; idx += NTHREADS) {
+      const int i = (int)(idx % N2), j = (int)(idx / N2);
+      if (i >= j) u[(int64_t)(N1 + j) * N + N1 + i] = C[(int64_t)j * na + (na - N2 + i)];
+    }
+    __syncthreads();
+    // L21: solve L22^T X = B, B = u(N1:, :N1) (backward substitution per column)
+    for (int j = tid; j < N1; j += NTHREADS) {
+      double* x = u + (int64_t)j * N + N1;
+      for (int i = N2 - 1; i >= 0; i--) {
+        double sacc = x[i];
+        for (int l = i + 1; l < N2; l++) sacc -= u[(int64_t)(N1 + i) * N + N1 + l] * x[l];
+        const double d = u[(int64_t)(N1 + i) * N + N1 + i];
+        if (d == 0.0) atomicCAS(&ra.ctl[2], 0, i + 1);
+        x[i] = sacc / (d == 0.0 ? 1.0 : d);
+      }
+    }
+    __syncthreads();
+    // u11 -= L21^T L21 (lower)
+    for (int64_t idx = tid; idx < (int64_t)N1 * N1; idx += NTHREADS) {
+      const int i = (int)(idx % N1), j = (int)(idx / N1);
+      if (i < j) continue;
+      double sacc = 0.0;
+      for (int l = 0; l < N2; l++) sacc += u[(int64_t)i * N + N1 + l] * u[(int64_t)j * N + N1 + l];
+      u[(int64_t)j * N + i] -= sacc;
+    }
+    __syncthreads();
+  } else {
+    __syncthreads();
+  }
+  // u11 = L11 with A = L11^T L11 (reverse Cholesky), bottom row first:
+  //   L(j,j) = sqrt(A(j,j)); L(j,i) = A(j,i)/L(j,j); A(i',i) -= L(j,i') L(j,i)
+  for (int j = N1 - 1; j >= 0; j--) {
+    const double d = u[(int64_t)j * N + j];
+    const bool bad = !(d > 0.0);
+    if (bad && tid == 0) atomicCAS(&ra.ctl[2], 0, j + 1);
+    const double piv = sqrt(bad ? 1.0 : d);
+    const double rp = 1.0 / piv;
+    __syncthreads();
+    for (int i = tid; i < j; i += NTHREADS) u[(int64_t)i * N + j] *= rp;  // row j, columns i < j
+    if (tid == 0) u[(int64_t)j * N + j] = piv;
+    __syncthreads();
+    for (int64_t idx = tid; idx < (int64_t)j * j; idx += NTHREADS) {
+      const int ip = (int)(idx % j), i = (int)(idx / j);  // (row ip, col i), ip >= i
+      if (ip < i) continue;
+      u[(int64_t)i * N + ip] -= u[(int64_t)ip * N + j] * u[(int64_t)i * N + j];
+    }
+    __syncthreads();
   }
 }
 
@@ -812,6 +1003,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_EXTRACT: run_extract(ra, t); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;
+      case T_HOUSE: run_house(ra, t, smem); break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;

@@ -81,6 +81,8 @@ struct Task {
   int32_t aux[4];   // op-specific integers (front id, column range, ...)
   double alpha, beta;
   Operand a, b, c;
+  int64_t off2;     // op-specific offset (base of the update-matrix region for
+                    // T_ASM / T_EXTRACT / T_HOUSE)
 };
 
 // Per-supernode description used by the gather/scatter tasks.

@@ -54,7 +54,9 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
     case CHB_OP_PROJECTED_INVERSE: rc = build_projected_inverse(*plan, *prog); break;
     case CHB_OP_LLT: rc = build_llt(*plan, *prog); break;
+    case CHB_OP_COMPLETION: rc = build_completion(*plan, *prog, k != 0); break;
     case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, flags != 0); break;
+    case CHB_OP_HESSIAN: rc = build_hessian(*plan, *prog, (int)k, flags); break;
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;

@@ -19,11 +19,11 @@ OPERAND = np.dtype([("off", "<i8"), ("ld", "<i4"), ("base", "u1"), ("mode", "u1"
                     ("diag", "<i4"), ("pad2", "<i4")])
 TASK = np.dtype({
     "names": ["op", "cmode", "nwait", "wait_off", "group", "m", "n", "k", "cdiag", "aux", "alpha", "beta",
-              "a", "b", "c"],
+              "a", "b", "c", "off2"],
     "formats": ["u1", "u1", "<u2", "<i4", "<i4", "<i4", "<i4", "<i4", "<i4", ("<i4", 4), "<f8", "<f8",
-                OPERAND, OPERAND, OPERAND],
-    "offsets": [0, 1, 2, 4, 8, 12, 16, 20, 24, 28, 48, 56, 64, 88, 112],
-    "itemsize": 136,
+                OPERAND, OPERAND, OPERAND, "<i8"],
+    "offsets": [0, 1, 2, 4, 8, 12, 16, 20, 24, 28, 48, 56, 64, 88, 112, 136],
+    "itemsize": 144,
 })
 FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4"), ("chbeg", "<i4"),
                   ("chend", "<i4"), ("parent", "<i4"), ("level", "<i4"), ("blk", "<i8"), ("upd", "<i8"),
@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_VEC = 9
+T_HOUSE, T_VEC = 8, 9
 B_X, B_WS, B_RHS = 0, 1, 4
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
@@ -148,6 +148,8 @@ class VM(object):
             self._extract(t)
         elif op == T_VEC:
             self._vec(t)
+        elif op == T_HOUSE:
+            self._house(t)
         elif op == T_COPY:
             m, n = int(t["m"]), int(t["n"])
             fl = int(t["aux"][0])
@@ -155,6 +157,21 @@ class VM(object):
             c = np.arange(n)[None, :]
             C = self.bases[int(t["c"]["base"])]
             cidx = int(t["c"]["off"]) + c * int(t["c"]["ld"]) + r
+            if fl & 16:  # transpose (optionally the strict upper part only)
+                A = self.bases[int(t["a"]["base"])]
+                src = int(t["a"]["off"]) + r * int(t["a"]["ld"]) + c
+                sel = (r < c) if (fl & 32) else np.ones((m, n), dtype=bool)
+                C[cidx[sel]] = float(t["alpha"]) * A[src[sel]]
+                return
+            if fl & 8:   # anti-transpose inside an nn x nn matrix
+                nn, i0, j0 = int(t["aux"][1]), int(t["aux"][2]), int(t["aux"][3])
+                A = self.bases[int(t["a"]["base"])]
+                gi, gj = i0 + r + 0 * c, j0 + c + 0 * r
+                low = gi >= gj
+                src = int(t["a"]["off"]) + (nn - 1 - gi) * int(t["a"]["ld"]) + (nn - 1 - gj)
+                dst = int(t["c"]["off"]) + gj * int(t["c"]["ld"]) + gi
+                C[dst[low]] = A[src[low]]
+                return
             if fl & 4:
                 C[cidx] = 0.0
             else:
@@ -182,7 +199,8 @@ class VM(object):
             ch = self.p.fronts[self.chidx[l]]
             Nc = int(ch["na"])
             r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
-            Uc = WS[int(ch["upd"]): int(ch["upd"]) + Nc * Nc].reshape((Nc, Nc), order="F")
+            o2 = int(t["off2"])
+            Uc = WS[o2 + int(ch["upd"]): o2 + int(ch["upd"]) + Nc * Nc].reshape((Nc, Nc), order="F")
             for q in range(Nc):
                 col = int(r[q])
                 if not (j0 <= col < j1):
@@ -237,6 +255,68 @@ class VM(object):
             vals[~top] = ub[uo + (r[~top] - nn) + j * na]
             WS[base + j * Nc: base + (j + 1) * Nc] = vals
 
+    def _house(self, t):
+        """update_factor (update_factor.c:3-108) with numpy."""
+        ch = self.p.fronts[int(t["aux"][0])]
+        f = self.p.fronts[int(ch["parent"])]
+        Nc, nn, na = int(ch["na"]), int(f["nn"]), int(f["na"])
+        r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+        A11 = (self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"]))
+        A21 = (self.bases[int(t["b"]["base"])], int(t["b"]["off"]), int(t["b"]["ld"]))
+        A22 = (self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
+
+        def F(i, j):   # j <= i, front coordinates
+            if j >= nn:
+                b, o, ld = A22
+                return b[o + (j - nn) * ld + (i - nn)]
+            if i >= nn:
+                b, o, ld = A21
+                return b[o + j * ld + (i - nn)]
+            b, o, ld = A11
+            return b[o + j * ld + i]
+        N1 = int(np.sum(r < nn))
+        N2 = Nc - N1
+        u = np.zeros((Nc, Nc))
+        for j in range(N1):
+            for i in range(j, Nc):
+                u[i, j] = F(r[i], r[j])
+        if N2 > 0:
+            C = np.zeros((na, N2))
+            for j in range(N2):
+                jj = r[N1 + j] - nn
+                for ii in range(jj, na):
+                    C[ii, j] = F(ii + nn, jj + nn)
+            for j in range(N2):
+                jj = r[Nc - 1 - j] - nn
+                ii = (na - jj) - (j + 1)
+                if ii == 0:
+                    continue
+                col, prow = N2 - 1 - j, na - 1 - j
+                r0 = prow - ii
+                x = C[r0:prow, col]
+                xn2 = float(np.dot(x, x))
+                alpha = C[prow, col]
+                if xn2 == 0.0:
+                    continue
+                beta = -np.copysign(np.sqrt(alpha * alpha + xn2), alpha)
+                tau = (beta - alpha) / beta
+                C[r0:prow, col] = x / (alpha - beta)
+                C[prow, col] = beta
+                v = np.concatenate([C[r0:prow, col], [1.0]])
+                blk = C[r0:prow + 1, :col]
+                C[r0:prow + 1, :col] = blk - tau * np.outer(v, v @ blk)
+            u[N1:, N1:] = np.tril(C[na - N2:, :])
+            L22 = u[N1:, N1:]
+            u[N1:, :N1] = np.linalg.solve(L22.T, u[N1:, :N1])
+            u[:N1, :N1] -= np.tril(u[N1:, :N1].T @ u[N1:, :N1])
+        A = np.tril(u[:N1, :N1]) + np.tril(u[:N1, :N1], -1).T
+        J = np.arange(N1)[::-1]
+        Lp = np.linalg.cholesky(A[np.ix_(J, J)])
+        u[:N1, :N1] = Lp.T[np.ix_(J, J)]
+        up = int(t["off2"]) + int(ch["upd"])
+        WS = self.bases[B_WS]
+        WS[up: up + Nc * Nc] = u.reshape(-1, order="F")
+
     def _extract(self, t):
         ch = self.p.fronts[int(t["aux"][0])]
         f = self.p.fronts[int(ch["parent"])]
@@ -247,7 +327,7 @@ class VM(object):
         Bb = (self.bases[int(t["b"]["base"])], int(t["b"]["off"]), int(t["b"]["ld"]))
         C = (self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
         WS = self.bases[B_WS]
-        up = int(ch["upd"])
+        up = int(t["off2"]) + int(ch["upd"])
         for q in range(q0, q1):
             col = int(r[q])
             for i in range(q, Nc):

@@ -1,0 +1,48 @@
+"""The C ABI library (CPU): it loads, exports every function that
+include/chompack_b200.h declares, and rejects inconsistent input with an
+error code and message rather than touching the device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from chompack_b200 import _native as N
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "chompack_b200.h")
+
+
+def test_every_declared_function_is_exported():
+    src = open(HEADER).read()
+    names = sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(chb_\w+)\s*\(", src, re.M)))
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(N.lib, n)]
+    assert not missing, missing
+
+
+def test_plan_rejects_inconsistent_blkptr():
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    A = grids.grid2d(8, seed=0)
+    s = cp.symbolic(A, p=cp.amd.order(A))
+    arrs = [np.ascontiguousarray(getattr(s, a), dtype=np.int64) for a in
+            ("snptr", "snpar", "relptr", "relidx", "chptr", "chidx", "blkptr", "snode", "p")]
+    arrs[6] = arrs[6].copy()
+    arrs[6][-1] += 1
+    h = N.PPLAN()
+    rc = N.plan_create(s.n, s.Nsn, *[N.ptr(a) for a in arrs], -1, ctypes.byref(h))
+    assert rc < 0
+    assert b"blkptr" in N.last_error()
+
+
+def test_host_only_plan_programs_and_workspace():
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    from chompack_b200.plan import Plan
+    A = grids.grid3d(8, seed=0)
+    s = cp.symbolic(A, p=cp.amd.order(A), merge_function=cp.merge_size_fill(16, 16))
+    pl = Plan(s, device=-1)
+    for op in (N.OP_CHOLESKY, N.OP_PROJECTED_INVERSE, N.OP_LLT):
+        info = pl.program_info(op)
+        assert info["tasks"] > 0 and info["ws_bytes"] >= 256 + 8 * info["upd_doubles"]
+    assert pl.workspace_bytes(N.OP_DOT) >= 8 * s.Nsn
