@@ -42,7 +42,9 @@ def sweep_flops(symb):
     chol = nn ** 3 / 3 + 2 * nn ** 2 * na + nn * na ** 2
     pinv = nn ** 3 / 3 + nn ** 3 + 2 * na ** 2 * nn + 2 * nn ** 2 * na
     llt = na * nn ** 2 + nn * nj ** 2
-    return {"cholesky": float(chol.sum()), "projected_inverse": float(pinv.sum()), "llt": float(llt.sum())}
+    comp = na ** 3 / 3 + 2 * na ** 2 * nn + nn ** 2 * na + 2 * nn ** 3 / 3
+    return {"cholesky": float(chol.sum()), "projected_inverse": float(pinv.sum()), "llt": float(llt.sum()),
+            "completion": float(comp.sum())}
 
 
 def build_problem(side=40, merge=(32, 32), seed=0):
@@ -54,53 +56,93 @@ def build_problem(side=40, merge=(32, 32), seed=0):
 
 
 class ClockSampler(object):
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """SM clock and clock-event-reason sampling during the timed region, by
+    NVML polling from a thread (every 2 ms; read-only queries).  The samples
+    are also written to gpurun_out/clocks_bench_<pid>.csv."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event-reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index):
-        self.index = index
-        self.proc = None
+    def __init__(self, dev):
+        self.dev = dev
+        self.thread = None
+        self.samples = []
         self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
 
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = getattr(torch.cuda.get_device_properties(self.dev), "uuid", None)
+        if uuid is not None:
+            u = str(uuid)
+            try:
+                return pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+            except Exception:
+                pass
+        return pynvml.nvmlDeviceGetHandleByIndex(self.dev.index or 0)
+
     def start(self):
+        import threading
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml
+            self.nv = pynvml
+            self.h = self._handle()
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            self.h = None
+            return
+        self.stop_flag = threading.Event()
+
+        def run():
+            nv = self.nv
+            while not self.stop_flag.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                    self.samples.append((time.time(), float(sm), int(rs), pw))
+                except Exception:
+                    pass
+                time.sleep(0.002)
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if not self.proc:
+        if self.thread is None:
             return None
-        self.proc.terminate()
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        if not self.samples:
+            return None
         try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.f.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            with open(self.path, "w") as f:
+                f.write("time,sm_mhz,reasons_mask,power_w\n")
+                for t, sm, rs, pw in self.samples:
+                    f.write("%.4f,%.0f,0x%x,%.1f\n" % (t, sm, rs, pw))
+        except OSError:
+            pass
+        reasons = set()
+        for _, _, rs, _ in self.samples:
+            for bit, nm in self.REASONS.items():
+                if rs & bit:
                     reasons.add(nm)
-        if not sm:
-            return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [x[1] for x in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": self.max_mhz, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": round(max(x[3] for x in self.samples), 1)}
+
+
+def profiled_traffic(name="engine_kernel_grid3d40.md"):
+    """DRAM bytes (read + write) per launch from the committed ncu summary."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return {k: int(v) for k, v in (kv.split("=") for kv in line.split(":", 1)[1].split())}
+    except OSError:
+        pass
+    return {}
 
 
 def fp64_peak_tflops(dev):
@@ -253,7 +295,7 @@ def main():
     if info != 0:
         raise RuntimeError("sweep status %d (%s)" % (info, N.last_error().decode()))
 
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(dev)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
@@ -276,6 +318,38 @@ def main():
         elapsed = float(tt[0])
         kern = {o: float(tt[1 + i]) for i, o in enumerate(ops)}
     value = step_flops * args.steps * world / elapsed / 1e9
+
+    # the other drop-in sweeps of the workload, timed alone after the step
+    # loop (not part of the step): completion of the projected inverse the
+    # step produced (both update modes) and llt of the factor
+    other = {}
+    Yw = Xw.clone()
+    Lw = X0.blkval.clone()
+    launch["cholesky"](plan.handle, Lw.data_ptr(), ws, nbytes, sp)
+    Cw = torch.empty_like(Yw)
+    reps = max(3, min(args.steps, 10))
+    for name, op, k, src, call in (
+            ("completion", N.OP_COMPLETION, 1, Yw, lambda w, nb: N.completion(plan.handle, Cw.data_ptr(), 1, w, nb, sp)),
+            ("completion_unfactored", N.OP_COMPLETION, 0, Yw,
+             lambda w, nb: N.completion(plan.handle, Cw.data_ptr(), 0, w, nb, sp)),
+            ("llt", N.OP_LLT, 0, Lw, lambda w, nb: N.llt(plan.handle, Cw.data_ptr(), w, nb, sp))):
+        w2, nb2 = plan.workspace(op, k)
+        ts = []
+        for it in range(reps + 1):
+            Cw.copy_(src)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if call(w2, nb2) < 0:
+                raise RuntimeError(N.last_error().decode())
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize(dev)
+        if N.info(plan.handle, w2, sp) != 0:
+            raise RuntimeError("%s status %s" % (name, N.last_error().decode()))
+        ms = float(np.median([a.elapsed_time(b) for a, b in ts[1:]]))
+        fkey = "completion" if name.startswith("completion") else name
+        other[name] = {"ms": round(ms, 4), "gflops": round(fl[fkey] / ms / 1e6, 3)}
 
     # end-to-end through the public API with host buffers
     e2e = None
@@ -300,6 +374,8 @@ def main():
 
     if rank == 0:
         peak = fp64_peak_tflops(dev)
+        na = np.diff(np.asarray(s.relptr)).astype(np.float64)
+        alg_bytes = int(16 * int(s.blkptr[-1]) + np.sum(16 * na * (na + 1) / 2))
         achieved = fl["cholesky"] / kern["cholesky"] / 1e12
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -310,11 +386,16 @@ def main():
                        "parallelism": "replicas x%d" % world},
             "gpu_launches": args.steps * len(ops),
             "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
-                         "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                         "traffic": profiled_traffic().get("cholesky"),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture "
+                                           "(profiles/engine_kernel_grid3d40.md)",
+                         "algorithmic_bytes": alg_bytes,
                          "kernel": "chb::engine_kernel (cholesky)",
                          "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; MEASURED_PEAKS.json "
                                         "lists bf16 and HBM only)"},
             "kernel_ms": {o: round(kern[o] * 1e3, 4) for o in ops},
+            "other_sweeps": other,
         }
         if clocks:
             out["clocks"] = clocks

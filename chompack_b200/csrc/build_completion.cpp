@@ -1,5 +1,6 @@
 // Task program of the maximum-determinant positive definite completion
 // (reference: completion.c:3-120, update_factor.c:3-108), reverse postorder.
+// The factored updates are built by stf_update_factor (stf.h).
 //
 // Input: Y = P(S^{-1}) in blkval; output: the factor L of S (in place).
 // Per supernode k, with P11 = blk(0:nn, 0:nn), P21 = blk(nn:nj, 0:nn) and
@@ -28,10 +29,10 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
   Stf S(B);
 
   // workspace: update matrices, then per front: Minv of V (na x 64), R and
-  // L'^{-1} (nn x nn each), Minv of R (nn x 64), and per child the
-  // Householder scratch of update_factor (na_parent x na_child)
+  // L'^{-1} (nn x nn each), Minv of R (nn x 64); then the scratch of the
+  // factored updates (handed out as they are built)
   int64_t ws = P.upd_total;
-  std::vector<int64_t> oMV(N), oR(N), oM(N), oMR(N), oH(N, 0);
+  std::vector<int64_t> oMV(N), oR(N), oM(N), oMR(N);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     oMV[k] = ws;
@@ -43,14 +44,11 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
     oMR[k] = ws;
     ws += (int64_t)f.nn * T;
   }
-  for (int64_t k = 0; k < N; k++) {
-    const FrontDesc& f = P.fronts[k];
-    if (f.parent != (int)k && factored) {
-      oH[k] = ws;
-      ws += (int64_t)P.fronts[f.parent].na * f.na + P.fronts[f.parent].na;
-    }
-  }
-  prog.ws_doubles = ws;
+  auto alloc = [&ws](int64_t n) {
+    const int64_t o = ws;
+    ws += n;
+    return o;
+  };
 
   // update matrices are tracked as matrices of their own
   std::vector<Mat> V(N);
@@ -79,30 +77,23 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
     for (int l = f.chbeg; l < f.chend; l++) {
       const int c = P.chidx[l];
       const int Nc = P.fronts[c].na;
+      if (factored) {
+        const int rc = stf_update_factor(S, kg, P, c, P11, P21, V[k], V[c], 0, alloc);
+        if (rc) return rc;
+        continue;
+      }
       std::vector<Stf::Acc> acc = fread;
       Stf::all(acc, V[c], true, true);
-      if (factored) {
-        Task t = make_task(T_HOUSE);
+      const int CH = 16;
+      for (int q0 = 0; q0 < Nc; q0 += CH) {
+        Task t = make_task(T_EXTRACT);
         t.aux[0] = c;
-        t.aux[1] = (int32_t)(uint32_t)(oH[c] & 0xffffffffLL);
-        t.aux[2] = (int32_t)(oH[c] >> 32);
+        t.aux[1] = q0;
+        t.aux[2] = std::min(Nc, q0 + CH);
         t.a = opnd(B_X, f.blk, nj);
         t.b = opnd(B_X, f.blk + nn, nj);
         t.c = opnd(B_WS, f.upd, std::max(na, 1));
-        const double est = 5.0 + (double)na * Nc * std::min(Nc, na) / 2e4;
-        S.submit(t, kg(0, c, 0), acc, -1, est);
-      } else {
-        const int CH = 16;
-        for (int q0 = 0; q0 < Nc; q0 += CH) {
-          Task t = make_task(T_EXTRACT);
-          t.aux[0] = c;
-          t.aux[1] = q0;
-          t.aux[2] = std::min(Nc, q0 + CH);
-          t.a = opnd(B_X, f.blk, nj);
-          t.b = opnd(B_X, f.blk + nn, nj);
-          t.c = opnd(B_WS, f.upd, std::max(na, 1));
-          S.submit(t, kg(0, c, q0), acc, -1, 3.0 + (double)(Nc - q0) * CH / 2000.0);
-        }
+        S.submit(t, kg(0, c, q0), acc, -1, 3.0 + (double)(Nc - q0) * CH / 2000.0);
       }
     }
     if (na > 0) {
@@ -130,34 +121,12 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
         }
     }
     // P11 := inv(R), P11 = R^T R: R = anti-transpose(P11) -> Cholesky -> inverse -> anti-transpose
-    auto antitr = [&](const Mat& src, const Mat& dst) {
-      kg.step++;
-      for (int j = 0; j < dst.ntc(); j++)
-        for (int i = j; i < dst.ntr(); i++) {
-          Task t = make_task(T_COPY);
-          t.m = dst.th(i);
-          t.n = dst.tw(j);
-          t.a = opnd(src.base, src.off, src.ld);
-          t.c = opnd(dst.base, dst.off, dst.ld);
-          t.aux[0] = 8 | 1;  // anti-transpose, lower part
-          t.aux[1] = nn;
-          t.aux[2] = i * T;
-          t.aux[3] = j * T;
-          // dst rows iT.. come from src columns nn-1-r, dst columns jT.. from src rows
-          const int c_hi = nn - 1 - i * T, c_lo = nn - i * T - dst.th(i);
-          const int r_hi = nn - 1 - j * T, r_lo = nn - j * T - dst.tw(j);
-          std::vector<Stf::Acc> acc{Stf::W(dst, i, j)};
-          for (int sj = c_lo / T; sj <= c_hi / T; sj++)
-            for (int si = r_lo / T; si <= r_hi / T; si++)
-              if (si >= sj) acc.push_back(Stf::R(src, si, sj));
-          S.submit(t, kg(i, j, 0), acc);
-        }
-    };
-    antitr(P11, R);
+    stf_antitranspose(S, kg, P11, R, nn);
     stf_potrf(S, kg, R, MR);
     stf_tri_inverse(S, kg, R, MR, M);
-    antitr(M, P11);
+    stf_antitranspose(S, kg, M, P11, nn);
   }
+  prog.ws_doubles = ws;
   return B.finish(prog, P.grid > 0 ? P.grid : 296);
 }
 

@@ -133,7 +133,8 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
 
   // workspace: V (update matrices of _scale) | per-U update matrices |
   // per front: diag inverses of L_kk (nn x 64), L_kk^{-1} (nn x nn), diag
-  // inverses of the front update (na x 64) | Householder scratch per child
+  // inverses of the front update (na x 64) | scratch of the factored updates
+  // (handed out as they are built)
   int64_t ws = 0;
   const int64_t oV = ws;
   ws += P.upd_total;
@@ -142,7 +143,7 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
     oW[u] = ws;
     ws += P.upd_total;
   }
-  std::vector<int64_t> oML(N), oMF(N), oMV(N), oH(N, 0);
+  std::vector<int64_t> oML(N), oMF(N), oMV(N);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     oML[k] = ws;
@@ -152,14 +153,11 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
     oMV[k] = ws;
     ws += (int64_t)f.na * T;
   }
-  for (int64_t k = 0; k < N; k++) {
-    const FrontDesc& f = P.fronts[k];
-    if (f.parent != (int)k && factored) {
-      oH[k] = ws;
-      ws += (int64_t)P.fronts[f.parent].na * f.na + P.fronts[f.parent].na;
-    }
-  }
-  prog.ws_doubles = ws;
+  auto alloc = [&ws](int64_t n) {
+    const int64_t o = ws;
+    ws += n;
+    return o;
+  };
 
   // tracked matrices
   std::vector<Mat> L11(N), L21(N), Y11(N), Y21(N), V(N), ML(N), MF(N), MV(N);
@@ -318,6 +316,7 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
   };
 
   // ----------------------------------------------------------- _scale
+  int err = 0;
   auto scale = [&]() {
     phase++;
     const bool tr1 = !adj;                     // op1 = T when !adj
@@ -330,24 +329,12 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
       // children's updates out of Y's front
       if (factored) {
         kg.step++;
-        std::vector<Stf::Acc> rd;
-        Stf::all(rd, Y11[k], false, true);
-        Stf::all(rd, Y21[k], false);
-        if (na > 0) Stf::all(rd, V[k], false, true);
         for (int l = f.chbeg; l < f.chend; l++) {
-          const int c = P.chidx[l];
-          const int Nc = P.fronts[c].na;
-          std::vector<Stf::Acc> acc = rd;
-          Stf::all(acc, V[c], true, true);
-          Task t = make_task(T_HOUSE);
-          t.aux[0] = c;
-          t.aux[1] = (int32_t)(uint32_t)(oH[c] & 0xffffffffLL);
-          t.aux[2] = (int32_t)(oH[c] >> 32);
-          t.a = opnd(B_Y, f.blk, nj);
-          t.b = opnd(B_Y, f.blk + nn, nj);
-          t.c = opnd(B_WS, oV + f.upd, std::max(na, 1));
-          t.off2 = oV;
-          S.submit(t, kg(0, c, 0), acc, -1, 5.0 + (double)na * Nc * std::min(Nc, na) / 2e4);
+          const int rc = stf_update_factor(S, kg, P, P.chidx[l], Y11[k], Y21[k], V[k], V[P.chidx[l]], oV, alloc);
+          if (rc) {
+            err = rc;
+            return;
+          }
         }
       } else {
         extract(kg, k, Y11[k], Y21[k], V[k], V, oV);
@@ -407,6 +394,8 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
   if (adj) m2t();
   else y2k();
   if (adj == inv) scale();
+  if (err) return err;
+  prog.ws_doubles = ws;
   return B.finish(prog, P.grid > 0 ? P.grid : 296);
 }
 

@@ -745,132 +745,157 @@ __device__ __forceinline__ double block_reduce_sum(double v, double* red) {
   return s;
 }
 
-// Factored update of child c = aux[0] (update_factor.c:3-108): with the
-// parent's front F = [F11, F21^T; F21, L_k] where V_k = L_k^T L_k, computes
-// the lower-triangular U_c with U_c^T U_c = F[r, r] (r the child's relative
-// indices), by the reference's steps: U_c(:, :N1) = F[r, r[:N1]]; the
-// columns r[N1:] of L_k are reduced to lower-triangular form by Householder
-// reflections, last column first (LAPACK dlarfg/dlarfx conventions: beta =
-// -sign(alpha) ||(alpha, x)||, tau = (beta - alpha)/beta, v = x/(alpha -
-// beta)); L21 solves L22^T L21 = F[r[N1:], r[:N1]]; then U_c(:N1, :N1) is the
-// "reverse" Cholesky of F[r[:N1], r[:N1]] - L21^T L21.  One CTA; the
-// Householder scratch (na x N2) is at WS + (aux[1] | aux[2] << 32).
-// Operands: a = F11 (ld nj), b = F21 (row nn at offset 0, ld nj), c = L_k.
-__device__ void run_house(const RunArgs& ra, const Task& t, double* smem) {
+// Blocked Householder QL of a factored update (update_factor.c:29-47).
+// For child c = aux[0] of front k, with V_k = L_k^T L_k (L_k lower, the
+// parent's update block, operand a of QL_GATHER) and the child's relative
+// indices r split as r[:N1] < nn <= r[N1:], the N2 columns
+// C(:, j) = L_k(:, jj_j), jj_j = r[N1 + j] - nn, are reduced to [0; L22] by
+// reflections applied last column first.  The reflection of column j acts on
+// rows [jj_j, prow_j], prow_j = na - N2 + j, with LAPACK's dlarfg/dlarfx
+// conventions: alpha = C(prow_j, j), x = C(jj_j:prow_j, j),
+// beta = -sign(alpha) * hypot(alpha, ||x||), tau = (beta - alpha) / beta,
+// v = [x / (alpha - beta); 1]; tau = 0 when x is empty or zero.
+//
+// A QL_PANEL task factors columns [c0, c1) inside shared memory (rows
+// [row0, row1] = [jj_c0, prow_{c1-1}], the rows its reflections touch),
+// applying each reflection to the panel's remaining columns only, and
+// writes, for the columns to its left (updated by MROW/GEMM tasks):
+//   W' (operand b): column c0 + i = reflector i, i = c1 - 1 - j (the order
+//     they are applied), explicit over rows [row0, row1];
+//   T  (operand c, nb x nb lower, ld c.ld): H_{c0} ... H_{c1-1} = I - W' T W'^T
+//     (LAPACK dlarft 'B','C': T(i,i) = tau_i,
+//      T(i+1:, i) = -tau_i T(i+1:, i+1:) W'(:, i+1:)^T w'_i).
+__device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
   const FrontDesc ch = ra.fronts[t.aux[0]];
   const FrontDesc f = ra.fronts[ch.parent];
   const int N = ch.na, nn = f.nn, na = f.na;
   const int32_t* __restrict__ r = ra.relidx + ch.relptr;
-  const double* __restrict__ F11 = ra.bases[t.a.base] + t.a.off;
-  const double* __restrict__ F21 = ra.bases[t.b.base] + t.b.off;
-  const double* __restrict__ F22 = ra.bases[t.c.base] + t.c.off;
-  const int ld11 = t.a.ld, ld21 = t.b.ld, ld22 = t.c.ld;
-  double* __restrict__ u = ra.bases[B_WS] + t.off2 + ch.upd;
-  const int64_t hoff = (int64_t)(uint32_t)t.aux[1] | ((int64_t)t.aux[2] << 32);
-  double* __restrict__ C = ra.bases[B_WS] + hoff;
-  double* red = smem;          // reduction scratch
-  double* sc = smem + 32;      // broadcast scalars
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // N1 = number of relative indices < nn (r is increasing)
   int lo = 0, hi = N;
   while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < nn) lo = mid + 1; else hi = mid; }
   const int N1 = lo, N2 = N - N1;
-  // leading N1 columns: u(i, j) = F(r[i], r[j]), i >= j
-  for (int64_t idx = tid; idx < (int64_t)N * N1; idx += NTHREADS) {
-    const int i = (int)(idx % N), j = (int)(idx / N);
-    if (i < j) continue;
-    const int ri = __ldg(r + i), rj = __ldg(r + j);
-    u[(int64_t)j * N + i] = (ri < nn) ? __ldcg(F11 + (int64_t)rj * ld11 + ri) : __ldcg(F21 + (int64_t)rj * ld21 + (ri - nn));
-  }
-  if (N2 > 0) {
-    // C(:, j) = L_k(:, r[N1 + j] - nn), rows from the diagonal down
-    for (int64_t idx = tid; idx < (int64_t)na * N2; idx += NTHREADS) {
-      const int ii = (int)(idx % na), j = (int)(idx / na);
+  const int c0 = t.aux[1], c1 = t.aux[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (t.aux[3] == QL_GATHER) {
+    const double* __restrict__ Lk = ra.bases[t.a.base] + t.a.off;
+    double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+    const int ldl = t.a.ld, ldc = t.c.ld;
+    for (int j = c0; j < c1; j++) {
       const int jj = __ldg(r + N1 + j) - nn;
-      if (ii >= jj) C[(int64_t)j * na + ii] = __ldcg(F22 + (int64_t)jj * ld22 + ii);
+      for (int i = tid; i < na; i += NTHREADS)
+        C[(int64_t)j * ldc + i] = (i >= jj) ? __ldcg(Lk + (int64_t)jj * ldl + i) : 0.0;
     }
-    __syncthreads();
-    for (int j = 0; j < N2; j++) {
-      const int jj = __ldg(r + N - 1 - j) - nn;
-      const int ii = (na - jj) - (j + 1);  // entries to annihilate
-      if (ii == 0) continue;
-      const int col = N2 - 1 - j, prow = na - 1 - j, r0 = prow - ii;  // x = C[r0:prow, col]
-      double* cc = C + (int64_t)col * na;
+    return;
+  }
+  double* __restrict__ C = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ W = ra.bases[t.b.base] + t.b.off;
+  double* __restrict__ Tg = ra.bases[t.c.base] + t.c.off;
+  const int ldc = t.a.ld, ldw = t.b.ld, ldt = t.c.ld;
+  const int nb = c1 - c0;
+  const int row0 = __ldg(r + N1 + c0) - nn, row1 = na - N2 + c1 - 1;
+  const int h = row1 - row0 + 1;
+  if (nb <= 0 || h <= 0 || ql_panel_doubles(h, nb) > ra.smem_doubles) {
+    if (tid == 0) atomicCAS(&ra.ctl[1], DE_NONE, DE_BAD_TASK);
+    return;
+  }
+  double* P = smem;                  // panel, column-major, ld h
+  double* G = smem + h * nb;         // nb x nb, ld nb (after the panel is out)
+  double* red = G + nb * nb;         // reduction scratch (32)
+  double* taus = red + 32;           // nb <= 64 (tau of reflector i)
+  int* lr0s = reinterpret_cast<int*>(taus + 64);   // 2 x 64 ints: support of reflector i
+  // load the panel
+  for (int idx = tid; idx < h * nb; idx += NTHREADS) {
+    const int q = idx % h, pc = idx / h;
+    P[idx] = __ldcg(C + (int64_t)(c0 + pc) * ldc + row0 + q);
+  }
+  __syncthreads();
+  for (int i = 0; i < nb; i++) {
+    const int col = c1 - 1 - i, pc = col - c0;
+    const int lr0 = __ldg(r + N1 + col) - nn - row0;   // first row of x (local)
+    const int lp = na - N2 + col - row0;               // pivot row (local)
+    double* pv = P + pc * h;
+    double tau = 0.0;
+    if (lp > lr0) {
       double part = 0.0;
-      for (int q = r0 + tid; q < prow; q += NTHREADS) part += cc[q] * cc[q];
-      const double xnorm2 = block_reduce_sum(part, red);
-      const double alpha = cc[prow];
-      if (xnorm2 == 0.0) {  // tau = 0: the reflection is the identity
+      for (int q = lr0 + tid; q < lp; q += NTHREADS) part += pv[q] * pv[q];
+      const double xn2 = block_reduce_sum(part, red);
+      if (xn2 != 0.0) {
+        const double alpha = pv[lp];
+        // dlapy2(alpha, ||x||)
+        const double xa = fabs(alpha), xb = sqrt(xn2);
+        const double w = fmax(xa, xb), z = fmin(xa, xb);
+        const double nrm = (z == 0.0) ? w : w * sqrt(1.0 + (z / w) * (z / w));
+        const double beta = -copysign(nrm, alpha);
+        tau = (beta - alpha) / beta;
+        const double scal = 1.0 / (alpha - beta);
+        __syncthreads();  // everyone has read pv[lp] and the norm
+        for (int q = lr0 + tid; q < lp; q += NTHREADS) pv[q] *= scal;
         __syncthreads();
-        continue;
-      }
-      const double beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
-      const double tau = (beta - alpha) / beta;
-      const double scal = 1.0 / (alpha - beta);
-      __syncthreads();
-      for (int q = r0 + tid; q < prow; q += NTHREADS) cc[q] *= scal;
-      if (tid == 0) cc[prow] = beta;
-      __syncthreads();
-      // H = I - tau v v^T with v = [x; 1] applied to columns 0..col-1, rows r0..prow
-      for (int q2 = warp; q2 < col; q2 += NTHREADS / 32) {
-        double* cq = C + (int64_t)q2 * na;
-        double w = 0.0;
-        for (int q = r0 + lane; q <= prow; q += 32) w += ((q == prow) ? 1.0 : cc[q]) * cq[q];
+        // H = I - tau v v^T on the panel columns to the left, rows [lr0, lp]
+        for (int q2 = warp; q2 < pc; q2 += NTHREADS / 32) {
+          double* cq = P + q2 * h;
+          double s = 0.0;
+          for (int q = lr0 + lane; q < lp; q += 32) s += pv[q] * cq[q];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        w *= tau;
-        for (int q = r0 + lane; q <= prow; q += 32) cq[q] -= ((q == prow) ? 1.0 : cc[q]) * w;
-      }
-      __syncthreads();
-    }
-    // L22 = last N2 rows of C (lower) into u(N1:, N1:)
-    for (int64_t idx = tid; idx < (int64_t)N2 * N2; idx += NTHREADS) {
-      const int i = (int)(idx % N2), j = (int)(idx / N2);
-      if (i >= j) u[(int64_t)(N1 + j) * N + N1 + i] = C[(int64_t)j * na + (na - N2 + i)];
-    }
-    __syncthreads();
-    // L21: solve L22^T X = B, B = u(N1:, :N1) (backward substitution per column)
-    for (int j = tid; j < N1; j += NTHREADS) {
-      double* x = u + (int64_t)j * N + N1;
-      for (int i = N2 - 1; i >= 0; i--) {
-        double sacc = x[i];
-        for (int l = i + 1; l < N2; l++) sacc -= u[(int64_t)(N1 + i) * N + N1 + l] * x[l];
-        const double d = u[(int64_t)(N1 + i) * N + N1 + i];
-        if (d == 0.0) atomicCAS(&ra.ctl[2], 0, i + 1);
-        x[i] = sacc / (d == 0.0 ? 1.0 : d);
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          s = tau * (s + cq[lp]);
+          for (int q = lr0 + lane; q < lp; q += 32) cq[q] -= pv[q] * s;
+          if (lane == 0) cq[lp] -= s;
+        }
+        if (tid == 0) pv[lp] = beta;
       }
     }
-    __syncthreads();
-    // u11 -= L21^T L21 (lower)
-    for (int64_t idx = tid; idx < (int64_t)N1 * N1; idx += NTHREADS) {
-      const int i = (int)(idx % N1), j = (int)(idx / N1);
-      if (i < j) continue;
-      double sacc = 0.0;
-      for (int l = 0; l < N2; l++) sacc += u[(int64_t)i * N + N1 + l] * u[(int64_t)j * N + N1 + l];
-      u[(int64_t)j * N + i] -= sacc;
+    if (tid == 0) {
+      taus[i] = tau;
+      lr0s[i] = lr0;
+      lr0s[64 + i] = lp;
     }
-    __syncthreads();
-  } else {
     __syncthreads();
   }
-  // u11 = L11 with A = L11^T L11 (reverse Cholesky), bottom row first:
-  //   L(j,j) = sqrt(A(j,j)); L(j,i) = A(j,i)/L(j,j); A(i',i) -= L(j,i') L(j,i)
-  for (int j = N1 - 1; j >= 0; j--) {
-    const double d = u[(int64_t)j * N + j];
-    const bool bad = !(d > 0.0);
-    if (bad && tid == 0) atomicCAS(&ra.ctl[2], 0, j + 1);
-    const double piv = sqrt(bad ? 1.0 : d);
-    const double rp = 1.0 / piv;
-    __syncthreads();
-    for (int i = tid; i < j; i += NTHREADS) u[(int64_t)i * N + j] *= rp;  // row j, columns i < j
-    if (tid == 0) u[(int64_t)j * N + j] = piv;
-    __syncthreads();
-    for (int64_t idx = tid; idx < (int64_t)j * j; idx += NTHREADS) {
-      const int ip = (int)(idx % j), i = (int)(idx / j);  // (row ip, col i), ip >= i
-      if (ip < i) continue;
-      u[(int64_t)i * N + ip] -= u[(int64_t)ip * N + j] * u[(int64_t)i * N + j];
+  // the panel back to C, then W' (explicit reflectors) in its place
+  for (int idx = tid; idx < h * nb; idx += NTHREADS) {
+    const int q = idx % h, pc = idx / h;
+    C[(int64_t)(c0 + pc) * ldc + row0 + q] = P[idx];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < h * nb; idx += NTHREADS) {
+    const int q = idx % h, pc = idx / h;
+    const int i = c1 - 1 - (c0 + pc);
+    const int a = lr0s[i], b = lr0s[64 + i];
+    const double v = (q < a || q > b) ? 0.0 : (q == b ? 1.0 : P[idx]);
+    P[idx] = v;
+    W[(int64_t)(c0 + i) * ldw + row0 + q] = v;
+  }
+  __syncthreads();
+  // G(a, b) = w'_a^T w'_b for a > b (w'_i is panel column nb - 1 - i)
+  for (int pr = warp; pr < nb * nb; pr += NTHREADS / 32) {
+    const int a = pr % nb, b = pr / nb;
+    if (a <= b) continue;
+    const double* wa = P + (nb - 1 - a) * h;
+    const double* wb = P + (nb - 1 - b) * h;
+    const int q0 = max(lr0s[a], lr0s[b]), q1 = min(lr0s[64 + a], lr0s[64 + b]);
+    double s = 0.0;
+    for (int q = q0 + lane; q <= q1; q += 32) s += wa[q] * wb[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) G[b * nb + a] = s;
+  }
+  __syncthreads();
+  // T in place of G's lower part, last column first
+  for (int i = nb - 1; i >= 0; i--) {
+    double v = 0.0;
+    const int rr = i + 1 + tid;
+    if (rr < nb) {
+      for (int s2 = i + 1; s2 <= rr; s2++) v += G[s2 * nb + rr] * G[i * nb + s2];
+      v *= -taus[i];
     }
     __syncthreads();
+    if (rr < nb) G[i * nb + rr] = v;
+    if (tid == 0) G[i * nb + i] = taus[i];
+    __syncthreads();
+  }
+  for (int idx = tid; idx < nb * nb; idx += NTHREADS) {
+    const int a = idx % nb, b = idx / nb;
+    Tg[(int64_t)b * ldt + a] = (a >= b) ? G[idx] : 0.0;
   }
 }
 
@@ -1003,7 +1028,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_EXTRACT: run_extract(ra, t); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;
-      case T_HOUSE: run_house(ra, t, smem); break;
+      case T_QL: run_ql(ra, t, smem); break;
+      case T_NOP: break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;
@@ -1021,15 +1047,17 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   }
 }
 
-size_t engine_smem_bytes() {
-  const size_t gemm = (size_t)2 * TILE * LDS;
-  return (gemm > (size_t)POTRF_SMEM_DOUBLES ? gemm : (size_t)POTRF_SMEM_DOUBLES) * sizeof(double);
-}
+static_assert(2 * TILE * LDS <= ENGINE_SMEM_BASE_DOUBLES, "GEMM staging exceeds the engine's shared memory");
+static_assert(POTRF_SMEM_DOUBLES <= ENGINE_SMEM_BASE_DOUBLES, "POTRF exceeds the engine's shared memory");
+
+size_t engine_smem_bytes() { return (size_t)ENGINE_SMEM_DOUBLES * sizeof(double); }
 
 // The dynamic shared-memory attribute must have been raised on the current
-// device by engine_occupancy() (done when a plan is created).
+// device by engine_occupancy() (done when a plan is created).  The launch
+// uses ra.smem_doubles (at least the GEMM/POTRF staging).
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream) {
-  size_t smem = engine_smem_bytes();
+  if (ra.smem_doubles < ENGINE_SMEM_BASE_DOUBLES || ra.smem_doubles > ENGINE_SMEM_DOUBLES) return cudaErrorInvalidValue;
+  size_t smem = (size_t)ra.smem_doubles * sizeof(double);
   engine_kernel<<<grid, NTHREADS, smem, stream>>>(ra);
   return cudaGetLastError();
 }

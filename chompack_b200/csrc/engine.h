@@ -20,6 +20,16 @@ constexpr int NTHREADS = 128;     // threads per CTA (4 warps)
 constexpr int KC = 16;            // K chunk staged through shared memory
 constexpr int LDS = TILE + 4;     // padded leading dimension of staged tiles
 constexpr int MAX_BASES = 64;     // base-pointer slots (see Base below)
+// Dynamic shared memory of the persistent kernel (doubles).  GEMM and POTRF
+// tasks need ENGINE_SMEM_BASE_DOUBLES (74 KB); programs with Householder
+// panels launch with ENGINE_SMEM_DOUBLES (112 KB, so that two CTAs still fit
+// an SM: 228 KB, 1 KB reserved per CTA).  The others keep the smaller
+// carve-out, which leaves more L1 for the register spills.
+constexpr int ENGINE_SMEM_BASE_DOUBLES = 9472;
+constexpr int ENGINE_SMEM_DOUBLES = 14336;
+// Shared-memory doubles a Householder panel of h rows and nb columns needs
+// (panel, then its nb x nb T factor, plus scalars).
+constexpr int ql_panel_doubles(int h, int nb) { return h * nb + nb * nb + 192; }
 
 // Base-pointer slots a task operand refers to.
 enum Base : uint8_t {
@@ -56,8 +66,16 @@ enum TaskOp : uint8_t {
   T_COPY = 5,     // strided copy / scale / zero of a tile
   T_INV = 6,      // inverse of a lower-triangular diagonal tile
   T_RPOTRF = 7,   // "reverse" Cholesky: S = L^T L with L lower (diag tile)
-  T_HOUSE = 8,    // Householder reduction of a factored update (one child)
-  T_VEC = 9       // vector ops for the triangular solve sweep
+  T_QL = 8,       // blocked Householder QL of update_factor (sub-op aux[3])
+  T_VEC = 9,      // vector ops for the triangular solve sweep
+  T_NOP = 10      // no work: joins dependencies
+};
+
+// Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the
+// parent-update columns C = L_k(:, r[N1:] - nn)).
+enum QlOp : int {
+  QL_GATHER = 0,  // C(:, j) = L_k(:, jj_j), zero above row jj_j
+  QL_PANEL = 1    // Householder reflections of the panel; W' and T factor
 };
 
 struct Operand {
@@ -82,7 +100,7 @@ struct Task {
   double alpha, beta;
   Operand a, b, c;
   int64_t off2;     // op-specific offset (base of the update-matrix region for
-                    // T_ASM / T_EXTRACT / T_HOUSE)
+                    // T_ASM / T_EXTRACT)
 };
 
 // Per-supernode description used by the gather/scatter tasks.
@@ -102,7 +120,7 @@ struct FrontDesc {
 struct RunArgs {
   const Task* tasks;
   int32_t ntasks;
-  int32_t pad;
+  int32_t smem_doubles;   // dynamic shared memory of this launch (doubles)
   const int2* waits;
   int* counters;          // ntasks task counters, then group counters
   int* ctl;               // [0] queue head, [1] error code, [2] info, [3] timeouts

@@ -110,6 +110,7 @@ extern "C" int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream
     std::memset(&ra, 0, sizeof(ra));
     ra.tasks = (const Task*)(base + tk_off);
     ra.ntasks = (int32_t)prog->tasks.size();
+    ra.smem_doubles = prog->smem_doubles;
     ra.waits = (const int2*)(base + wt_off);
     ra.ctl = (int*)(base + ctl_off);
     ra.counters = (int*)(base + cnt_off);

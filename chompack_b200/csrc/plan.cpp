@@ -60,6 +60,8 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;
+  for (const Task& t : prog->tasks)
+    if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
   Program* p = prog.get();
   plan->progs[key] = std::move(prog);
   return p;
@@ -91,6 +93,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   std::memset(&ra, 0, sizeof(ra));
   ra.tasks = prog->d_tasks;
   ra.ntasks = (int32_t)prog->tasks.size();
+  ra.smem_doubles = prog->smem_doubles;
   ra.waits = prog->d_waits;
   ra.ctl = (int*)w;
   ra.counters = (int*)(w + L.counters_off);

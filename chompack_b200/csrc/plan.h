@@ -19,6 +19,7 @@ struct Program {
   std::vector<int2> waits;
   int64_t ncounters = 0;   // tasks + groups
   int64_t ws_doubles = 0;  // doubles of workspace (update matrices + scratch)
+  int smem_doubles = ENGINE_SMEM_BASE_DOUBLES;  // dynamic shared memory per CTA
   Task* d_tasks = nullptr;
   int2* d_waits = nullptr;
   ~Program();

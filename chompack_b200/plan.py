@@ -42,7 +42,7 @@ class Plan(object):
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h:
+        if h and N is not None and getattr(N, "plan_destroy", None) is not None:  # not during interpreter teardown
             N.plan_destroy(h)
             self.handle = None
 

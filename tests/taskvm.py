@@ -31,7 +31,8 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_HOUSE, T_VEC = 8, 9
+T_QL, T_VEC, T_NOP = 8, 9, 10
+QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
@@ -148,8 +149,10 @@ class VM(object):
             self._extract(t)
         elif op == T_VEC:
             self._vec(t)
-        elif op == T_HOUSE:
-            self._house(t)
+        elif op == T_QL:
+            self._ql(t)
+        elif op == T_NOP:
+            pass
         elif op == T_COPY:
             m, n = int(t["m"]), int(t["n"])
             fl = int(t["aux"][0])
@@ -255,67 +258,75 @@ class VM(object):
             vals[~top] = ub[uo + (r[~top] - nn) + j * na]
             WS[base + j * Nc: base + (j + 1) * Nc] = vals
 
-    def _house(self, t):
-        """update_factor (update_factor.c:3-108) with numpy."""
+    def _ql(self, t):
+        """Blocked Householder QL of update_factor (engine.cu run_ql) with
+        numpy: QL_GATHER copies the parent-update columns, QL_PANEL reduces a
+        panel and writes the explicit reflectors W' and the T factor."""
         ch = self.p.fronts[int(t["aux"][0])]
         f = self.p.fronts[int(ch["parent"])]
         Nc, nn, na = int(ch["na"]), int(f["nn"]), int(f["na"])
         r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
-        A11 = (self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"]))
-        A21 = (self.bases[int(t["b"]["base"])], int(t["b"]["off"]), int(t["b"]["ld"]))
-        A22 = (self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
-
-        def F(i, j):   # j <= i, front coordinates
-            if j >= nn:
-                b, o, ld = A22
-                return b[o + (j - nn) * ld + (i - nn)]
-            if i >= nn:
-                b, o, ld = A21
-                return b[o + j * ld + (i - nn)]
-            b, o, ld = A11
-            return b[o + j * ld + i]
         N1 = int(np.sum(r < nn))
         N2 = Nc - N1
-        u = np.zeros((Nc, Nc))
-        for j in range(N1):
-            for i in range(j, Nc):
-                u[i, j] = F(r[i], r[j])
-        if N2 > 0:
-            C = np.zeros((na, N2))
-            for j in range(N2):
-                jj = r[N1 + j] - nn
-                for ii in range(jj, na):
-                    C[ii, j] = F(ii + nn, jj + nn)
-            for j in range(N2):
-                jj = r[Nc - 1 - j] - nn
-                ii = (na - jj) - (j + 1)
-                if ii == 0:
-                    continue
-                col, prow = N2 - 1 - j, na - 1 - j
-                r0 = prow - ii
-                x = C[r0:prow, col]
-                xn2 = float(np.dot(x, x))
-                alpha = C[prow, col]
-                if xn2 == 0.0:
-                    continue
-                beta = -np.copysign(np.sqrt(alpha * alpha + xn2), alpha)
-                tau = (beta - alpha) / beta
-                C[r0:prow, col] = x / (alpha - beta)
-                C[prow, col] = beta
-                v = np.concatenate([C[r0:prow, col], [1.0]])
-                blk = C[r0:prow + 1, :col]
-                C[r0:prow + 1, :col] = blk - tau * np.outer(v, v @ blk)
-            u[N1:, N1:] = np.tril(C[na - N2:, :])
-            L22 = u[N1:, N1:]
-            u[N1:, :N1] = np.linalg.solve(L22.T, u[N1:, :N1])
-            u[:N1, :N1] -= np.tril(u[N1:, :N1].T @ u[N1:, :N1])
-        A = np.tril(u[:N1, :N1]) + np.tril(u[:N1, :N1], -1).T
-        J = np.arange(N1)[::-1]
-        Lp = np.linalg.cholesky(A[np.ix_(J, J)])
-        u[:N1, :N1] = Lp.T[np.ix_(J, J)]
-        up = int(t["off2"]) + int(ch["upd"])
-        WS = self.bases[B_WS]
-        WS[up: up + Nc * Nc] = u.reshape(-1, order="F")
+        c0, c1, sub = int(t["aux"][1]), int(t["aux"][2]), int(t["aux"][3])
+        if sub == QL_GATHER:
+            Lb, Lo, ldl = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
+            Cb, Co, ldc = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
+            for j in range(c0, c1):
+                jj = int(r[N1 + j]) - nn
+                col = np.zeros(na)
+                col[jj:] = Lb[Lo + jj * ldl + jj: Lo + jj * ldl + na]
+                Cb[Co + j * ldc: Co + j * ldc + na] = col
+            return
+        Cb, Co, ldc = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
+        Wb, Wo, ldw = self.bases[int(t["b"]["base"])], int(t["b"]["off"]), int(t["b"]["ld"])
+        Tb, To, ldt = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
+        nb = c1 - c0
+        row0 = int(r[N1 + c0]) - nn
+        row1 = na - N2 + c1 - 1
+        h = row1 - row0 + 1
+        ci = Co + (c0 + np.arange(nb))[None, :] * ldc + row0 + np.arange(h)[:, None]
+        Pn = Cb[ci].copy()
+        taus = np.zeros(nb)
+        sup = []
+        for i in range(nb):
+            col = c1 - 1 - i
+            pc = col - c0
+            lr0 = int(r[N1 + col]) - nn - row0
+            lp = na - N2 + col - row0
+            sup.append((lr0, lp))
+            if lp <= lr0:
+                continue
+            x = Pn[lr0:lp, pc]
+            xn2 = float(np.dot(x, x))
+            if xn2 == 0.0:
+                continue
+            alpha = Pn[lp, pc]
+            beta = -np.copysign(np.hypot(alpha, np.sqrt(xn2)), alpha)
+            tau = (beta - alpha) / beta
+            Pn[lr0:lp, pc] = x / (alpha - beta)
+            v = np.concatenate([Pn[lr0:lp, pc], [1.0]])
+            blk = Pn[lr0:lp + 1, :pc]
+            Pn[lr0:lp + 1, :pc] = blk - tau * np.outer(v, v @ blk)
+            Pn[lp, pc] = beta
+            taus[i] = tau
+        Cb[ci] = Pn
+        Wp = np.zeros((h, nb))
+        for i in range(nb):
+            lr0, lp = sup[i]
+            pc = nb - 1 - i
+            Wp[lr0:lp, i] = Pn[lr0:lp, pc]
+            Wp[lp, i] = 1.0
+        wi = Wo + (c0 + np.arange(nb))[None, :] * ldw + row0 + np.arange(h)[:, None]
+        Wb[wi] = Wp
+        G = Wp.T @ Wp
+        T = np.zeros((nb, nb))
+        for i in range(nb - 1, -1, -1):
+            T[i, i] = taus[i]
+            if i + 1 < nb:
+                T[i + 1:, i] = -taus[i] * (T[i + 1:, i + 1:] @ G[i + 1:, i])
+        ti = To + np.arange(nb)[None, :] * ldt + np.arange(nb)[:, None]
+        Tb[ti] = T
 
     def _extract(self, t):
         ch = self.p.fronts[int(t["aux"][0])]
