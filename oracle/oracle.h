@@ -17,4 +17,31 @@ int orc_cholesky(int64_t n, int64_t nsn, const int64_t* snpost, const int64_t* s
                  const int64_t* relidx, const int64_t* chptr, const int64_t* chidx, const int64_t* blkptr,
                  double* blkval, double* fws, double* upd, int64_t* upd_size);
 
+void orc_llt(int64_t n, int64_t nsn, const int64_t* snpost, const int64_t* snptr, const int64_t* relptr,
+             const int64_t* relidx, const int64_t* chptr, const int64_t* chidx, const int64_t* blkptr,
+             double* blkval, double* fws, double* upd, int64_t* upd_size);
+
+int orc_projected_inverse(int64_t n, int64_t nsn, const int64_t* snpost, const int64_t* snptr,
+                          const int64_t* relptr, const int64_t* relidx, const int64_t* chptr, const int64_t* chidx,
+                          const int64_t* blkptr, double* blkval, double* fws, double* upd, int64_t* upd_size);
+
+int orc_completion(int64_t n, int64_t nsn, const int64_t* snpost, const int64_t* snptr, const int64_t* relptr,
+                   const int64_t* relidx, const int64_t* chptr, const int64_t* chidx, const int64_t* blkptr,
+                   double* blkval, double* fws, double* upd, int64_t* upd_size, int factored_updates);
+
+int orc_hessian(int64_t n, int64_t nsn, const int64_t* snpost, const int64_t* snptr, const int64_t* relptr,
+                const int64_t* relidx, const int64_t* chptr, const int64_t* chidx, const int64_t* blkptr,
+                const double* lblkval, const double* yblkval, double** ublkval, int64_t nu, double* fws,
+                double* upd, int64_t* upd_size, int inv, int adj, int factored_updates);
+
+void orc_trsm(char trans, int nrhs, double alpha, int64_t n, int64_t nsn, const int64_t* snpost,
+              const int64_t* snptr, const int64_t* snode, const int64_t* relptr, const int64_t* relidx,
+              const int64_t* chptr, const int64_t* chidx, const int64_t* blkptr, const int64_t* p,
+              const double* blkval, double* b, int ldb, double* fws, double* upd, int64_t* upd_size);
+
+int orc_update_factor(const int64_t* r, int nn, int na, double* u, int N, const double* f, int ldf, double* C);
+
+double orc_dot(int64_t nsn, const int64_t* snptr, const int64_t* sncolptr, const int64_t* blkptr,
+               const double* x, const double* y);
+
 #endif

@@ -54,3 +54,29 @@ def block_errors(symb, x, ref):
 def assert_blocks_close(symb, x, ref, rtol=RTOL):
     e = block_errors(symb, x, ref)
     assert e <= rtol, "scaled block error %.3e exceeds %.1e" % (e, rtol)
+
+
+def rowsign_errors(symb, x, ref):
+    """Like block_errors, but each row of a supernode's off-diagonal block may
+    match the reference up to its sign.  Used for single applications of the
+    factored-update Hessian factors (adj == inv): those rows are multiplied
+    by the update factor L_k of update_factor.c, whose row signs are fixed by
+    Householder pivots that can be exactly zero in exact arithmetic, where the
+    reference's sign comes from its BLAS's rounding."""
+    x = np.asarray(x)
+    ref = np.asarray(ref)
+    worst = 0.0
+    for k in range(symb.Nsn):
+        nn = int(symb.snptr[k + 1] - symb.snptr[k])
+        nj = int(symb.sncolptr[k + 1] - symb.sncolptr[k])
+        b = slice(int(symb.blkptr[k]), int(symb.blkptr[k + 1]))
+        xm = x[b].reshape((nj, nn), order="F").copy()
+        rm = ref[b].reshape((nj, nn), order="F")
+        for i in range(nn, nj):
+            if np.abs(xm[i] + rm[i]).max() < np.abs(xm[i] - rm[i]).max():
+                xm[i] = -xm[i]
+        mask = np.tril(np.ones((nj, nn), dtype=bool))
+        rv = rm[mask]
+        scale = np.maximum(np.abs(rv), FLOOR * max(np.abs(rv).max(), 1e-300))
+        worst = max(worst, float((np.abs(xm[mask] - rv) / scale).max()))
+    return worst
