@@ -20,9 +20,7 @@ from . import amd
 __all__ = ["spmatrix", "tril", "triu", "symmetrize", "perm", "eye", "symbolic", "merge_size_fill", "peo",
            "cspmatrix", "amd"]
 
-try:
-    from .cbase import cholesky, llt, projected_inverse, completion, hessian, trsm, dot  # noqa: F401
-    __all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot"]
-except ImportError as _e:  # pragma: no cover - only while the sweeps are being built
-    if "cbase" not in str(_e):
-        raise
+from .cbase import cholesky, llt, projected_inverse, completion, hessian, trsm, dot  # noqa: E402,F401
+from . import autograd  # noqa: E402,F401
+
+__all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot", "autograd"]

@@ -1,0 +1,137 @@
+"""Differentiable chordal log-determinant.
+
+    f(X) = log det X,     X symmetric positive definite with chordal pattern
+
+on the values of a cspmatrix (its `blkval` tensor, the reference block
+layout).  A function of the stored entries x (lower trapezoid of each
+supernode block) sees the symmetric matrix X with X_ij = X_ji = x_ij, so
+
+    df/dx = w .* Y,       Y = P(X^{-1}) = projected_inverse(cholesky(X))
+
+with w = 2 below the diagonal, 1 on it, 0 in the strict upper part of a
+diagonal block (the weights of `dot`: <A, B> = sum w a b).  The second
+derivative is the Hessian of the barrier: d<Y, C>/dX = -H_X(C), with
+H_X(C) = P(X^{-1} C X^{-1}) = hessian(L, Y, C, adj=None), so the backward
+of the gradient is -w .* H_X(unpack(c)).
+
+Forward: one `cholesky` sweep and a log-det reduction of the factor's
+diagonal.  Backward: one `projected_inverse` sweep (the reverse multifrontal
+adjoint of the factorisation).  Double backward: one full `hessian`
+application.  All three run as the package's CUDA sweeps; torch only holds
+the tensors and the autograd graph.
+
+A leading batch dimension of value sets on one pattern (values of shape
+(B, blkptr[Nsn])) is supported; each value set is swept on its own.
+"""
+import torch
+
+from . import _native as N
+from . import cbase
+from .cspmatrix import cspmatrix
+
+__all__ = ["logdet", "logdet_values", "logdet_gradient", "logdet_hvp"]
+
+
+def _stream(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise RuntimeError("%s failed: %s" % (what, N.last_error().decode()))
+
+
+def _factor(symb, x):
+    """Cholesky factor values of one value set (a new tensor)."""
+    L = cspmatrix(symb, blkval=x.detach().clone().contiguous())
+    cbase.cholesky(L)
+    return L
+
+
+def _logdet_of_factor(symb, L):
+    v = L.blkval
+    plan = symb.plan(v.device.index)
+    ws, nb = plan.workspace(N.OP_DOT)
+    out = torch.empty(1, dtype=torch.float64, device=v.device)
+    _check(N.logdet(plan.handle, v.data_ptr(), out.data_ptr(), ws, nb, _stream(v.device)), "logdet")
+    return out[0]
+
+
+def _sym_weight(symb, x, alpha=1.0):
+    """alpha * w .* x (a new tensor)."""
+    y = torch.empty_like(x)
+    plan = symb.plan(x.device.index)
+    _check(N.sym_weight(plan.handle, x.data_ptr(), y.data_ptr(), float(alpha), _stream(x.device)), "sym_weight")
+    return y
+
+
+class _LogdetGrad(torch.autograd.Function):
+    """x -> w .* P(X^{-1}), given the factor values L of X."""
+
+    @staticmethod
+    def forward(ctx, x, L, symb):
+        Y = cspmatrix(symb, blkval=L.clone(), factor=True)
+        cbase.projected_inverse(Y)
+        ctx.save_for_backward(L, Y.blkval)
+        ctx.symb = symb
+        return _sym_weight(symb, Y.blkval)
+
+    @staticmethod
+    def backward(ctx, c):
+        L, Yv = ctx.saved_tensors
+        symb = ctx.symb
+        U = cspmatrix(symb, blkval=c.detach().to(torch.float64).contiguous().clone())
+        cbase.hessian(cspmatrix(symb, blkval=L, factor=True), cspmatrix(symb, blkval=Yv), U, adj=None)
+        return _sym_weight(symb, U.blkval, -1.0), None, None
+
+
+class _Logdet(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, symb):
+        L = _factor(symb, x)
+        ctx.save_for_backward(x, L.blkval)
+        ctx.symb = symb
+        return _logdet_of_factor(symb, L)
+
+    @staticmethod
+    def backward(ctx, g):
+        x, Lv = ctx.saved_tensors
+        return g * _LogdetGrad.apply(x, Lv, ctx.symb), None
+
+
+def logdet_values(x, symb):
+    """log det of the chordal SPD matrix with block values x (1-D, or
+    (B, n_values) for B value sets on `symb`'s pattern), differentiable
+    (first and second order)."""
+    if not isinstance(x, torch.Tensor) or x.device.type != "cuda" or x.dtype != torch.float64:
+        raise ValueError("values must be a float64 CUDA tensor")
+    if x.dim() == 1:
+        return _Logdet.apply(x, symb)
+    return torch.stack([_Logdet.apply(x[b], symb) for b in range(x.shape[0])])
+
+
+def logdet(X):
+    """log det of a cspmatrix X (not a factor), differentiable through
+    X.blkval."""
+    if X.is_factor is not False:
+        raise ValueError("X must be a cspmatrix")
+    return logdet_values(X.blkval, X.symb)
+
+
+def logdet_gradient(X):
+    """The gradient of log det at X as a cspmatrix: Y = P(X^{-1})
+    (cholesky followed by projected_inverse, without autograd)."""
+    Y = cspmatrix(X.symb, blkval=X.blkval.detach().clone())
+    cbase.cholesky(Y)
+    cbase.projected_inverse(Y)
+    return Y
+
+
+def logdet_hvp(L, Y, U):
+    """The second directional derivative of log det at X = L L^T along the
+    cspmatrix U: -H_X(U) = -P(X^{-1} U X^{-1}), as a new cspmatrix (L the
+    factor, Y the projected inverse)."""
+    V = cspmatrix(U.symb, blkval=U.blkval.detach().clone())
+    cbase.hessian(L, Y, V, adj=None)
+    V.blkval.mul_(-1.0)
+    return V

@@ -87,6 +87,28 @@ extern "C" int chb_dot(chb_plan* plan, const double* x, const double* y, double*
   return 0;
 }
 
+extern "C" int chb_logdet(chb_plan* plan, const double* l, double* result, void* work, size_t work_bytes,
+                          void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  const size_t need = 256 + (size_t)(plan->nsn + 1) * sizeof(double);
+  if (work_bytes < need || !work) return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, need);
+  double* partial = (double*)((char*)work + 256);
+  cudaError_t e = logdet_launch(l, plan->d_fronts, (int)plan->nsn, partial, result, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(-100 - (int)e, "logdet launch failed: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int chb_sym_weight(chb_plan* plan, const double* x, double* y, double alpha, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  cudaError_t e = symw_launch(x, y, alpha, plan->d_fronts, (int)plan->nsn, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(-100 - (int)e, "sym_weight launch failed: %s", cudaGetErrorString(e));
+  return 0;
+}
+
 extern "C" int chb_info(chb_plan* plan, void* work, void* stream) {
   clear_error();
   int rc = check_plan(plan);

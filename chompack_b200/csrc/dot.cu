@@ -50,7 +50,59 @@ __global__ void __launch_bounds__(DOT_THREADS) dot_final(const double* __restric
   const double s = block_sum(acc, sh);
   if (threadIdx.x == 0) *out = s;
 }
+// log det X = 2 * sum_k sum_j log L_kk(j, j) from the factor's diagonal
+// blocks; one partial per supernode, added by dot_final.
+__global__ void __launch_bounds__(DOT_THREADS) logdet_blocks(const double* __restrict__ l,
+                                                             const FrontDesc* __restrict__ fronts, int nsn,
+                                                             double* __restrict__ partial) {
+  __shared__ double sh[DOT_THREADS];
+  for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
+    const FrontDesc f = fronts[k];
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < f.nn; j += DOT_THREADS) acc += 2.0 * log(l[f.blk + (int64_t)j * f.nj + j]);
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[k] = s;
+    __syncthreads();
+  }
+}
+
+// y = alpha * w .* x over the stored entries, w = 2 below the diagonal, 1 on
+// it, 0 in the strict upper part of a diagonal block: the map from a
+// chordal symmetric matrix to the gradient of a function of its stored
+// entries (<A, B> = sum w a b).
+__global__ void __launch_bounds__(DOT_THREADS) symw_blocks(const double* __restrict__ x, double* __restrict__ y,
+                                                           double alpha, const FrontDesc* __restrict__ fronts,
+                                                           int nsn) {
+  for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
+    const FrontDesc f = fronts[k];
+    const int64_t total = (int64_t)f.nj * f.nn;
+    for (int64_t idx = threadIdx.x; idx < total; idx += DOT_THREADS) {
+      const int r = (int)(idx % f.nj), c = (int)(idx / f.nj);
+      const double w = (r > c) ? 2.0 : (r == c ? 1.0 : 0.0);
+      y[f.blk + idx] = alpha * w * x[f.blk + idx];
+    }
+  }
+}
 }  // namespace
+
+cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, double* partial, double* out,
+                          cudaStream_t stream) {
+  if (nsn > 0) {
+    int grid = nsn < 4096 ? nsn : 4096;
+    logdet_blocks<<<grid, DOT_THREADS, 0, stream>>>(l, fronts, nsn, partial);
+  }
+  dot_final<<<1, DOT_THREADS, 0, stream>>>(partial, nsn, out);
+  return cudaGetLastError();
+}
+
+cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,
+                        cudaStream_t stream) {
+  if (nsn > 0) {
+    int grid = nsn < 4096 ? nsn : 4096;
+    symw_blocks<<<grid, DOT_THREADS, 0, stream>>>(x, y, alpha, fronts, nsn);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
                        double* out, cudaStream_t stream) {

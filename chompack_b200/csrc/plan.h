@@ -84,6 +84,10 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
 size_t engine_smem_bytes();
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream);
 int engine_occupancy(int* blocks_per_sm);
+cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, double* partial, double* out,
+                          cudaStream_t stream);
+cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,
+                        cudaStream_t stream);
 cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
                        double* out, cudaStream_t stream);
 

@@ -142,6 +142,20 @@ int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const doubl
 int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
             size_t work_bytes, void* stream);
 
+/* log det X from its factor L (the blkval chb_cholesky leaves):
+ * 2 * sum of log L_kk(j, j) over the diagonal blocks, deterministic.  No
+ * single reference routine: the reference's callers form it from the
+ * factor's diagonal (L.diag(), symbolic.py:1113-1128).  Workspace as for
+ * CHB_OP_DOT. */
+int chb_logdet(chb_plan* plan, const double* l, double* result, void* work, size_t work_bytes, void* stream);
+
+/* y = alpha * w .* x over the stored block entries, w = 2 below the
+ * diagonal, 1 on it, 0 in the strict upper part of each diagonal block: maps
+ * a chordal symmetric matrix to the gradient, with respect to the stored
+ * entries, of <X, .> (the inner product of dot).  x and y may alias.  No
+ * reference counterpart (used by the autograd layer). */
+int chb_sym_weight(chb_plan* plan, const double* x, double* y, double alpha, void* stream);
+
 /* Profiling: when `buffer` (device memory, 32 bytes per task) is set, the
  * next sweeps whose task count fits `capacity_tasks` record per task the
  * global-timer ns at claim, start (dependencies met) and end, and the SM id
