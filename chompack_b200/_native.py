@@ -75,6 +75,11 @@ hessian = _sig("chb_hessian", ctypes.c_int, [PPLAN, vp, vp, ctypes.POINTER(vp), 
                                              ctypes.c_int, vp, ctypes.c_size_t, vp])
 trsm = _sig("chb_trsm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
 dot = _sig("chb_dot", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
+plan_merge = _sig("chb_plan_merge", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                                    ctypes.POINTER(PPLAN)])
+plan_batch_info = _sig("chb_plan_batch_info", ctypes.c_int, [PPLAN, ctypes.POINTER(i64), ctypes.POINTER(i64)])
+logdet_batch = _sig("chb_logdet_batch", ctypes.c_int, [PPLAN, vp, vp, vp, ctypes.c_size_t, vp])
+dot_batch = _sig("chb_dot_batch", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 logdet = _sig("chb_logdet", ctypes.c_int, [PPLAN, vp, vp, vp, ctypes.c_size_t, vp])
 sym_weight = _sig("chb_sym_weight", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_double, vp])
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])

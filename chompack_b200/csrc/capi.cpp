@@ -100,6 +100,43 @@ extern "C" int chb_logdet(chb_plan* plan, const double* l, double* result, void*
   return 0;
 }
 
+// Per-matrix reductions of a merged plan (chb_plan_merge): results[m] for
+// each of its matrices (a plan from chb_plan_create has one).
+static int batch_reduce(chb_plan* plan, const double* a, const double* b, bool logdet, double* results, void* work,
+                        size_t work_bytes, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  const size_t need = 256 + (size_t)(plan->nsn + 1) * sizeof(double);
+  if (work_bytes < need || !work) return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, need);
+  double* partial = (double*)((char*)work + 256);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = logdet ? logdet_partials(a, plan->d_fronts, (int)plan->nsn, partial, st)
+                         : dot_partials(a, b, plan->d_fronts, (int)plan->nsn, partial, st);
+  if (e == cudaSuccess) e = segment_sums(partial, plan->d_seg, (int)plan->seg.size() - 1, results, st);
+  if (e != cudaSuccess) return set_error(-100 - (int)e, "reduction launch failed: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int chb_logdet_batch(chb_plan* plan, const double* l, double* results, void* work, size_t work_bytes,
+                                void* stream) {
+  return batch_reduce(plan, l, nullptr, true, results, work, work_bytes, stream);
+}
+
+extern "C" int chb_dot_batch(chb_plan* plan, const double* x, const double* y, double* results, void* work,
+                             size_t work_bytes, void* stream) {
+  return batch_reduce(plan, x, y, false, results, work, work_bytes, stream);
+}
+
+extern "C" int chb_plan_batch_info(const chb_plan* plan, int64_t* count, int64_t* seg_out) {
+  clear_error();
+  if (!plan) return set_error(-1, "null plan");
+  if (count) *count = (int64_t)plan->seg.size() - 1;
+  if (seg_out)
+    for (size_t i = 0; i < plan->seg.size(); i++) seg_out[i] = plan->seg[i];
+  return 0;
+}
+
 extern "C" int chb_sym_weight(chb_plan* plan, const double* x, double* y, double alpha, void* stream) {
   clear_error();
   int rc = check_plan(plan);

@@ -83,7 +83,37 @@ __global__ void __launch_bounds__(DOT_THREADS) symw_blocks(const double* __restr
     }
   }
 }
+// out[m] = sum of partial[seg[m] .. seg[m+1]) in a fixed order (one CTA per
+// segment): the per-matrix results of a merged plan.
+__global__ void __launch_bounds__(DOT_THREADS) seg_final(const double* __restrict__ partial,
+                                                         const int64_t* __restrict__ seg, int count,
+                                                         double* __restrict__ out) {
+  __shared__ double sh[DOT_THREADS];
+  for (int m = blockIdx.x; m < count; m += gridDim.x) {
+    double acc = 0.0;
+    for (int64_t i = seg[m] + threadIdx.x; i < seg[m + 1]; i += DOT_THREADS) acc += partial[i];
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) out[m] = s;
+    __syncthreads();
+  }
+}
 }  // namespace
+
+cudaError_t segment_sums(const double* partial, const int64_t* seg, int count, double* out, cudaStream_t stream) {
+  if (count > 0) seg_final<<<count < 4096 ? count : 4096, DOT_THREADS, 0, stream>>>(partial, seg, count, out);
+  return cudaGetLastError();
+}
+
+cudaError_t logdet_partials(const double* l, const FrontDesc* fronts, int nsn, double* partial, cudaStream_t stream) {
+  if (nsn > 0) logdet_blocks<<<nsn < 4096 ? nsn : 4096, DOT_THREADS, 0, stream>>>(l, fronts, nsn, partial);
+  return cudaGetLastError();
+}
+
+cudaError_t dot_partials(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
+                         cudaStream_t stream) {
+  if (nsn > 0) dot_blocks<<<nsn < 4096 ? nsn : 4096, DOT_THREADS, 0, stream>>>(x, y, fronts, nsn, partial);
+  return cudaGetLastError();
+}
 
 cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, double* partial, double* out,
                           cudaStream_t stream) {

@@ -116,6 +116,38 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
 
 using namespace chb;
 
+// Device copies of the plan's symbolic data (skipped with device < 0: a
+// host-only plan for introspection) and the persistent grid size.
+static int upload_plan(chb_plan* P) {
+  const int device = P->device;
+  if (device < 0) return 0;
+  const int64_t nsn = P->nsn, n = P->n, nrel = (int64_t)P->relidx.size();
+  CUDA_TRY(cudaSetDevice(device));
+  if (nsn > 0) {
+    CUDA_TRY(cudaMalloc(&P->d_fronts, nsn * sizeof(FrontDesc)));
+    CUDA_TRY(cudaMemcpy(P->d_fronts, P->fronts.data(), nsn * sizeof(FrontDesc), cudaMemcpyHostToDevice));
+  }
+  if (nrel > 0) {
+    CUDA_TRY(cudaMalloc(&P->d_relidx, nrel * sizeof(int32_t)));
+    CUDA_TRY(cudaMemcpy(P->d_relidx, P->relidx.data(), nrel * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (!P->chidx.empty()) {
+    CUDA_TRY(cudaMalloc(&P->d_chidx, P->chidx.size() * sizeof(int32_t)));
+    CUDA_TRY(cudaMemcpy(P->d_chidx, P->chidx.data(), P->chidx.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (n > 0) {
+    CUDA_TRY(cudaMalloc(&P->d_perm, n * sizeof(int64_t)));
+    CUDA_TRY(cudaMemcpy(P->d_perm, P->perm.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(cudaMalloc(&P->d_seg, P->seg.size() * sizeof(int64_t)));
+  CUDA_TRY(cudaMemcpy(P->d_seg, P->seg.data(), P->seg.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+  int per_sm = 0, nsm = 0;
+  if (engine_occupancy(&per_sm) != 0 || per_sm <= 0) return set_error(-12, "engine kernel cannot be resident");
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  P->grid = per_sm * nsm;
+  return 0;
+}
+
 extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, const int64_t* snpar,
                                const int64_t* relptr, const int64_t* relidx, const int64_t* chptr,
                                const int64_t* chidx, const int64_t* blkptr, const int64_t* snode, const int64_t* p,
@@ -188,30 +220,63 @@ extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, con
   }
   P->nlevels = nsn ? maxlv + 1 : 0;
 
-  // device upload (skipped with device < 0: host-only plan for introspection)
-  if (device >= 0) {
-    CUDA_TRY(cudaSetDevice(device));
-    if (nsn > 0) {
-      CUDA_TRY(cudaMalloc(&P->d_fronts, nsn * sizeof(FrontDesc)));
-      CUDA_TRY(cudaMemcpy(P->d_fronts, P->fronts.data(), nsn * sizeof(FrontDesc), cudaMemcpyHostToDevice));
+  P->seg.assign({0, nsn});
+  int rc = upload_plan(P.get());
+  if (rc) return rc;
+  *out = P.release();
+  return 0;
+}
+
+extern "C" int chb_plan_merge(const chb_plan* const* plans, int count, int device, chb_plan** out) {
+  clear_error();
+  if (!out) return set_error(-1, "null output pointer");
+  *out = nullptr;
+  if (count <= 0 || !plans) return set_error(-1, "merge: no plans");
+  std::unique_ptr<chb_plan> P(new chb_plan());
+  P->device = device;
+  P->seg.push_back(0);
+  int64_t n_off = 0, nsn_off = 0, rel_off = 0, ch_off = 0, blk_off = 0, upd = 0, vpos = 0;
+  for (int m = 0; m < count; m++) {
+    const chb_plan* Q = plans[m];
+    if (!Q) return set_error(-1, "merge: null plan %d", m);
+    for (int64_t k = 0; k < Q->nsn; k++) {
+      FrontDesc f = Q->fronts[k];
+      f.relptr += (int32_t)rel_off;
+      f.chbeg += (int32_t)ch_off;
+      f.chend += (int32_t)ch_off;
+      f.parent += (int32_t)nsn_off;
+      f.blk += blk_off;
+      f.upd = upd;
+      f.col0 += n_off;
+      f.vpos = vpos;
+      upd += (int64_t)f.na * f.na;
+      vpos += f.na;
+      P->fronts.push_back(f);
+      P->snpar.push_back(Q->snpar[k] + (int32_t)nsn_off);
+      P->level.push_back(Q->level[k]);
+      P->snptr.push_back(Q->snptr[k] + n_off);
     }
-    if (nrel > 0) {
-      CUDA_TRY(cudaMalloc(&P->d_relidx, nrel * sizeof(int32_t)));
-      CUDA_TRY(cudaMemcpy(P->d_relidx, P->relidx.data(), nrel * sizeof(int32_t), cudaMemcpyHostToDevice));
-    }
-    if (!P->chidx.empty()) {
-      CUDA_TRY(cudaMalloc(&P->d_chidx, P->chidx.size() * sizeof(int32_t)));
-      CUDA_TRY(cudaMemcpy(P->d_chidx, P->chidx.data(), P->chidx.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    }
-    if (n > 0) {
-      CUDA_TRY(cudaMalloc(&P->d_perm, n * sizeof(int64_t)));
-      CUDA_TRY(cudaMemcpy(P->d_perm, p, n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    }
-    int per_sm = 0, nsm = 0;
-    if (engine_occupancy(&per_sm) != 0 || per_sm <= 0) return set_error(-12, "engine kernel cannot be resident");
-    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-    P->grid = per_sm * nsm;
+    for (int32_t r : Q->relidx) P->relidx.push_back(r);
+    for (int32_t c : Q->chidx) P->chidx.push_back(c + (int32_t)nsn_off);
+    for (int64_t v : Q->snode) P->snode.push_back(v + n_off);
+    for (int64_t v : Q->perm) P->perm.push_back(v + n_off);
+    P->nlevels = std::max(P->nlevels, Q->nlevels);
+    n_off += Q->n;
+    nsn_off += Q->nsn;
+    rel_off += (int64_t)Q->relidx.size();
+    ch_off += (int64_t)Q->chidx.size();
+    blk_off += Q->blk_total;
+    P->seg.push_back(nsn_off);
+    if (nsn_off > INT32_MAX / 2 || rel_off > INT32_MAX || ch_off > INT32_MAX)
+      return set_error(-7, "merge: the batch exceeds the 32-bit index range");
   }
+  P->snptr.push_back(n_off);
+  P->n = n_off;
+  P->nsn = nsn_off;
+  P->blk_total = blk_off;
+  P->upd_total = upd;
+  int rc = upload_plan(P.get());
+  if (rc) return rc;
   *out = P.release();
   return 0;
 }
@@ -224,6 +289,7 @@ extern "C" int chb_plan_destroy(chb_plan* plan) {
   if (plan->d_relidx) cudaFree(plan->d_relidx);
   if (plan->d_chidx) cudaFree(plan->d_chidx);
   if (plan->d_perm) cudaFree(plan->d_perm);
+  if (plan->d_seg) cudaFree(plan->d_seg);
   delete plan;
   return 0;
 }

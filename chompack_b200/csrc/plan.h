@@ -63,6 +63,8 @@ struct chb_plan {
   int32_t* d_relidx = nullptr;
   int32_t* d_chidx = nullptr;
   int64_t* d_perm = nullptr;    // p (trsm row gather)
+  std::vector<int64_t> seg;     // matrices of a merged plan: supernodes [seg[m], seg[m+1])
+  int64_t* d_seg = nullptr;
   int grid = 0;                 // persistent grid size
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
@@ -88,6 +90,10 @@ cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, dou
                           cudaStream_t stream);
 cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,
                         cudaStream_t stream);
+cudaError_t segment_sums(const double* partial, const int64_t* seg, int count, double* out, cudaStream_t stream);
+cudaError_t logdet_partials(const double* l, const FrontDesc* fronts, int nsn, double* partial, cudaStream_t stream);
+cudaError_t dot_partials(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
+                         cudaStream_t stream);
 cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
                        double* out, cudaStream_t stream);
 

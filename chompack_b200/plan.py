@@ -20,6 +20,39 @@ class Plan(object):
     """Uploaded symbolic factorisation.  device=None picks the current CUDA
     device; device=-1 builds a host-only plan (introspection only)."""
 
+    @classmethod
+    def merged(cls, plans, device=None):
+        """One plan over the disjoint union of `plans` (chb_plan_merge): a
+        batch swept by one launch per sweep."""
+        if device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("chompack_b200 sweeps need a CUDA device (no CPU fallback)")
+            device = torch.cuda.current_device()
+        self = cls.__new__(cls)
+        self.device = int(device)
+        self.symb = None
+        self._keep = list(plans)
+        arr = (ctypes.c_void_p * len(plans))(*[p.handle.value if hasattr(p.handle, "value") else p.handle
+                                               for p in plans])
+        h = N.PPLAN()
+        if self.device >= 0:
+            with torch.cuda.device(self.device):
+                rc = N.plan_merge(arr, len(plans), self.device, ctypes.byref(h))
+        else:
+            rc = N.plan_merge(arr, len(plans), self.device, ctypes.byref(h))
+        N.check(rc, "plan_merge")
+        self.handle = h
+        self._ws = {}
+        return self
+
+    def batch_segments(self):
+        """Supernode ranges of the matrices of this plan (count + 1 offsets)."""
+        cnt = ctypes.c_int64()
+        N.check(N.plan_batch_info(self.handle, ctypes.byref(cnt), None), "plan_batch_info")
+        seg = (ctypes.c_int64 * (cnt.value + 1))()
+        N.check(N.plan_batch_info(self.handle, None, seg), "plan_batch_info")
+        return list(seg)
+
     def __init__(self, symb, device=None):
         if device is None:
             if not torch.cuda.is_available():

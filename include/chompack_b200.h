@@ -156,6 +156,27 @@ int chb_logdet(chb_plan* plan, const double* l, double* result, void* work, size
  * reference counterpart (used by the autograd layer). */
 int chb_sym_weight(chb_plan* plan, const double* x, double* y, double alpha, void* stream);
 
+/* Batches.  chb_plan_merge builds one plan over the disjoint union of the
+ * given plans' clique trees (a forest): supernodes, columns, relative
+ * indices and block values are concatenated in the order given, so a batch
+ * of matrices, or of value sets on one pattern (the same plan repeated),
+ * is factored by ONE launch of each sweep on the concatenated blkval.  The
+ * inputs may be host-only plans (device < 0) and stay owned by the caller.
+ * The batched counterpart the reference lacks (its wrapper takes one
+ * cspmatrix per call, cbase.c:187-284). */
+int chb_plan_merge(const chb_plan* const* plans, int count, int device, chb_plan** out);
+
+/* The matrices of a (merged) plan: count, and their supernode ranges
+ * seg[m] .. seg[m+1] (count + 1 entries; may be NULL). */
+int chb_plan_batch_info(const chb_plan* plan, int64_t* count, int64_t* seg);
+
+/* Per-matrix log det (from the factor) and <X, Y> of a merged plan:
+ * results[m], m < count (device doubles).  Workspace as for CHB_OP_DOT. */
+int chb_logdet_batch(chb_plan* plan, const double* l, double* results, void* work, size_t work_bytes,
+                     void* stream);
+int chb_dot_batch(chb_plan* plan, const double* x, const double* y, double* results, void* work,
+                  size_t work_bytes, void* stream);
+
 /* Profiling: when `buffer` (device memory, 32 bytes per task) is set, the
  * next sweeps whose task count fits `capacity_tasks` record per task the
  * global-timer ns at claim, start (dependencies met) and end, and the SM id
