@@ -46,7 +46,17 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   for (int64_t k = 0; k < N; k++)
     if (P.fronts[k].na > 0) uc_group[k] = B.new_group();
 
-  std::vector<int> last_top, last_bot, trsm_top, trsm_prev, trsmb, last_mrow;
+  // a dependency on a task's end, or on an early-signal group
+  struct Dep {
+    int id = -1;
+    bool group = false;
+  };
+  auto wait_dep = [&](int task, const Dep& d) {
+    if (d.group) B.wait_group(task, d.id);
+    else B.wait_task(task, d.id);
+  };
+  std::vector<int> last_top, last_bot, trsmb, last_mrow;
+  std::vector<Dep> trsm_top, trsm_prev;
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int nn = f.nn, na = f.na, nj = f.nj;
@@ -69,7 +79,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       for (int j = nn; j < nj; j++) colwork[j] += nj - j;  // zeroing of U_k
       double total = 0.0;
       for (double w : colwork) total += w;
-      const double target = std::max(8192.0, total / 64.0);
+      const double target = std::max(4096.0, total / 256.0);
       int j0 = 0;
       while (j0 < nj) {
         int j1 = j0;
@@ -90,8 +100,8 @@ int build_cholesky(const chb_plan& P, Program& prog) {
 
     last_top.assign((size_t)NBc * NBc, -1);
     last_bot.assign((size_t)std::max(NBb, 1) * NBc, -1);
-    trsm_top.assign(NBc, -1);
-    trsm_prev.assign(NBc, -1);
+    trsm_top.assign(NBc, Dep());
+    trsm_prev.assign(NBc, Dep());
     trsmb.assign(std::max(NBb, 1), -1);
     last_mrow.assign(NBc, -1);
     int pot = -1;
@@ -112,16 +122,39 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         else B.wait_task(pot, last_top[(size_t)c * NBc + c]);
       }
       const Operand Mcc = opnd(B_WS, M + (int64_t)cT * nn + cT, nn, OM_TRI_N, 0);
-      // TRSM of the top tiles below the diagonal: P(r,c) := P(r,c) * M_cc^T
+      // TRSM of the top tiles below the diagonal: P(r,c) := P(r,c) * M_cc^T.
+      // The next diagonal block's tile goes through the look-ahead task,
+      // which also applies that tile's rank-64 update of the next diagonal
+      // tile, so the chain POTRF(c) -> POTRF(c+1) has one task between.
       for (int r = 0; r < NBc; r++) trsm_prev[r] = trsm_top[r];
-      for (int r = c + 1; r < NBc; r++) {
+      if (c + 1 < NBc) {
+        const int r = c + 1, rT = r * T;
+        Task t = make_task(T_LA);
+        t.m = bw(r);
+        t.n = bc;
+        t.k = bc;
+        t.a = opnd(B_X, blk + (int64_t)cT * nj + rT, nj);
+        t.b = Mcc;
+        t.c = opnd(B_X, blk + (int64_t)rT * nj + rT, nj);
+        int id = B.add(t, {lv, c, 1, (int)k, c, r}, -1, 11.0);
+        B.wait_task(id, pot);
+        if (c > 0) {
+          B.wait_task(id, last_top[(size_t)r * NBc + c]);
+          B.wait_task(id, last_top[(size_t)r * NBc + r]);
+        }
+        trsm_top[r].id = B.early_signal(id, 7.0);
+        trsm_top[r].group = true;
+        last_top[(size_t)r * NBc + r] = id;
+      }
+      for (int r = c + 2; r < NBc; r++) {
         const int rT = r * T;
         Operand pr = opnd(B_X, blk + (int64_t)cT * nj + rT, nj);
         Task t = gemm(bw(r), bc, bc, 1.0, pr, Mcc, 0.0, pr);
         int id = B.add(t, {lv, c, 1, (int)k, c, r});
         B.wait_task(id, pot);
         if (c > 0) B.wait_task(id, last_top[(size_t)r * NBc + c]);
-        trsm_top[r] = id;
+        trsm_top[r].id = id;
+        trsm_top[r].group = false;
       }
       // TRSM of the bottom tiles into S_k
       for (int i = 0; i < NBb; i++) {
@@ -153,7 +186,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
           t.aux[3] = (int32_t)(moff >> 32);
           int id = B.add(t, {lv, c, 3, (int)k, j, 0});
           B.wait_task(id, pot);
-          B.wait_task(id, trsm_prev[c]);
+          wait_dep(id, trsm_prev[c]);
           if (c - 1 > j) B.wait_task(id, last_mrow[j]);
           last_mrow[j] = id;
         }
@@ -163,13 +196,14 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         const int jT = j * T;
         Operand pj = opnd(B_X, blk + (int64_t)cT * nj + jT, nj);
         for (int r = j; r < NBc; r++) {
+          if (r == c + 1 && j == c + 1) continue;  // done by the look-ahead task
           const int rT = r * T;
           Operand pr = opnd(B_X, blk + (int64_t)cT * nj + rT, nj);
           Operand cc = opnd(B_X, blk + (int64_t)jT * nj + rT, nj);
           Task t = gemm(bw(r), bw(j), bc, -1.0, pr, pj, 1.0, cc, r == j, 0);
           int id = B.add(t, {lv, c, 2, (int)k, j, r});
-          B.wait_task(id, trsm_top[r]);
-          B.wait_task(id, trsm_top[j]);
+          wait_dep(id, trsm_top[r]);
+          wait_dep(id, trsm_top[j]);
           if (c > 0) B.wait_task(id, last_top[(size_t)r * NBc + j]);
           last_top[(size_t)r * NBc + j] = id;
         }
@@ -180,7 +214,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
           Task t = gemm(bh(i), bw(j), bc, -1.0, sa, pj, 1.0, cc);
           int id = B.add(t, {lv, c, 2, (int)k, j, NBc + i});
           B.wait_task(id, trsmb[i]);
-          B.wait_task(id, trsm_top[j]);
+          wait_dep(id, trsm_top[j]);
           if (c > 0) B.wait_task(id, last_bot[(size_t)i * NBc + j]);
           last_bot[(size_t)i * NBc + j] = id;
         }

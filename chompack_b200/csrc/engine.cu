@@ -249,15 +249,38 @@ __device__ void store_acc(double* __restrict__ C, int ldc, int m, int n, bool lo
 }
 
 // ------------------------------------------------------------------ GEMM
-__device__ void run_gemm(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
-  const Opnd A = make_opnd(ra, t.a), B = make_opnd(ra, t.b);
-  double* C = ra.bases[t.c.base] + t.c.off;
-  const int ldc = t.c.ld, m = t.m, n = t.n, K = t.k, cdiag = t.cdiag;
-  const bool lower = t.cmode == CM_LOWER;
-  const double alpha = t.alpha, beta = t.beta;
-  Acc acc;
-  gemm_acc(A, B, m, n, K, sm, acc);
-  store_acc(C, ldc, m, n, lower, cdiag, alpha, beta, acc);
+// GEMM task (T_GEMM), and the look-ahead step of the blocked Cholesky
+// (T_LA) as two passes through the same code.  T_LA, with the next diagonal
+// tile D (operand c, m x m, lower part), the tile A below the current
+// diagonal block (operand a, m x n, overwritten) and M = L_cc^{-1} (operand
+// b, read as lower-triangular):
+//   pass 0: L = A M^T -> A;  early signal (aux[3] - 1, when aux[3] > 0)
+//   pass 1: D -= L L^T (lower part), L read back from L2
+// Both passes share one inlined copy of the GEMM code: a second copy (or a
+// call) makes the persistent kernel spill.
+__device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
+  const bool la = t.op == T_LA;
+  const int passes = la ? 2 : 1;
+  for (int ph = 0; ph < passes; ph++) {
+    const Operand& ob = (la && ph == 1) ? t.a : t.b;
+    const Operand& oc = (la && ph == 0) ? t.a : t.c;
+    const Opnd A = make_opnd(ra, t.a), B = make_opnd(ra, ob);
+    const int m = t.m, n = (la && ph == 1) ? t.m : t.n, K = (la && ph == 1) ? t.n : t.k;
+    const bool lower = la ? ph == 1 : t.cmode == CM_LOWER;
+    const int cdiag = la ? 0 : t.cdiag;
+    const double alpha = la ? (ph == 0 ? 1.0 : -1.0) : t.alpha;
+    const double beta = la ? (ph == 0 ? 0.0 : 1.0) : t.beta;
+    Acc acc;
+    gemm_acc(A, B, m, n, K, sm, acc);
+    store_acc(ra.bases[oc.base] + oc.off, oc.ld, m, n, lower, cdiag, alpha, beta, acc);
+    if (la && ph == 0) {
+      __syncthreads();
+      if (threadIdx.x == 0 && t.aux[3] > 0) {
+        __threadfence();
+        red_release_add(ra.counters + (t.aux[3] - 1), 1);
+      }
+    }
+  }
 }
 
 // C = alpha * M2 * (opA * opB^T), M2 = lower-triangular m x m tile (operand
@@ -413,19 +436,32 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
       double a[16];
 #pragma unroll
       for (int c = 0; c < 16; c++) a[c] = sL[(j0 + c) * LD + j0 + il];
+      // The pivot column goes to the other lanes through shared memory (one
+      // store per lane, then broadcast loads): fifteen double shuffles per
+      // pivot are throughput-bound and cost 2.5x more on this part.
+      // The next pivot, a(jj+1, jj+1) - l(jj+1, jj)^2, is formed by lane
+      // jj+1 from its own values right after its multiplier, so the chain
+      // from pivot to pivot is shuffle -> rsqrt -> multiply -> FMA and the
+      // broadcast and the other updates run beside it.
+      double* colb = sT;  // free until the inverse assembly: 2 x 16 doubles
+      double dn = a[0];
 #pragma unroll
       for (int jj = 0; jj < 16; jj++) {
-        const double d = __shfl_sync(0xffffffffu, a[jj], jj);
+        const double d = __shfl_sync(0xffffffffu, dn, jj);
         const bool bad = !(d > 0.0);
         if (bad && lane == 0 && j0 + jj < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + jj + 1);
         const double x = bad ? 1.0 : d;
         const double rs = rsqrt(x);
-        a[jj] = (il == jj) ? x * rs : ((il > jj) ? a[jj] * rs : a[jj]);
+        const double l = (il == jj) ? x * rs : a[jj] * rs;
+        a[jj] = (il >= jj) ? l : a[jj];
+        if (jj + 1 < 16) dn = fma(-l, l, a[jj + 1]);
         if (lane == jj) rdiag[j0 + jj] = rs;
+        if (lane < 16) colb[16 * (jj & 1) + il] = l;
+        __syncwarp();
 #pragma unroll
         for (int kk = jj + 1; kk < 16; kk++) {
-          const double lkj = __shfl_sync(0xffffffffu, a[jj], kk);
-          if (il >= kk) a[kk] -= a[jj] * lkj;
+          const double lkj = colb[16 * (jj & 1) + kk];
+          if (il >= kk) a[kk] = fma(-l, lkj, a[kk]);
         }
       }
       if (lane < 16) {
@@ -437,15 +473,19 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
       __syncwarp();
       POTRF_STAMP(1);
       // inverse of the block: lane c < 16 holds column c,
-      // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c)
-      double m[16];
+      // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c),
+      // right-looking: as soon as M(l, c) is known it is added into the
+      // partial sums of all later rows, so the dependent chain per row is
+      // one multiply and one FMA (FP64 latency, not the row's dot product)
+      double m[16], sacc[16];
 #pragma unroll
-      for (int r = 0; r < 16; r++) {
-        double sacc = 0.0;
+      for (int r = 0; r < 16; r++) sacc[r] = 0.0;
 #pragma unroll
-        for (int l = 0; l < r; l++) sacc += sL[(j0 + l) * LD + j0 + r] * m[l];
-        const double rd = rdiag[j0 + r];
-        m[r] = (r == il) ? rd : ((r > il) ? -rd * sacc : 0.0);
+      for (int l = 0; l < 16; l++) {
+        const double rd = rdiag[j0 + l];
+        m[l] = (l == il) ? rd : ((l > il) ? -rd * sacc[l] : 0.0);
+#pragma unroll
+        for (int r = l + 1; r < 16; r++) sacc[r] = fma(sL[(j0 + l) * LD + j0 + r], m[l], sacc[r]);
       }
       if (lane < 16) {
 #pragma unroll
@@ -1021,7 +1061,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     __syncthreads();
     if (s_abort) break;
     switch (t.op) {
-      case T_GEMM: run_gemm(ra, t, sm); break;
+      case T_GEMM:
+      case T_LA: run_gemm_or_la(ra, t, sm); break;
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem); break;
       case T_ASM: run_asm(ra, t); break;

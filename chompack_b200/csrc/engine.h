@@ -13,6 +13,12 @@
 
 #include <vector_types.h>  // int2
 
+#ifdef __CUDACC__
+#define CHB_HD __host__ __device__
+#else
+#define CHB_HD
+#endif
+
 namespace chb {
 
 constexpr int TILE = 64;          // tile edge (rows/cols of a C tile)
@@ -29,7 +35,7 @@ constexpr int ENGINE_SMEM_BASE_DOUBLES = 9472;
 constexpr int ENGINE_SMEM_DOUBLES = 14336;
 // Shared-memory doubles a Householder panel of h rows and nb columns needs
 // (panel, then its nb x nb T factor, plus scalars).
-constexpr int ql_panel_doubles(int h, int nb) { return h * nb + nb * nb + 192; }
+CHB_HD constexpr int ql_panel_doubles(int h, int nb) { return h * nb + nb * nb + 192; }
 
 // Base-pointer slots a task operand refers to.
 enum Base : uint8_t {
@@ -68,7 +74,8 @@ enum TaskOp : uint8_t {
   T_RPOTRF = 7,   // "reverse" Cholesky: S = L^T L with L lower (diag tile)
   T_QL = 8,       // blocked Householder QL of update_factor (sub-op aux[3])
   T_VEC = 9,      // vector ops for the triangular solve sweep
-  T_NOP = 10      // no work: joins dependencies
+  T_NOP = 10,     // no work: joins dependencies
+  T_LA = 11       // Cholesky look-ahead: L = A21 M^T (early signal), A22 -= L L^T
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the

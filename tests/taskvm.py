@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_QL, T_VEC, T_NOP = 8, 9, 10
+T_QL, T_VEC, T_NOP, T_LA = 8, 9, 10, 11
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -153,6 +153,13 @@ class VM(object):
             self._ql(t)
         elif op == T_NOP:
             pass
+        elif op == T_LA:  # L = A M^T -> A; D -= tril(L L^T)
+            m, n, K = int(t["m"]), int(t["n"]), int(t["k"])
+            A = _operand(self.bases[int(t["a"]["base"])], t["a"], m, K)
+            Mt = _operand(self.bases[int(t["b"]["base"])], t["b"], n, K)
+            L = A @ Mt.T
+            _store(self.bases[int(t["a"]["base"])], t["a"], m, n, L, False, 0, 0.0)
+            _store(self.bases[int(t["c"]["base"])], t["c"], m, m, -(L @ L.T), True, 0, 1.0)
         elif op == T_COPY:
             m, n = int(t["m"]), int(t["n"])
             fl = int(t["aux"][0])
@@ -387,7 +394,8 @@ class VM(object):
             ready[j] = ready[-1]
             ready.pop()
             order.append(i)
-            for cid in (i, int(tasks[i]["group"])):
+            early = int(tasks[i]["aux"][3]) - 1 if int(tasks[i]["op"]) == T_LA else -1
+            for cid in (i, int(tasks[i]["group"]), early):
                 if cid < 0:
                     continue
                 counters[cid] += 1
