@@ -12,7 +12,8 @@
 //   U_c = F[r_c, r_c] for every child c      (:62-71)
 //   blk = [Y11 (lower, upper zeroed); S21]   (:36-38, :73)
 // M is built tile-wise: inverses of the 64x64 diagonal tiles (independent)
-// and the block rows below them (M(c, j) = -M_cc sum_l L(c, l) M(l, j)).
+// and, right-looking, the tiles below them (M(c, j) = -M_cc sum_l L(c, l)
+// M(l, j), the sum accumulated as the M(l, j) become final).
 // Y11 and S21 live in scratch until every reader of the factor block is done,
 // then are copied back into blkval.
 #include "dag.h"
@@ -38,7 +39,15 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       ws += (int64_t)f.na * f.nn;
     }
   }
-  prog.ws_doubles = ws;
+  // split-K scratch, handed out as the long-K tiles are built
+  const int KSPLIT = 384;
+  auto scratch = [&ws](int K, int kc) {
+    const int p = split_count(K, kc);
+    if (p == 1) return (int64_t)0;
+    const int64_t o = ws;
+    ws += (int64_t)p * TILE * TILE;
+    return o;
+  };
 
   // group: the parent's extract tasks that produce V_k (k non-root)
   std::vector<int> vready(N, -1);
@@ -69,33 +78,41 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       t.aux[2] = 1;  // invert only
       inv[c] = B.add(t, {lv, 0, 0, (int)k, c, 0});
     }
-    // block rows of M below the diagonal tiles
-    last_mrow.assign(NBc, -1);
-    for (int c = 1; c < NBc; c++) {
-      const int cT = c * T;
-      for (int j = 0; j < c; j++) {
-        const int jT = j * T;
-        Task t = make_task(T_MROW);
-        t.m = bw(c);
-        t.n = T;
-        t.k = cT - jT;
-        t.alpha = -1.0;
-        t.a = opnd(B_X, blk + (int64_t)jT * nj + cT, nj);
-        t.b = opnd(B_WS, M + (int64_t)jT * nn + jT, nn, OM_TRI_T, 0);
-        t.c = opnd(B_WS, M + (int64_t)jT * nn + cT, nn);
-        const int64_t moff = M + (int64_t)cT * nn + cT;
-        t.aux[0] = B_WS;
-        t.aux[1] = nn;
-        t.aux[2] = (int32_t)(uint32_t)(moff & 0xffffffffLL);
-        t.aux[3] = (int32_t)(moff >> 32);
-        int id = B.add(t, {lv, 1, c, (int)k, j, 0});
+    // M below the diagonal tiles, right-looking by block column j: as soon
+    // as M(l, j) is final, T(c, j) += L(c, l) M(l, j) for every c > l
+    // (accumulated in place at M(c, j)); then M(l+1, j) = -M_{l+1} T(l+1, j).
+    // The chain per column is two 64x64 tiles per block row.
+    std::vector<int> fin((size_t)NBc * NBc, -1);  // last writer of M(c, j)
+    for (int j = 0; j < NBc; j++) {
+      const int jT = j * T;
+      fin[(size_t)j * NBc + j] = inv[j];
+      for (int l = j; l + 1 < NBc; l++) {
+        const int lT = l * T;
+        for (int c = l + 1; c < NBc; c++) {
+          const int cT = c * T;
+          Operand a = opnd(B_X, blk + (int64_t)lT * nj + cT, nj);          // L(c, l)
+          Operand b = opnd(B_WS, M + (int64_t)jT * nn + lT, nn, OM_T, 0);  // M(l, j)^T
+          Operand cc = opnd(B_WS, M + (int64_t)jT * nn + cT, nn);          // T(c, j)
+          Task t = gemm(bw(c), bw(j), bw(l), 1.0, a, b, l == j ? 0.0 : 1.0, cc);
+          int id = B.add(t, {lv, 1, l, (int)k, j, c});
+          B.wait_task(id, fin[(size_t)l * NBc + j]);
+          if (l > j) B.wait_task(id, fin[(size_t)c * NBc + j]);
+          fin[(size_t)c * NBc + j] = id;
+        }
+        const int c = l + 1, cT = c * T;
+        Operand a = opnd(B_WS, M + (int64_t)cT * nn + cT, nn);            // M_cc (lower)
+        Operand b = opnd(B_WS, M + (int64_t)jT * nn + cT, nn, OM_T, 0);   // T(c, j)^T
+        Operand cc = opnd(B_WS, M + (int64_t)jT * nn + cT, nn);
+        Task t = gemm(bw(c), bw(j), bw(c), -1.0, a, b, 0.0, cc);
+        int id = B.add(t, {lv, 1, c, (int)k, j, c});
         B.wait_task(id, inv[c]);
-        B.wait_task(id, inv[j]);
-        if (c - 1 > j) B.wait_task(id, last_mrow[j]);
-        last_mrow[j] = id;
+        B.wait_task(id, fin[(size_t)c * NBc + j]);
+        fin[(size_t)c * NBc + j] = id;
       }
     }
-    // Y11 = M^T M (lower tiles)
+    last_mrow.assign(NBc, -1);
+    for (int j = 0; j < NBc; j++) last_mrow[j] = fin[(size_t)(NBc - 1) * NBc + j];
+    // Y11 = M^T M (lower tiles), long K split
     std::vector<int> y11(NBc * NBc, -1);
     for (int i = 0; i < NBc; i++) {
       for (int j = 0; j <= i; j++) {
@@ -104,18 +121,20 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         Operand b = opnd(B_WS, M + (int64_t)jT * nn + iT, nn, i == j ? OM_TRI_T : OM_T, 0);
         Operand c = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
         Task t = gemm(bw(i), bw(j), nn - iT, 1.0, a, b, 0.0, c, i == j, 0);
-        int id = B.add(t, {lv, 2, 0, (int)k, j, i});
-        B.wait_task(id, inv[i]);
-        B.wait_task(id, inv[j]);
-        if (i < NBc - 1) B.wait_task(id, last_mrow[i]);
-        if (j < NBc - 1) B.wait_task(id, last_mrow[j]);
-        y11[i * NBc + j] = id;
+        SplitTask st = add_split_gemm(B, t, KSPLIT, scratch(t.k, KSPLIT), {lv, 2, 0, (int)k, j, i});
+        for (int id : st.parts) {
+          B.wait_task(id, inv[i]);
+          B.wait_task(id, inv[j]);
+          B.wait_task(id, last_mrow[i]);
+          B.wait_task(id, last_mrow[j]);
+        }
+        y11[i * NBc + j] = st.out;
       }
     }
     const int yfinal = B.new_group();
     const int sgroup = na > 0 ? B.new_group() : -1;
     if (na > 0) {
-      // S21 = -V_k W
+      // S21 = -V_k W (long K split)
       for (int i = 0; i < NBb; i++) {
         for (int j = 0; j < NBc; j++) {
           const int iT = i * T, jT = j * T;
@@ -123,11 +142,11 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           Operand b = opnd(B_X, blk + (int64_t)jT * nj + nn, nj, OM_T, 0);
           Operand c = opnd(B_WS, S + (int64_t)jT * na + iT, na);
           Task t = gemm(bh(i), bw(j), na, -1.0, a, b, 0.0, c);
-          int id = B.add(t, {lv, 3, 0, (int)k, j, i}, sgroup);
-          B.wait_group(id, vready[k]);
+          SplitTask st = add_split_gemm(B, t, KSPLIT, scratch(t.k, KSPLIT), {lv, 3, 0, (int)k, j, i}, sgroup);
+          for (int id : st.parts) B.wait_group(id, vready[k]);
         }
       }
-      // Y11 -= S21^T W
+      // Y11 -= S21^T W (long K split)
       for (int i = 0; i < NBc; i++) {
         for (int j = 0; j <= i; j++) {
           const int iT = i * T, jT = j * T;
@@ -135,9 +154,9 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           Operand b = opnd(B_X, blk + (int64_t)jT * nj + nn, nj, OM_T, 0);
           Operand c = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
           Task t = gemm(bw(i), bw(j), na, -1.0, a, b, 1.0, c, i == j, 0);
-          int id = B.add(t, {lv, 4, 0, (int)k, j, i}, yfinal);
-          B.wait_task(id, y11[i * NBc + j]);
-          B.wait_group(id, sgroup);
+          SplitTask st = add_split_gemm(B, t, KSPLIT, scratch(t.k, KSPLIT), {lv, 4, 0, (int)k, j, i}, yfinal);
+          for (int id : st.parts) B.wait_group(id, sgroup);
+          B.wait_task(st.out, y11[i * NBc + j]);
         }
       }
     } else {
@@ -205,6 +224,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       }
     }
   }
+  prog.ws_doubles = ws;
   return B.finish(prog, P.grid > 0 ? P.grid : 296);
 }
 

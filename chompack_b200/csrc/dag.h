@@ -95,14 +95,16 @@ struct DagBuilder {
   // Rough duration model of a task on one CTA (microseconds); only the
   // relative sizes matter for the priority order.
   static double estimate(const Task& t) {
+    // fitted to per-task traces of the 40^3 sweeps on B200
+    const double mnk = (double)t.m * t.n * t.k / (64.0 * 64.0 * 64.0);
     switch (t.op) {
-      case T_GEMM:
-      case T_MROW:
-        return 3.0 + 4.5 * ((double)t.m * t.n * t.k) / (64.0 * 64.0 * 64.0) + (t.op == T_MROW ? 5.0 : 0.0);
-      case T_POTRF:  // measured on B200: ~46 us for a full 64x64 tile, nearly flat in m
-        return 8.0 + 0.6 * t.m;
-      default:
-        return 4.0;
+      case T_GEMM: return 3.0 + 6.0 * mnk;
+      case T_MROW: return 11.0 + 6.0 * mnk;
+      case T_LA: return 15.0;
+      case T_POTRF: return t.aux[2] ? 11.0 : 27.0;  // invert-only : factor + inverse
+      case T_SUM: return 3.0 + 0.5 * t.aux[0];
+      case T_COPY: return 3.5;
+      default: return 6.0;
     }
   }
 
@@ -244,6 +246,18 @@ struct DagBuilder {
   }
 };
 
+// An operand advanced by k0 along its K dimension.
+inline Operand shift_k(Operand o, int k0) {
+  switch (o.mode) {
+    case OM_N: o.off += (int64_t)k0 * o.ld; break;
+    case OM_T: o.off += k0; break;
+    case OM_TRI_N: o.off += (int64_t)k0 * o.ld; o.diag -= k0; break;
+    case OM_TRI_T: o.off += k0; o.diag += k0; break;
+    default: o.pad2 += k0; break;  // OM_SYM: column offset of k = 0
+  }
+  return o;
+}
+
 inline Operand opnd(uint8_t base, int64_t off, int ld, uint8_t mode = OM_N, int diag = 0) {
   Operand o;
   std::memset(&o, 0, sizeof(o));
@@ -282,5 +296,63 @@ inline Task gemm(int m, int n, int k, double alpha, const Operand& a, const Oper
 }
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+}  // namespace chb
+
+namespace chb {
+
+// A GEMM task split along K into chunks of at most kc: the partial products
+// (parts, independent) go to scratch tiles (64 x 64, ld 64, 4096 doubles
+// apart, at WS offset `scratch`), and one T_SUM task (`out`) folds them into
+// C with the task's alpha, beta and mask.  Waits on the inputs belong on
+// every part, waits on C's previous writer on `out` only.  With K <= kc the
+// task is emitted as is (parts = {out}).
+struct SplitTask {
+  std::vector<int> parts;
+  int out;
+};
+
+inline int split_count(int K, int kc) { return K > kc ? (K + kc - 1) / kc : 1; }
+
+inline SplitTask add_split_gemm(DagBuilder& B, const Task& t, int kc, int64_t scratch, const SchedKey& key,
+                                int group = -1) {
+  SplitTask st;
+  const int p = split_count(t.k, kc);
+  if (p == 1) {
+    st.out = B.add(t, key, group);
+    st.parts.push_back(st.out);
+    return st;
+  }
+  const int chunk = (t.k + p - 1) / p;
+  for (int q = 0; q < p; q++) {
+    const int k0 = q * chunk, kq = std::min(chunk, t.k - k0);
+    Task u = t;
+    u.k = kq;
+    u.a = shift_k(t.a, k0);
+    u.b = shift_k(t.b, k0);
+    u.alpha = 1.0;
+    u.beta = 0.0;
+    u.cmode = CM_FULL;
+    u.cdiag = 0;
+    u.c = opnd(B_WS, scratch + (int64_t)q * TILE * TILE, TILE);
+    SchedKey kk = key;
+    kk.rank = key.rank * 64 + q;
+    st.parts.push_back(B.add(u, kk));
+  }
+  Task s = make_task(T_SUM);
+  s.m = t.m;
+  s.n = t.n;
+  s.alpha = t.alpha;
+  s.beta = t.beta;
+  s.cmode = t.cmode;
+  s.cdiag = t.cdiag;
+  s.a = opnd(B_WS, scratch, TILE);
+  s.c = t.c;
+  s.aux[0] = p;
+  s.aux[1] = TILE * TILE;
+  st.out = B.add(s, key, group, 2.0 + 0.4 * p);
+  for (int id : st.parts) B.wait_task(st.out, id);
+  return st;
+}
 
 }  // namespace chb

@@ -283,6 +283,43 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
   }
 }
 
+// Reduction of split-K partial products (T_SUM): C = alpha * sum_q P_q +
+// beta * C over the m x n tile (masked to r + cdiag >= c when cmode is
+// CM_LOWER), P_q at a.off + q * aux[1] (ld a.ld), q = 0 .. aux[0]-1 added in
+// order, so the result does not depend on the schedule.
+__device__ void run_sum(const RunArgs& ra, const Task& t) {
+  const double* __restrict__ P = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+  const int ldp = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n, np = t.aux[0];
+  const int64_t stride = (int64_t)(uint32_t)t.aux[1];
+  const bool lower = t.cmode == CM_LOWER;
+  constexpr int E = TILE * TILE / NTHREADS / 2;  // elements per thread and half
+  // a thread's elements of one partial are loaded together (E loads in
+  // flight), partial after partial; two halves keep the registers in check
+#pragma unroll 1
+  for (int half = 0; half < 2; half++) {
+    double acc[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) acc[e] = 0.0;
+    for (int q = 0; q < np; q++) {
+      const double* Pq = P + q * stride;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
+        if (r < m && c < n) acc[e] += __ldcg(Pq + (int64_t)c * ldp + r);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
+      if (r >= m || c >= n || (lower && r + t.cdiag < c)) continue;
+      double v = t.alpha * acc[e];
+      if (t.beta != 0.0) v += t.beta * __ldcg(C + (int64_t)c * ldc + r);
+      C[(int64_t)c * ldc + r] = v;
+    }
+  }
+}
+
 // C = alpha * M2 * (opA * opB^T), M2 = lower-triangular m x m tile (operand
 // `c` of the task holds C; M2 is described by aux: base aux[0], ld aux[1],
 // offset (aux[2] | aux[3] << 32)).
@@ -1071,6 +1108,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_VEC: run_vec(ra, t); break;
       case T_QL: run_ql(ra, t, smem); break;
       case T_NOP: break;
+      case T_SUM: run_sum(ra, t); break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;

@@ -75,7 +75,8 @@ enum TaskOp : uint8_t {
   T_QL = 8,       // blocked Householder QL of update_factor (sub-op aux[3])
   T_VEC = 9,      // vector ops for the triangular solve sweep
   T_NOP = 10,     // no work: joins dependencies
-  T_LA = 11       // Cholesky look-ahead: L = A21 M^T (early signal), A22 -= L L^T
+  T_LA = 11,      // Cholesky look-ahead: L = A21 M^T (early signal), A22 -= L L^T
+  T_SUM = 12      // C = alpha * sum of aux[0] partial tiles (stride aux[1]) + beta * C
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the

@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_QL, T_VEC, T_NOP, T_LA = 8, 9, 10, 11
+T_QL, T_VEC, T_NOP, T_LA, T_SUM = 8, 9, 10, 11, 12
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -153,6 +153,16 @@ class VM(object):
             self._ql(t)
         elif op == T_NOP:
             pass
+        elif op == T_SUM:  # C = alpha * sum_q P_q + beta * C (in order)
+            m, n, p, stride = int(t["m"]), int(t["n"]), int(t["aux"][0]), int(t["aux"][1])
+            Pb, Po, ldp = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
+            r = np.arange(m)[:, None]
+            c = np.arange(n)[None, :]
+            acc = np.zeros((m, n))
+            for q in range(p):
+                acc = acc + Pb[Po + q * stride + c * ldp + r]
+            _store(self.bases[int(t["c"]["base"])], t["c"], m, n, float(t["alpha"]) * acc,
+                   int(t["cmode"]) == 1, int(t["cdiag"]), float(t["beta"]))
         elif op == T_LA:  # L = A M^T -> A; D -= tril(L L^T)
             m, n, K = int(t["m"]), int(t["n"]), int(t["k"])
             A = _operand(self.bases[int(t["a"]["base"])], t["a"], m, K)
