@@ -312,11 +312,10 @@ def main():
         dist.barrier()
     elapsed = t0.elapsed_time(t1) / 1e3
     kern = {op: float(np.mean([a.elapsed_time(b) for a, b in ev_k[op]])) / 1e3 for op in ops}
-    if world > 1:
-        tt = torch.tensor([elapsed] + [kern[o] for o in ops], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt[0])
-        kern = {o: float(tt[1 + i]) for i, o in enumerate(ops)}
+    # the job ends with the slowest rank (chompack_b200.shard, NCCL here)
+    from chompack_b200 import shard
+    elapsed = shard.max_over_ranks(elapsed, device=dev)
+    kern = {o: shard.max_over_ranks(kern[o], device=dev) for o in ops}
     value = step_flops * args.steps * world / elapsed / 1e9
 
     # the other drop-in sweeps of the workload, timed alone after the step
