@@ -842,7 +842,27 @@ __device__ __forceinline__ double block_reduce_sum(double v, double* red) {
 //   T  (operand c, nb x nb lower, ld c.ld): H_{c0} ... H_{c1-1} = I - W' T W'^T
 //     (LAPACK dlarft 'B','C': T(i,i) = tau_i,
 //      T(i+1:, i) = -tau_i T(i+1:, i+1:) W'(:, i+1:)^T w'_i).
+// Phase timing for development builds (-DCHB_PROFILE_QL); compiled out
+// otherwise.
+#ifdef CHB_PROFILE_QL
+__device__ unsigned long long g_ql_phase[12];
+#define QL_STAMP(i)                                                  \
+  do {                                                               \
+    __syncthreads();                                                 \
+    long long now_ = clock64();                                      \
+    if (threadIdx.x == 0) atomicAdd(&g_ql_phase[i], now_ - qstamp_); \
+    qstamp_ = now_;                                                  \
+  } while (0)
+#else
+#define QL_STAMP(i) \
+  do {              \
+  } while (0)
+#endif
+
 __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
+#ifdef CHB_PROFILE_QL
+  long long qstamp_ = clock64();
+#endif
   const FrontDesc ch = ra.fronts[t.aux[0]];
   const FrontDesc f = ra.fronts[ch.parent];
   const int N = ch.na, nn = f.nn, na = f.na;
@@ -851,7 +871,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
   while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < nn) lo = mid + 1; else hi = mid; }
   const int N1 = lo, N2 = N - N1;
   const int c0 = t.aux[1], c1 = t.aux[2];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   if (t.aux[3] == QL_GATHER) {
     const double* __restrict__ Lk = ra.bases[t.a.base] + t.a.off;
     double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
@@ -885,6 +905,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
     P[idx] = __ldcg(C + (int64_t)(c0 + pc) * ldc + row0 + q);
   }
   __syncthreads();
+  QL_STAMP(0);
   for (int i = 0; i < nb; i++) {
     const int col = c1 - 1 - i, pc = col - c0;
     const int lr0 = __ldg(r + N1 + col) - nn - row0;   // first row of x (local)
@@ -895,6 +916,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
       double part = 0.0;
       for (int q = lr0 + tid; q < lp; q += NTHREADS) part += pv[q] * pv[q];
       const double xn2 = block_reduce_sum(part, red);
+      QL_STAMP(5);
       if (xn2 != 0.0) {
         const double alpha = pv[lp];
         // dlapy2(alpha, ||x||)
@@ -907,17 +929,48 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
         __syncthreads();  // everyone has read pv[lp] and the norm
         for (int q = lr0 + tid; q < lp; q += NTHREADS) pv[q] *= scal;
         __syncthreads();
-        // H = I - tau v v^T on the panel columns to the left, rows [lr0, lp]
-        for (int q2 = warp; q2 < pc; q2 += NTHREADS / 32) {
-          double* cq = P + q2 * h;
-          double s = 0.0;
-          for (int q = lr0 + lane; q < lp; q += 32) s += pv[q] * cq[q];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          s = tau * (s + cq[lp]);
-          for (int q = lr0 + lane; q < lp; q += 32) cq[q] -= pv[q] * s;
-          if (lane == 0) cq[lp] -= s;
+        QL_STAMP(6);
+        // H = I - tau v v^T on the panel columns to the left, rows [lr0, lp]:
+        // w_q = tau v^T C(:, q) with a group of tpc threads per column (row
+        // slices, two partial sums, shuffle reduction inside the group), then
+        // C -= v w^T over all (row, column) pairs
+        double* wq = G;  // G is unused until the reflections are done
+        int tpc = 32;
+        while (tpc > 1 && tpc * pc > NTHREADS) tpc >>= 1;
+        {
+          const int q2 = tid / tpc, sub = tid % tpc;
+          double s0 = 0.0, s1 = 0.0;
+          if (q2 < pc) {
+            const double* cq = P + q2 * h;
+            int q = lr0 + sub;
+            for (; q + tpc < lp; q += 2 * tpc) {
+              s0 = fma(pv[q], cq[q], s0);
+              s1 = fma(pv[q + tpc], cq[q + tpc], s1);
+            }
+            if (q < lp) s0 = fma(pv[q], cq[q], s0);
+            if (sub == 0) s1 += cq[lp];
+          }
+          double s = s0 + s1;
+          for (int o = tpc >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          if (q2 < pc && sub == 0) wq[q2] = tau * s;
         }
+        __syncthreads();
+        QL_STAMP(7);
+        // rows on R lanes (the smallest power of two covering the reflector),
+        // columns on NTHREADS / R groups: no division per element
+        const int len = lp - lr0 + 1;
+        int R = 1;
+        while (R < len && R < NTHREADS) R <<= 1;
+        {
+          const int rl = tid % R, cg = tid / R, ncg = NTHREADS / R;
+          for (int q = lr0 + rl; q <= lp; q += R) {
+            const double vq = (q == lp) ? 1.0 : pv[q];
+#pragma unroll 4
+            for (int q2 = cg; q2 < pc; q2 += ncg) P[q2 * h + q] = fma(-vq, wq[q2], P[q2 * h + q]);
+          }
+        }
+        __syncthreads();
+        QL_STAMP(8);
         if (tid == 0) pv[lp] = beta;
       }
     }
@@ -928,6 +981,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
     }
     __syncthreads();
   }
+  QL_STAMP(1);
   // the panel back to C, then W' (explicit reflectors) in its place
   for (int idx = tid; idx < h * nb; idx += NTHREADS) {
     const int q = idx % h, pc = idx / h;
@@ -943,27 +997,64 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
     W[(int64_t)(c0 + i) * ldw + row0 + q] = v;
   }
   __syncthreads();
-  // G(a, b) = w'_a^T w'_b for a > b (w'_i is panel column nb - 1 - i)
-  for (int pr = warp; pr < nb * nb; pr += NTHREADS / 32) {
-    const int a = pr % nb, b = pr / nb;
-    if (a <= b) continue;
-    const double* wa = P + (nb - 1 - a) * h;
-    const double* wb = P + (nb - 1 - b) * h;
-    const int q0 = max(lr0s[a], lr0s[b]), q1 = min(lr0s[64 + a], lr0s[64 + b]);
-    double s = 0.0;
-    for (int q = q0 + lane; q <= q1; q += 32) s += wa[q] * wb[q];
+  QL_STAMP(2);
+  // G(a, b) = w'_a^T w'_b for a > b (w'_i is panel column nb - 1 - i):
+  // each thread a 4 x 4 block of G over all rows (8 loads feed 16 FMAs, no
+  // cross-lane reductions)
+  {
+    const int nbb = (nb + 3) >> 2;
+    for (int blk = tid; blk < nbb * (nbb + 1) / 2; blk += NTHREADS) {
+      int bi = 0;
+      while ((bi + 1) * (bi + 2) / 2 <= blk) bi++;
+      const int bj = blk - bi * (bi + 1) / 2;
+      const double* wa[4];
+      const double* wb[4];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) G[b * nb + a] = s;
+      for (int x = 0; x < 4; x++) {
+        wa[x] = P + (nb - 1 - min(4 * bi + x, nb - 1)) * h;
+        wb[x] = P + (nb - 1 - min(4 * bj + x, nb - 1)) * h;
+      }
+      double acc[4][4];
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+      for (int q = 0; q < h; q++) {
+        double va[4], vb[4];
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+          va[x] = wa[x][q];
+          vb[x] = wb[x][q];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+          for (int y = 0; y < 4; y++) acc[x][y] = fma(va[x], vb[y], acc[x][y]);
+      }
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+          const int a = 4 * bi + x, b2 = 4 * bj + y;
+          if (a < nb && b2 < a) G[b2 * nb + a] = acc[x][y];
+        }
+    }
   }
   __syncthreads();
+  QL_STAMP(3);
   // T in place of G's lower part, last column first
   for (int i = nb - 1; i >= 0; i--) {
     double v = 0.0;
     const int rr = i + 1 + tid;
-    if (rr < nb) {
-      for (int s2 = i + 1; s2 <= rr; s2++) v += G[s2 * nb + rr] * G[i * nb + s2];
-      v *= -taus[i];
+    if (rr < nb) {  // two partial sums: the chain is half as long
+      double v1 = 0.0;
+      int s2 = i + 1;
+      for (; s2 + 1 <= rr; s2 += 2) {
+        v = fma(G[s2 * nb + rr], G[i * nb + s2], v);
+        v1 = fma(G[(s2 + 1) * nb + rr], G[i * nb + s2 + 1], v1);
+      }
+      if (s2 <= rr) v = fma(G[s2 * nb + rr], G[i * nb + s2], v);
+      v = -taus[i] * (v + v1);
     }
     __syncthreads();
     if (rr < nb) G[i * nb + rr] = v;
@@ -974,6 +1065,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
     const int a = idx % nb, b = idx / nb;
     Tg[(int64_t)b * ldt + a] = (a >= b) ? G[idx] : 0.0;
   }
+  QL_STAMP(4);
 }
 
 // ------------------------------------------------------- solve vectors

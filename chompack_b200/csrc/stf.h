@@ -92,6 +92,33 @@ struct Stf {
     }
     return id;
   }
+  // Accesses of a task already added to the builder (e.g. by
+  // add_split_gemm): the same inference as submit.
+  void submit_existing(int id, const std::vector<Acc>& acc) {
+    for (const Acc& a : acc) {
+      auto it = st.find(a.key);
+      if (it == st.end()) continue;
+      if (it->second.last >= 0 && it->second.last != id) B.wait_task(id, it->second.last);
+      if (a.write)
+        for (int r : it->second.readers)
+          if (r != id) B.wait_task(id, r);
+    }
+    for (const Acc& a : acc) {
+      TileState& s = st[a.key];
+      if (a.write) {
+        s.last = id;
+        s.readers.clear();
+      } else if (s.last != id) {
+        s.readers.push_back(id);
+      }
+    }
+  }
+  static std::vector<Acc> reads_only(const std::vector<Acc>& acc) {
+    std::vector<Acc> r;
+    for (const Acc& a : acc)
+      if (!a.write) r.push_back(a);
+    return r;
+  }
   // A group wait on top of the inferred ones (e.g. a child's update coming
   // from a tracked matrix of another front is handled by tiles; this is for
   // explicit groups).
@@ -369,6 +396,8 @@ inline int stf_update_factor(Stf& S, KeyGen& kg, const chb_plan& P, int c, const
       for (int t2 = 0; t2 * TILE < c0; t2++) {
         const int x0 = t2 * TILE, w = std::min(TILE, c0 - x0);
         {
+          // Z = T (W'^T C): long K (the panel's row span) is split, each
+          // part carrying the T factor (it distributes over the sum)
           std::vector<Stf::Acc> acc{Stf::W(Z, 0, t2), Stf::R(Tp, 0, 0)};
           rows_acc(acc, Wp, row0, row1 + 1, 0, false);
           rows_acc(acc, C, row0, row1 + 1, t2, false);
@@ -384,7 +413,12 @@ inline int stf_update_factor(Stf& S, KeyGen& kg, const chb_plan& P, int c, const
           t.aux[1] = TILE;
           t.aux[2] = (int32_t)(uint32_t)(Tp.off & 0xffffffffLL);
           t.aux[3] = (int32_t)(Tp.off >> 32);
-          S.submit(t, kg(0, c, t2), acc);
+          const int KS = 384;
+          const int64_t scr = split_count(h, KS) > 1 ? alloc((int64_t)split_count(h, KS) * TILE * TILE) : 0;
+          SplitTask st = add_split_gemm(S.B, t, KS, scr, kg(0, c, t2));
+          for (size_t q = 0; q < st.parts.size(); q++)
+            S.submit_existing(st.parts[q], st.parts.size() == 1 ? acc : S.reads_only(acc));
+          if (st.parts.size() > 1) S.submit_existing(st.out, {Stf::W(Z, 0, t2)});
         }
         for (int i = row0 / TILE; i <= row1 / TILE; i++) {
           const int rs = std::max(i * TILE, row0), re = std::min(i * TILE + TILE, row1 + 1);
