@@ -43,8 +43,11 @@ def sweep_flops(symb):
     pinv = nn ** 3 / 3 + nn ** 3 + 2 * na ** 2 * nn + 2 * nn ** 2 * na
     llt = na * nn ** 2 + nn * nj ** 2
     comp = na ** 3 / 3 + 2 * na ** 2 * nn + nn ** 2 * na + 2 * nn ** 3 / 3
+    hess = 4 * na ** 2 * nn + 2 * na * nn ** 2 + nj * nn ** 2 + nn ** 3 + na ** 2 * nn   # one G application
+    trsm = 2 * (nn ** 2 + 2 * na * nn)                                                   # per right-hand side
     return {"cholesky": float(chol.sum()), "projected_inverse": float(pinv.sum()), "llt": float(llt.sum()),
-            "completion": float(comp.sum())}
+            "completion": float(comp.sum()), "hessian_G": float(hess.sum()), "trsm_rhs": float(trsm.sum()),
+            "potrf_updates": float((na ** 3 / 3).sum())}
 
 
 def build_problem(side=40, merge=(32, 32), seed=0):
@@ -227,8 +230,31 @@ def cpu_baseline(s, A, budget_s=15.0):
         ref.projected_inverse(s, x)
         times.append(time.perf_counter() - t0)
     med = float(np.median(times))
-    return {"value": round(step_flops / med / 1e9, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
-            "sample": "%d full runs of cholesky+projected_inverse (median %.1f ms)" % (len(times), med * 1e3)}
+    out = {"value": round(step_flops / med / 1e9, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
+           "sample": "%d full runs of cholesky+projected_inverse (median %.1f ms)" % (len(times), med * 1e3)}
+    # the other drop-in sweeps once each, for the same comparison
+    L = x0.copy()
+    ref.cholesky(s, L)
+    Y = L.copy()
+    ref.projected_inverse(s, Y)
+    other = {}
+
+    def once(name, fn, flops):
+        t0 = time.perf_counter()
+        fn()
+        dt = time.perf_counter() - t0
+        other[name] = {"ms": round(dt * 1e3, 2), "gflops": round(flops / dt / 1e9, 3)}
+    once("completion", lambda: ref.completion(s, Y.copy(), factored_updates=True), fl["completion"])
+    once("completion_unfactored", lambda: ref.completion(s, Y.copy(), factored_updates=False), fl["completion"])
+    once("llt", lambda: ref.llt(s, L.copy()), fl["llt"])
+    B = np.asfortranarray(np.random.default_rng(5).standard_normal((s.n, 8)))
+    once("trsm_N_nrhs8", lambda: ref.trsm(s, L, B.copy(order="F"), trans="N"), fl["trsm_rhs"] * 8)
+    U = Y * np.random.default_rng(6).standard_normal(Y.size)
+    for fu in (1, 0):
+        once("hessian_full_fu%d" % fu, lambda: ref.hessian(s, L, Y, [U.copy()], adj=None, factored_updates=bool(fu)),
+             2 * fl["hessian_G"] + (0 if fu else 2 * fl["potrf_updates"]))
+    out["other_sweeps"] = other
+    return out
 
 
 def main():
@@ -349,6 +375,44 @@ def main():
         ms = float(np.median([a.elapsed_time(b) for a, b in ts[1:]]))
         fkey = "completion" if name.startswith("completion") else name
         other[name] = {"ms": round(ms, 4), "gflops": round(fl[fkey] / ms / 1e6, 3)}
+
+    # triangular solves with 8 right-hand sides, and the full Hessian H(U)
+    # (adj=None: two passes) on one direction U, both update forms
+    def timed(fn, reps):
+        ts = []
+        for it in range(reps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            ts.append((e0, e1))
+        torch.cuda.synchronize(dev)
+        return float(np.median([a.elapsed_time(b) for a, b in ts[1:]]))
+    nrhs = 8
+    Bd = torch.randn(s.n, nrhs, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(5))
+    for tr in "NT":
+        wt, nbt = plan.workspace(N.OP_TRSM, nrhs, 1 if tr == "T" else 0)
+        Bt = Bd.t().contiguous()   # column-major n x nrhs
+        ms = timed(lambda: N.trsm(plan.handle, tr.encode(), nrhs, 1.0, Lw.data_ptr(), Bt.data_ptr(), s.n, wt, nbt, sp),
+                   reps)
+        other["trsm_%s_nrhs%d" % (tr, nrhs)] = {"ms": round(ms, 4), "gflops": round(fl["trsm_rhs"] * nrhs / ms / 1e6, 3)}
+    import ctypes
+    Ud = Yw * torch.randn(Yw.shape, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(6))
+    Uw = torch.empty_like(Ud)
+    uarr = (ctypes.c_void_p * 1)(Uw.data_ptr())
+    for fu in (1, 0):
+        for a in (0, 1):
+            plan.workspace(N.OP_HESSIAN, 1, a | fu << 2)
+        def full_hessian():
+            Uw.copy_(Ud)
+            for a in (0, 1):   # adj = inv = False first, then adj toggled (the reference's adj=None)
+                wh, nbh = plan.workspace(N.OP_HESSIAN, 1, a | fu << 2)
+                if N.hessian(plan.handle, Lw.data_ptr(), Yw.data_ptr(), uarr, 1, a, 0, fu, wh, nbh, sp) < 0:
+                    raise RuntimeError(N.last_error().decode())
+        ms = timed(full_hessian, max(2, reps // 2))
+        hf = 2 * fl["hessian_G"] + (0 if fu else 2 * fl["potrf_updates"])
+        other["hessian_full_fu%d" % fu] = {"ms": round(ms, 4), "gflops": round(hf / ms / 1e6, 3)}
 
     # end-to-end through the public API with host buffers
     e2e = None
