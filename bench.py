@@ -265,6 +265,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-other", action="store_true", help="skip the timings of the other sweeps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -348,12 +349,13 @@ def main():
     # loop (not part of the step): completion of the projected inverse the
     # step produced (both update modes) and llt of the factor
     other = {}
+    sweeps_other = not args.no_other
     Yw = Xw.clone()
     Lw = X0.blkval.clone()
     launch["cholesky"](plan.handle, Lw.data_ptr(), ws, nbytes, sp)
     Cw = torch.empty_like(Yw)
     reps = max(3, min(args.steps, 10))
-    for name, op, k, src, call in (
+    for name, op, k, src, call in () if not sweeps_other else (
             ("completion", N.OP_COMPLETION, 1, Yw, lambda w, nb: N.completion(plan.handle, Cw.data_ptr(), 1, w, nb, sp)),
             ("completion_unfactored", N.OP_COMPLETION, 0, Yw,
              lambda w, nb: N.completion(plan.handle, Cw.data_ptr(), 0, w, nb, sp)),
@@ -389,9 +391,9 @@ def main():
             ts.append((e0, e1))
         torch.cuda.synchronize(dev)
         return float(np.median([a.elapsed_time(b) for a, b in ts[1:]]))
-    nrhs = 8
+    nrhs = 8 if sweeps_other else 0
     Bd = torch.randn(s.n, nrhs, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(5))
-    for tr in "NT":
+    for tr in ("NT" if sweeps_other else ""):
         wt, nbt = plan.workspace(N.OP_TRSM, nrhs, 1 if tr == "T" else 0)
         Bt = Bd.t().contiguous()   # column-major n x nrhs
         ms = timed(lambda: N.trsm(plan.handle, tr.encode(), nrhs, 1.0, Lw.data_ptr(), Bt.data_ptr(), s.n, wt, nbt, sp),
@@ -401,7 +403,7 @@ def main():
     Ud = Yw * torch.randn(Yw.shape, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(6))
     Uw = torch.empty_like(Ud)
     uarr = (ctypes.c_void_p * 1)(Uw.data_ptr())
-    for fu in (1, 0):
+    for fu in ((1, 0) if sweeps_other else ()):
         for a in (0, 1):
             plan.workspace(N.OP_HESSIAN, 1, a | fu << 2)
         def full_hessian():
