@@ -49,6 +49,7 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
     ws += n;
     return o;
   };
+  S.alloc = alloc;  // long-K products are split
 
   // update matrices are tracked as matrices of their own
   std::vector<Mat> V(N);
@@ -82,10 +83,12 @@ int build_completion(const chb_plan& P, Program& prog, bool factored) {
         if (rc) return rc;
         continue;
       }
-      std::vector<Stf::Acc> acc = fread;
-      Stf::all(acc, V[c], true, true);
-      const int CH = 16;
+      // 64-column chunks of the child's update: each writes its own column
+      // tile, so the chunks run in parallel
+      const int CH = TILE;
       for (int q0 = 0; q0 < Nc; q0 += CH) {
+        std::vector<Stf::Acc> acc = fread;
+        for (int i = q0 / TILE; i < V[c].ntr(); i++) acc.push_back(Stf::W(V[c], i, q0 / TILE));
         Task t = make_task(T_EXTRACT);
         t.aux[0] = c;
         t.aux[1] = q0;

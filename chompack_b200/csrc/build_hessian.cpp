@@ -59,7 +59,7 @@ void right_mult(Stf& S, KeyGen& kg, const Mat& X, const Mat& Tm, bool transT) {
           acc.push_back(Stf::R(Tm, j, l));
         }
       }
-      S.submit(t, kg(i, j, 0), acc);
+      S.gemm(t, kg(i, j, 0), acc);
     }
   }
 }
@@ -88,7 +88,7 @@ void left_mult(Stf& S, KeyGen& kg, const Mat& X, const Mat& Tm, bool transT) {
           acc.push_back(Stf::R(Tm, l, i));
         }
       }
-      S.submit(t, kg(i, j, 0), acc);
+      S.gemm(t, kg(i, j, 0), acc);
     }
   }
 }
@@ -103,7 +103,7 @@ void tile_gemm(Stf& S, KeyGen& kg, const Mat& C, double alpha, double beta, bool
       std::vector<Stf::Acc> acc = reads;
       acc.push_back(Stf::W(C, i, j));
       Task t = gemm(C.th(i), C.tw(j), K, alpha, aop(i), bop(j), beta, C.op(i, j), lower && i == j, 0);
-      S.submit(t, kg(i, j, 0), acc);
+      S.gemm(t, kg(i, j, 0), acc);
     }
 }
 
@@ -158,6 +158,7 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
     ws += n;
     return o;
   };
+  S.alloc = alloc;  // long-K products are split
 
   // tracked matrices
   std::vector<Mat> L11(N), L21(N), Y11(N), Y21(N), V(N), ML(N), MF(N), MV(N);
@@ -192,22 +193,41 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
         const Mat& F11 = U11[u][k];
         const Mat& F21 = U21[u][k];
         const Mat& F22 = W[u][k];
+        // extend-add in 64-column chunks of the front (each writes its own
+        // column tiles of F11/F21 or F22, so the chunks run in parallel)
         auto extend_add = [&](bool zero) {
           kg.step++;
-          std::vector<Stf::Acc> acc;
-          Stf::all(acc, F11, true, true);
-          Stf::all(acc, F21, true);
-          Stf::all(acc, F22, true, true);
-          for (int l = f.chbeg; l < f.chend; l++) Stf::all(acc, W[u][P.chidx[l]], false, true);
-          Task t = make_task(T_ASM);
-          t.aux[0] = (int32_t)k;
-          t.aux[1] = 0;
-          t.aux[2] = nj;
-          t.aux[3] = zero ? 1 : 0;
-          t.a = opnd((uint8_t)(B_U0 + u), f.blk, nj);
-          t.c = opnd(B_WS, oW[u] + f.upd, std::max(na, 1));
-          t.off2 = oW[u];
-          S.submit(t, kg(0, 0, 0), acc, -1, 3.0 + (double)nj * nj / 4000.0);
+          std::vector<Stf::Acc> rd;
+          for (int l = f.chbeg; l < f.chend; l++) Stf::all(rd, W[u][P.chidx[l]], false, true);
+          // chunk boundaries on the tile grids of F11/F21 (from 0) and of
+          // F22 (from nn), so no two chunks write the same tile
+          std::vector<int> cuts;
+          for (int j = 0; j < nn; j += T) cuts.push_back(j);
+          for (int j = nn; j < nj; j += T) cuts.push_back(j);
+          cuts.push_back(nj);
+          for (size_t ci = 0; ci + 1 < cuts.size(); ci++) {
+            const int j0 = cuts[ci], j1 = std::min(cuts[ci + 1], j0 + T);
+            std::vector<Stf::Acc> acc = rd;
+            if (j0 < nn) {
+              const int jt = j0 / T;  // nn-column tiles: front tile jt spans [jt*T, jt*T+T)
+              for (int i = jt; i < F11.ntr(); i++) acc.push_back(Stf::W(F11, i, jt));
+              for (int i = 0; i < F21.ntr(); i++) acc.push_back(Stf::W(F21, i, jt));
+            }
+            if (j1 > nn) {
+              const int c0t = (std::max(j0, nn) - nn) / T, c1t = (j1 - 1 - nn) / T;
+              for (int ct = c0t; ct <= c1t; ct++)
+                for (int i = ct; i < F22.ntr(); i++) acc.push_back(Stf::W(F22, i, ct));
+            }
+            Task t = make_task(T_ASM);
+            t.aux[0] = (int32_t)k;
+            t.aux[1] = j0;
+            t.aux[2] = j1;
+            t.aux[3] = zero ? 1 : 0;
+            t.a = opnd((uint8_t)(B_U0 + u), f.blk, nj);
+            t.c = opnd(B_WS, oW[u] + f.upd, std::max(na, 1));
+            t.off2 = oW[u];
+            S.submit(t, kg(0, j0 / T, 0), acc, -1, 3.0 + (double)nj * (j1 - j0) / 4000.0);
+          }
         };
         if (!inv) {
           extend_add(true);
@@ -257,17 +277,21 @@ int build_hessian(const chb_plan& P, Program& prog, int nu, int flags) {
     for (int l = f.chbeg; l < f.chend; l++) {
       const int c = P.chidx[l];
       const int Nc = P.fronts[c].na;
-      std::vector<Stf::Acc> acc = rd;
-      Stf::all(acc, dst[c], true, true);
-      Task t = make_task(T_EXTRACT);
-      t.aux[0] = c;
-      t.aux[1] = 0;
-      t.aux[2] = Nc;
-      t.a = opnd(F11.base, F11.off, F11.ld);
-      t.b = opnd(F21.base, F21.off, F21.ld);
-      t.c = opnd(F22.base, F22.off, F22.ld);
-      t.off2 = dst_base;
-      S.submit(t, kg(0, c, 0), acc, -1, 3.0 + (double)Nc * Nc / 4000.0);
+      // 64-column chunks of the child's update (disjoint column tiles)
+      for (int q0 = 0; q0 < Nc; q0 += TILE) {
+        const int qt = q0 / TILE;
+        std::vector<Stf::Acc> acc = rd;
+        for (int i = qt; i < dst[c].ntr(); i++) acc.push_back(Stf::W(dst[c], i, qt));
+        Task t = make_task(T_EXTRACT);
+        t.aux[0] = c;
+        t.aux[1] = q0;
+        t.aux[2] = std::min(Nc, q0 + TILE);
+        t.a = opnd(F11.base, F11.off, F11.ld);
+        t.b = opnd(F21.base, F21.off, F21.ld);
+        t.c = opnd(F22.base, F22.off, F22.ld);
+        t.off2 = dst_base;
+        S.submit(t, kg(0, c, q0), acc, -1, 3.0 + (double)(Nc - q0) * TILE / 4000.0);
+      }
     }
   };
 

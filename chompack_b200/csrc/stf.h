@@ -42,6 +42,10 @@ struct Stf {
   DagBuilder& B;
   std::unordered_map<uint64_t, TileState> st;
   int next_mat = 0;
+  // Workspace allocator (doubles) for split-K scratch; products with K above
+  // ksplit are split along K when it is set.
+  std::function<int64_t(int64_t)> alloc;
+  int ksplit = 384;
 
   explicit Stf(DagBuilder& b) : B(b) {}
 
@@ -112,6 +116,21 @@ struct Stf {
         s.readers.push_back(id);
       }
     }
+  }
+  // A GEMM-type task (T_GEMM or T_MROW): split along K into parallel parts
+  // and a fixed-order sum when long and a scratch allocator is set; the
+  // parts carry the reads of `acc`, the sum its writes.
+  int gemm(const Task& t, const SchedKey& key, const std::vector<Acc>& acc) {
+    if (!alloc || split_count(t.k, ksplit) == 1) return submit(t, key, acc);
+    const int64_t scr = alloc((int64_t)split_count(t.k, ksplit) * TILE * TILE);
+    SplitTask sp = add_split_gemm(B, t, ksplit, scr, key);
+    const std::vector<Acc> rd = reads_only(acc);
+    std::vector<Acc> wr;
+    for (const Acc& a : acc)
+      if (a.write) wr.push_back(a);
+    for (int id : sp.parts) submit_existing(id, rd);
+    submit_existing(sp.out, wr);
+    return sp.out;
   }
   static std::vector<Acc> reads_only(const std::vector<Acc>& acc) {
     std::vector<Acc> r;
@@ -218,11 +237,15 @@ inline void stf_syrk_t(Stf& S, KeyGen& kg, const Mat& X, const Mat& C, double al
       Operand a = opnd(X.base, X.at(0, i * TILE), X.ld, OM_T);
       Operand b = opnd(X.base, X.at(0, j * TILE), X.ld, OM_T);
       Task t = gemm(C.th(i), C.tw(j), X.rows, alpha, a, b, beta, C.op(i, j), i == j, 0);
-      S.submit(t, kg(i, j, 0), acc);
+      S.gemm(t, kg(i, j, 0), acc);
     }
 }
 
-// M := L^{-1} (both n x n, lower tiles), from the diagonal-tile inverses.
+// M := L^{-1} (both n x n, lower tiles), from the diagonal-tile inverses,
+// right-looking by block column j: as soon as M(l, j) is final,
+// T(c, j) += L(c, l) M(l, j) for every c > l (accumulated in place at
+// M(c, j)), then M(l+1, j) = -Minv_{l+1} T(l+1, j).  The dependent chain per
+// column is two 64x64 tiles per block row.
 inline void stf_tri_inverse(Stf& S, KeyGen& kg, const Mat& L, const Mat& Minv, const Mat& M) {
   const int nb = L.ntr();
   kg.step++;
@@ -234,28 +257,18 @@ inline void stf_tri_inverse(Stf& S, KeyGen& kg, const Mat& L, const Mat& Minv, c
     t.c = M.op(c, c);
     S.submit(t, kg(c, c, 0), {Stf::R(Minv, c, 0), Stf::W(M, c, c)});
   }
-  for (int c = 1; c < nb; c++) {
+  for (int l = 0; l + 1 < nb; l++) {
     kg.step++;
-    for (int j = 0; j < c; j++) {
-      Task t = make_task(T_MROW);
-      t.m = L.tw(c);
-      t.n = L.tw(j);
-      t.k = (c - j) * TILE;
-      t.alpha = -1.0;
-      t.a = L.op(c, j);
-      t.b = opnd(M.base, M.at(j * TILE, j * TILE), M.ld, OM_TRI_T, 0);
-      t.c = M.op(c, j);
-      const int64_t moff = Minv.at(c * TILE, 0);
-      t.aux[0] = Minv.base;
-      t.aux[1] = Minv.ld;
-      t.aux[2] = (int32_t)(uint32_t)(moff & 0xffffffffLL);
-      t.aux[3] = (int32_t)(moff >> 32);
-      std::vector<Stf::Acc> acc{Stf::W(M, c, j), Stf::R(Minv, c, 0)};
-      for (int l = j; l < c; l++) {
-        acc.push_back(Stf::R(L, c, l));
-        acc.push_back(Stf::R(M, l, j));
+    for (int j = 0; j <= l; j++) {
+      for (int c = l + 1; c < nb; c++) {
+        Operand b = opnd(M.base, M.at(l * TILE, j * TILE), M.ld, OM_T, 0);  // M(l, j)^T
+        Task t = gemm(L.tw(c), L.tw(j), L.tw(l), 1.0, L.op(c, l), b, l == j ? 0.0 : 1.0, M.op(c, j));
+        S.submit(t, kg(c, j, 1), {Stf::W(M, c, j), Stf::R(L, c, l), Stf::R(M, l, j)});
       }
-      S.submit(t, kg(c, j, 1), acc);
+      const int c = l + 1;
+      Operand b = opnd(M.base, M.at(c * TILE, j * TILE), M.ld, OM_T, 0);   // T(c, j)^T
+      Task t = gemm(L.tw(c), L.tw(j), L.tw(c), -1.0, Minv.op(c, 0), b, 0.0, M.op(c, j));
+      S.submit(t, kg(c, j, 2), {Stf::W(M, c, j), Stf::R(Minv, c, 0)});
     }
   }
 }
@@ -326,11 +339,12 @@ inline int stf_update_factor(Stf& S, KeyGen& kg, const chb_plan& P, int c, const
     std::vector<Stf::Acc> rd;
     Stf::all(rd, F11, false, true);
     Stf::all(rd, F21, false);
-    const int CH = 16;
+    const int CH = TILE;  // one column tile of U11/U21 per chunk: parallel chunks
     for (int q0 = 0; q0 < N1; q0 += CH) {
       std::vector<Stf::Acc> acc = rd;
-      Stf::all(acc, U11, true, true);
-      Stf::all(acc, U21, true);
+      const int qt = q0 / TILE;
+      for (int i = qt; i < U11.ntr(); i++) acc.push_back(Stf::W(U11, i, qt));
+      for (int i = 0; i < U21.ntr(); i++) acc.push_back(Stf::W(U21, i, qt));
       Task t = make_task(T_EXTRACT);
       t.aux[0] = c;
       t.aux[1] = q0;
@@ -413,12 +427,7 @@ inline int stf_update_factor(Stf& S, KeyGen& kg, const chb_plan& P, int c, const
           t.aux[1] = TILE;
           t.aux[2] = (int32_t)(uint32_t)(Tp.off & 0xffffffffLL);
           t.aux[3] = (int32_t)(Tp.off >> 32);
-          const int KS = 384;
-          const int64_t scr = split_count(h, KS) > 1 ? alloc((int64_t)split_count(h, KS) * TILE * TILE) : 0;
-          SplitTask st = add_split_gemm(S.B, t, KS, scr, kg(0, c, t2));
-          for (size_t q = 0; q < st.parts.size(); q++)
-            S.submit_existing(st.parts[q], st.parts.size() == 1 ? acc : S.reads_only(acc));
-          if (st.parts.size() > 1) S.submit_existing(st.out, {Stf::W(Z, 0, t2)});
+          S.gemm(t, kg(0, c, t2), acc);
         }
         for (int i = row0 / TILE; i <= row1 / TILE; i++) {
           const int rs = std::max(i * TILE, row0), re = std::min(i * TILE + TILE, row1 + 1);
