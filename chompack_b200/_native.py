@@ -84,6 +84,7 @@ logdet = _sig("chb_logdet", ctypes.c_int, [PPLAN, vp, vp, vp, ctypes.c_size_t, v
 sym_weight = _sig("chb_sym_weight", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_double, vp])
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
 set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
+plan_set_schedule = _sig("chb_plan_set_schedule", ctypes.c_int, [PPLAN, ctypes.c_int])
 
 OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)
 HESSIAN_MAX_U = 59   # U matrices per chb_hessian call (base slots 5..63)

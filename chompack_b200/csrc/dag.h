@@ -242,6 +242,35 @@ struct DagBuilder {
       prog.tasks[i] = tk;
     }
     prog.ncounters = (int64_t)nt + (int64_t)group_size.size();
+    // dynamic scheduling data: waits per task, waiters per counter, the
+    // value at which each counter is complete, the initially ready tasks
+    const int64_t nc = prog.ncounters;
+    prog.npend.assign(nt, 0);
+    prog.succ_off.assign(nc + 1, 0);
+    prog.ctarget.assign(nc, 1);
+    for (size_t g = 0; g < group_size.size(); g++) prog.ctarget[nt + g] = std::max(group_size[g], 1);
+    for (int i = 0; i < nt; i++) {
+      const Task& tk = prog.tasks[i];
+      prog.npend[i] = tk.nwait;
+      for (int w = 0; w < tk.nwait; w++) prog.succ_off[prog.waits[tk.wait_off + w].x + 1]++;
+    }
+    for (int64_t c = 0; c < nc; c++) prog.succ_off[c + 1] += prog.succ_off[c];
+    prog.succ.assign(prog.succ_off[nc], 0);
+    {
+      std::vector<int> fill(prog.succ_off.begin(), prog.succ_off.end() - 1);
+      for (int i = 0; i < nt; i++) {
+        const Task& tk = prog.tasks[i];
+        for (int w = 0; w < tk.nwait; w++) prog.succ[fill[prog.waits[tk.wait_off + w].x]++] = i;
+      }
+    }
+    const int nwords = (nt + 63) / 64, nsumm = (nwords + 63) / 64;
+    prog.ready0.assign(nwords, 0ull);
+    prog.summ0.assign(nsumm, 0ull);
+    for (int i = 0; i < nt; i++)
+      if (prog.npend[i] == 0) {
+        prog.ready0[i >> 6] |= 1ull << (i & 63);
+        prog.summ0[i >> 12] |= 1ull << ((i >> 6) & 63);
+      }
     return 0;
   }
 };

@@ -1,13 +1,16 @@
 // Persistent task-graph executor for the multifrontal sweeps (sm_100a).
 //
-// One kernel launch runs a whole sweep.  Each CTA (128 threads) loops:
-// claim the next task index with an atomic counter, wait until the counters
-// the task depends on reach their targets (bounded spin; on timeout the CTA
-// records DE_TIMEOUT and leaves, so a planning error can never hang the
-// GPU), execute the task, then publish its counter with release semantics.
+// One kernel launch runs a whole sweep, in one of two schedules.  Static:
+// each CTA (128 threads) claims the next task index in list order with an
+// atomic counter, waits until the counters the task depends on reach their
+// targets (bounded spin; on timeout the CTA records DE_TIMEOUT and leaves,
+// so a planning error can never hang the GPU), executes the task, then
+// publishes its counter with release semantics.  Dynamic: a finished task
+// releases its waiters itself and keeps one of them; idle CTAs claim the
+// others from a ready bitmap (bounded polling, same timeout rule).
 //
 // Dense FP64 tile arithmetic uses the double-precision tensor-core MMA
-// (mma.sync m8n8k4 f64): a 64x64 C tile is split over 4 warps, 32x32 each.
+// (mma.sync m16n8k4 f64): a 64x64 C tile is split over 4 warps, 32x32 each.
 // Operand tiles are staged through shared memory with L2-coherent loads
 // (__ldcg), since tiles produced by other CTAs in the same launch must not be
 // read from a stale L1 line.
@@ -30,6 +33,228 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
 }
 
 __device__ __forceinline__ int ld_volatile(const int* p) { return *((const volatile int*)p); }
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// ------------------------------------------------------ dynamic schedule
+// Ready tasks are bits of a bitmap (64 tasks per word, bit = list position)
+// with a summary bitmap of the nonzero words.  ctl[5] is the finished
+// frontier: every task in the words below it has finished, so no ready bit
+// can appear there again; ctl[4] counts finished tasks.
+//
+// A finished task decrements the pending counts of its waiters (one lane of
+// warp 0 per waiter, acq_rel).  Of the waiters it makes ready, the CTA keeps
+// the one of lowest list position and runs it next, so a chain of dependent
+// tasks never passes through the bitmap; the others are published with a
+// release OR into the bitmap and claimed by idle CTAs with an acquire AND.
+//
+// Summary invariant: a word that turns nonzero has its summary bit set after
+// it; a claimer that clears a summary bit re-reads the word after the clear
+// and sets the bit again if the word is nonzero.  The fences between the word
+// and summary accesses on both sides keep a nonzero word from ever losing its
+// summary bit.
+__device__ __forceinline__ int atom_add_acq_rel(int* p, int v) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void red_or_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.or.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long atom_and_acquire(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acquire.gpu.global.and.b64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ unsigned long long atom_and_acq_rel(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.and.b64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
+// Publishes ready task s: its bit (release: the waiter's inputs are visible
+// to whoever acquires the bit), then its word's summary bit (release: after
+// the word).  Neither waits for a reply.
+__device__ __forceinline__ void publish_ready(const RunArgs& ra, int s) {
+  red_or_release(ra.ready + (s >> 6), 1ull << (s & 63));
+  red_or_release(ra.summ + (s >> 12), 1ull << ((s >> 6) & 63));
+}
+
+// Clears the summary bit of a word seen empty.  The acq_rel AND reads the
+// summary after any publish that set the bit, so the word re-read below
+// shows that publish's task (unless it was claimed since).
+__device__ __forceinline__ void clear_summary(const RunArgs& ra, int wi) {
+  const unsigned long long bit = 1ull << (wi & 63);
+  atom_and_acq_rel(ra.summ + (wi >> 6), ~bit);
+  if (ld_relaxed_u64(ra.ready + wi) != 0) red_or_release(ra.summ + (wi >> 6), bit);
+}
+
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit_and_wait_later() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Releases the waiters listed in succ[b, e) (warp 0); the first 32 come
+// from pre (shared memory) when it is given.  With handoff, the released
+// waiter of lowest list position (below *next, the earlier candidate)
+// becomes *next and is not published; the displaced candidate is.
+__device__ __forceinline__ void release_list(const RunArgs& ra, int b, int e, const int* pre, bool handoff,
+                                             int* next) {
+  const int lane = threadIdx.x & 31;
+  for (int i0 = b; i0 < e; i0 += 32) {
+    int s = -1;
+    if (i0 + lane < e) {
+      s = (pre && i0 == b) ? pre[lane] : __ldg(ra.succ + i0 + lane);
+      if (atom_add_acq_rel(ra.pend + s, -1) != 1) s = -1;
+    }
+    __syncwarp();  // orders every lane's acquire before the other lanes' publishes
+    if (!handoff) {
+      if (s >= 0) publish_ready(ra, s);
+      continue;
+    }
+    int m = (s >= 0) ? s : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int prev = *next;
+    const int keep = min(m, prev);
+    if (s >= 0 && s != keep) publish_ready(ra, s);
+    if (lane == 0 && prev != 0x7fffffff && prev != keep) publish_ready(ra, prev);
+    *next = keep;
+  }
+}
+
+// Advances the finished frontier over every word whose tasks have all
+// finished.
+__device__ __forceinline__ void advance_frontier(const RunArgs& ra) {
+  __threadfence();
+  int cur = ld_volatile(&ra.ctl[5]);
+  while (cur < ra.nwords) {
+    const int cnt = min(64, ra.ntasks - 64 * cur);
+    if (ld_volatile(ra.wclaimed + cur) < cnt) break;
+    const int prev = atomicCAS(&ra.ctl[5], cur, cur + 1);
+    cur = (prev == cur) ? cur + 1 : prev;
+  }
+}
+
+// Claims the word's set bit of rank (blockIdx.x mod its popcount), so that
+// CTAs claiming at once spread over the word (lane 0).  Returns the task, or
+// -1 when the word has emptied (then, for a word found through the summary,
+// its summary bit is cleared).
+__device__ __forceinline__ int claim_in_word(const RunArgs& ra, int wi, unsigned long long w, bool from_summary) {
+  while (w) {
+    const unsigned lo = (unsigned)w, hi = (unsigned)(w >> 32);
+    const int plo = __popc(lo), r = (int)(blockIdx.x % (unsigned)(plo + __popc(hi)));
+    const int pos = r < plo ? (int)__fns(lo, 0, r + 1) : 32 + (int)__fns(hi, 0, r - plo + 1);
+    const unsigned long long bit = 1ull << pos;
+    const unsigned long long old = atom_and_acquire(ra.ready + wi, ~bit);
+    if (old & bit) return wi * 64 + pos;
+    w = old;
+  }
+  if (from_summary) clear_summary(ra, wi);
+  return -1;
+}
+
+// Claims a ready task for this CTA (warp 0; every lane returns it): first in
+// the 32 bitmap words from the cached frontier *lo, then through the summary
+// beyond them.  Returns ntasks when every task has finished, when a device
+// error is set, or when nothing became ready within the spin limit
+// (DE_TIMEOUT).
+__device__ __forceinline__ int claim_task(const RunArgs& ra, int* lo) {
+  const int lane = threadIdx.x & 31;
+  int64_t spins = 0;
+  unsigned ns = 64;
+  for (;;) {
+    const int wi = *lo + lane;
+    const unsigned long long w = (wi < ra.nwords) ? ld_relaxed_u64(ra.ready + wi) : 0ull;
+    int stop = 0, front = 0;
+    if (lane == 0) {
+      stop = ld_volatile(&ra.ctl[4]) >= ra.ntasks || ld_volatile(&ra.ctl[1]) != 0;
+      front = ld_volatile(&ra.ctl[5]);
+    }
+    if (__shfl_sync(0xffffffffu, stop, 0)) return ra.ntasks;
+    front = __shfl_sync(0xffffffffu, front, 0);
+    unsigned bal = __ballot_sync(0xffffffffu, w != 0);
+    while (bal) {
+      const int src = __ffs(bal) - 1;
+      bal &= bal - 1;
+      const unsigned long long ww = __shfl_sync(0xffffffffu, w, src);
+      int got = -1;
+      if (lane == 0) got = claim_in_word(ra, *lo + src, ww, false);
+      got = __shfl_sync(0xffffffffu, got, 0);
+      if (got >= 0) return got;
+    }
+    if (front > *lo) {
+      *lo = front;
+      continue;
+    }
+    // beyond the window: summary words from the one holding word *lo + 32
+    const int first = *lo + 32;
+    for (int s0 = first >> 6; s0 < ra.nsumm; s0 += 32) {
+      unsigned long long sw = (s0 + lane < ra.nsumm) ? ld_relaxed_u64(ra.summ + s0 + lane) : 0ull;
+      if (s0 + lane == (first >> 6)) sw &= ~0ull << (first & 63);
+      unsigned sb = __ballot_sync(0xffffffffu, sw != 0);
+      while (sb) {
+        const int src = __ffs(sb) - 1;
+        sb &= sb - 1;
+        unsigned long long bits = __shfl_sync(0xffffffffu, sw, src);
+        int got = -1;
+        if (lane == 0) {
+          while (bits && got < 0) {
+            const int wj = (s0 + src) * 64 + __ffsll((long long)bits) - 1;
+            bits &= bits - 1;
+            got = claim_in_word(ra, wj, ld_relaxed_u64(ra.ready + wj), true);
+          }
+        }
+        got = __shfl_sync(0xffffffffu, got, 0);
+        if (got >= 0) return got;
+      }
+    }
+    if (++spins > ra.spin_limit) {
+      if (lane == 0) {
+        atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+        atomicAdd(&ra.ctl[3], 1);
+      }
+      return ra.ntasks;
+    }
+    __nanosleep(ns);
+    if (ns < 512) ns <<= 1;
+  }
+}
+
+// After task ti (warp 0, the CTA's writes ordered before by __syncthreads):
+// releases the waiters of the task (the first 32 prefetched into pre) and,
+// when the task completes its group, of the group; counts the task into its
+// bitmap word's finished tasks and the finished count.  Returns the released
+// waiter this CTA runs next, or -1 (also when a device error is set).
+__device__ __forceinline__ int finish_task(const RunArgs& ra, int ti, int group, int sb, int se, const int* pre) {
+  const int lane = threadIdx.x & 31;
+  int next = 0x7fffffff;
+  int gdone = 0, filled = 0, err = 0;
+  if (lane == 0 && group >= 0) gdone = atom_add_acq_rel(ra.counters + group, 1) + 1 == __ldg(ra.ctarget + group);
+  if (lane == 1) filled = atomicAdd(ra.wclaimed + (ti >> 6), 1) + 1 == min(64, ra.ntasks - (ti & ~63));
+  if (lane == 2) err = ld_volatile(&ra.ctl[1]);
+  cp_async_wait_all();
+  release_list(ra, sb, se, pre, true, &next);
+  if (__shfl_sync(0xffffffffu, gdone, 0))
+    release_list(ra, __ldg(ra.succ_off + group), __ldg(ra.succ_off + group + 1), nullptr, true, &next);
+  if (lane == 1 && filled) advance_frontier(ra);
+  if (lane == 0) red_release_add(&ra.ctl[4], 1);
+  if (__shfl_sync(0xffffffffu, err, 2) != 0 && next != 0x7fffffff) {
+    if (lane == 0) publish_ready(ra, next);  // left for the exit path; nothing runs after an error
+    next = 0x7fffffff;
+  }
+  return next == 0x7fffffff ? -1 : next;
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -275,9 +500,15 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
     store_acc(ra.bases[oc.base] + oc.off, oc.ld, m, n, lower, cdiag, alpha, beta, acc);
     if (la && ph == 0) {
       __syncthreads();
-      if (threadIdx.x == 0 && t.aux[3] > 0) {
-        __threadfence();
-        red_release_add(ra.counters + (t.aux[3] - 1), 1);
+      if (t.aux[3] > 0) {
+        if (ra.dynamic) {
+          const int c = t.aux[3] - 1;
+          if (threadIdx.x < 32)
+            release_list(ra, __ldg(ra.succ_off + c), __ldg(ra.succ_off + c + 1), nullptr, false, nullptr);
+        } else if (threadIdx.x == 0) {
+          __threadfence();
+          red_release_add(ra.counters + (t.aux[3] - 1), 1);
+        }
       }
     }
   }
@@ -1150,45 +1381,91 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   extern __shared__ double smem[];
   __shared__ int s_task;
   __shared__ int s_abort;
+  __shared__ int s_next;      // dynamic: the waiter this CTA released and runs next, or -1
+  __shared__ int s_succ[2];   // dynamic: waiter range of the current task
+  __shared__ int s_pre[32];   // dynamic: its first 32 waiters (cp.async during the task)
   __shared__ __align__(16) Task s_t;
+  static_assert(sizeof(Task) == 36 * 4, "task record is 36 words");
   SmemLayout sm{smem, smem + TILE * LDS};
+  __shared__ int s_lo;        // dynamic: this CTA's copy of the finished frontier
+  if (threadIdx.x == 0) {
+    s_next = -1;
+    s_lo = 0;
+  }
   for (;;) {
-    if (threadIdx.x == 0) s_task = atomicAdd(&ra.ctl[0], 1);
-    __syncthreads();
-    const int ti = s_task;
-    if (ti >= ra.ntasks) break;
-    {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(ra.tasks + ti);
-      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_t);
-      for (int w = threadIdx.x; w < (int)(sizeof(Task) / 4); w += NTHREADS) dst[w] = __ldg(src + w);
-    }
-    __syncthreads();
-    const Task& t = s_t;
-    if (threadIdx.x == 0) {
-      if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
-      int abort = 0;
-      for (int w = 0; w < t.nwait && !abort; w++) {
-        const int2 wt = ra.waits[t.wait_off + w];
-        int64_t spins = 0;
-        unsigned ns = 16;
-        while (ld_acquire(ra.counters + wt.x) < wt.y) {
-          if (++spins > ra.spin_limit) {
-            atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
-            atomicAdd(&ra.ctl[3], 1);
-            abort = 1;
-            break;
+    if (ra.dynamic) {
+      // warp 0: the next task (handed over by the last one, or claimed), its
+      // record and waiter range in one round of loads, its first waiters
+      // prefetched asynchronously
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        __syncwarp();
+        const unsigned long long t0 = ra.trace ? global_ns() : 0ull;
+        int c = s_next;
+        if (c < 0) c = claim_task(ra, &s_lo);
+        if (c < ra.ntasks) {
+          const uint32_t* src = reinterpret_cast<const uint32_t*>(ra.tasks + c);
+          uint32_t* dst = reinterpret_cast<uint32_t*>(&s_t);
+          const uint32_t v0 = __ldg(src + lane);
+          const uint32_t v1 = lane < 4 ? __ldg(src + 32 + lane) : 0u;
+          const int so = (lane == 4 || lane == 5) ? __ldg(ra.succ_off + c + lane - 4) : 0;
+          dst[lane] = v0;
+          if (lane < 4) dst[32 + lane] = v1;
+          const int b = __shfl_sync(0xffffffffu, so, 4), e = __shfl_sync(0xffffffffu, so, 5);
+          if (lane == 0) {
+            s_succ[0] = b;
+            s_succ[1] = e;
           }
-          if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
-          __nanosleep(ns);
-          if (ns < 128) ns <<= 1;
+          if (lane < e - b) cp_async4(&s_pre[lane], ra.succ + b + lane);
+          cp_async_commit_and_wait_later();
+          if (lane == 0 && ra.trace) {
+            ra.trace[4 * (int64_t)c] = t0;
+            ra.trace[4 * (int64_t)c + 1] = global_ns();
+          }
         }
+        if (lane == 0) s_task = c;
       }
-      if (!abort && ld_volatile(&ra.ctl[1]) != 0) abort = 1;
-      s_abort = abort;
-      if (ra.trace) ra.trace[4 * (int64_t)ti + 1] = global_ns();
+      __syncthreads();
+      if (s_task >= ra.ntasks) break;
+    } else {
+      if (threadIdx.x == 0) s_task = atomicAdd(&ra.ctl[0], 1);
+      __syncthreads();
+      const int ti = s_task;
+      if (ti >= ra.ntasks) break;
+      {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(ra.tasks + ti);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&s_t);
+        for (int w = threadIdx.x; w < 36; w += NTHREADS) dst[w] = __ldg(src + w);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
+        int abort = 0;
+        for (int w = 0; w < s_t.nwait && !abort; w++) {
+          const int2 wt = ra.waits[s_t.wait_off + w];
+          int64_t spins = 0;
+          unsigned ns = 16;
+          while (ld_acquire(ra.counters + wt.x) < wt.y) {
+            if (++spins > ra.spin_limit) {
+              atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+              atomicAdd(&ra.ctl[3], 1);
+              abort = 1;
+              break;
+            }
+            if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
+            __nanosleep(ns);
+            if (ns < 128) ns <<= 1;
+          }
+        }
+        if (!abort && ld_volatile(&ra.ctl[1]) != 0) abort = 1;
+        s_abort = abort;
+        if (ra.trace) ra.trace[4 * (int64_t)ti + 1] = global_ns();
+      }
+      __syncthreads();
+      if (s_abort) break;
     }
-    __syncthreads();
-    if (s_abort) break;
+    const int ti = s_task;
+    const Task& t = s_t;
     switch (t.op) {
       case T_GEMM:
       case T_LA: run_gemm_or_la(ra, t, sm); break;
@@ -1206,14 +1483,19 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
         break;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      if (ra.trace) {
-        ra.trace[4 * (int64_t)ti + 2] = global_ns();
-        ra.trace[4 * (int64_t)ti + 3] = (unsigned long long)sm_id() | ((unsigned long long)t.op << 32);
+    if (threadIdx.x == 0 && ra.trace) {
+      ra.trace[4 * (int64_t)ti + 2] = global_ns();
+      ra.trace[4 * (int64_t)ti + 3] = (unsigned long long)sm_id() | ((unsigned long long)t.op << 32);
+    }
+    if (!ra.dynamic) {
+      if (threadIdx.x == 0) {
+        __threadfence();
+        red_release_add(ra.counters + ti, 1);
+        if (t.group >= 0) red_release_add(ra.counters + t.group, 1);
       }
-      __threadfence();
-      red_release_add(ra.counters + ti, 1);
-      if (t.group >= 0) red_release_add(ra.counters + t.group, 1);
+    } else if (threadIdx.x < 32) {
+      const int nx = finish_task(ra, ti, t.group, s_succ[0], s_succ[1], s_pre);
+      if (threadIdx.x == 0) s_next = nx;
     }
   }
 }

@@ -141,6 +141,22 @@ struct RunArgs {
   int64_t ldb;            // leading dimension of the right-hand sides (trsm)
   double alpha;           // scale applied by the trsm gather
   unsigned long long* trace;  // optional: 4 words per task (claim, start, end, sm | op << 32)
+  // Dynamic scheduling (dynamic != 0): a finished task decrements the
+  // pending counts of its successors (CSR succ_off / succ per counter) and
+  // sets the ready bits of those that reach zero; CTAs claim the ready task
+  // of lowest list position.  ctl[4] counts finished tasks, ctl[5] is the
+  // first word of the ready bitmap that may hold an unclaimed task.
+  int dynamic;
+  int nwords;                     // ready-bitmap words (64 tasks each)
+  int nsumm;                      // summary words (64 bitmap words each)
+  int pad2;
+  int* pend;                      // unmet dependencies per task
+  unsigned long long* ready;      // ready, unclaimed tasks
+  unsigned long long* summ;       // nonzero ready words
+  int* wclaimed;                  // claimed tasks per bitmap word
+  const int* succ_off;            // ncounters + 1
+  const int* succ;
+  const int* ctarget;             // value at which a counter is complete
 };
 
 // Sub-operations of T_VEC (triangular solve sweep).

@@ -1,6 +1,8 @@
 // Plan creation (symbolic upload), program cache and program launch.
 #include "plan.h"
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <cstring>
 
@@ -12,6 +14,12 @@ namespace chb {
 Program::~Program() {
   if (d_tasks) cudaFree(d_tasks);
   if (d_waits) cudaFree(d_waits);
+  if (d_npend) cudaFree(d_npend);
+  if (d_succ_off) cudaFree(d_succ_off);
+  if (d_succ) cudaFree(d_succ);
+  if (d_ctarget) cudaFree(d_ctarget);
+  if (d_ready0) cudaFree(d_ready0);
+  if (d_summ0) cudaFree(d_summ0);
 }
 
 static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -19,7 +27,12 @@ static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 WsLayout ws_layout(const Program& p) {
   WsLayout L;
   L.counters_off = 256;
-  L.dbl_off = round_up(L.counters_off + (size_t)p.ncounters * sizeof(int), 256);
+  const size_t nt = p.tasks.size(), nw = p.ready0.size(), ns = p.summ0.size();
+  L.pend_off = round_up(L.counters_off + (size_t)p.ncounters * sizeof(int), 256);
+  L.ready_off = round_up(L.pend_off + nt * sizeof(int), 256);
+  L.summ_off = round_up(L.ready_off + nw * sizeof(unsigned long long), 256);
+  L.wcl_off = round_up(L.summ_off + ns * sizeof(unsigned long long), 256);
+  L.dbl_off = round_up(L.wcl_off + nw * sizeof(int), 256);
   L.total = L.dbl_off + (size_t)p.ws_doubles * sizeof(double);
   return L;
 }
@@ -39,7 +52,20 @@ static int upload_program(Program& prog) {
     CUDA_TRY(cudaMalloc(&prog.d_waits, prog.waits.size() * sizeof(int2)));
     CUDA_TRY(cudaMemcpy(prog.d_waits, prog.waits.data(), prog.waits.size() * sizeof(int2), cudaMemcpyHostToDevice));
   }
-  return 0;
+  auto up = [](auto** dst, const auto& v) -> int {
+    if (v.empty()) return 0;
+    const size_t bytes = v.size() * sizeof(v[0]);
+    CUDA_TRY(cudaMalloc((void**)dst, bytes));
+    CUDA_TRY(cudaMemcpy(*dst, v.data(), bytes, cudaMemcpyHostToDevice));
+    return 0;
+  };
+  int rc = up(&prog.d_npend, prog.npend);
+  if (!rc) rc = up(&prog.d_succ_off, prog.succ_off);
+  if (!rc) rc = up(&prog.d_succ, prog.succ);
+  if (!rc) rc = up(&prog.d_ctarget, prog.ctarget);
+  if (!rc) rc = up(&prog.d_ready0, prog.ready0);
+  if (!rc) rc = up(&prog.d_summ0, prog.summ0);
+  return rc;
 }
 
 // Builds the host side of a program only (no device upload); used by the
@@ -62,6 +88,11 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   if (rc != 0) return nullptr;
   for (const Task& t : prog->tasks)
     if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
+  // Default schedule per sweep, by measurement on a 3-D grid of 64,000
+  // unknowns: the chains of small dependent tasks of cholesky, llt and trsm
+  // run faster in static list order (a CTA already waits on the next task);
+  // the other sweeps gain from running whichever task is ready.
+  prog->static_default = op == CHB_OP_CHOLESKY || op == CHB_OP_LLT || op == CHB_OP_TRSM;
   Program* p = prog.get();
   plan->progs[key] = std::move(prog);
   return p;
@@ -107,6 +138,32 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.perm = plan->d_perm;
   ra.ldb = run_ldb;
   ra.alpha = run_alpha;
+  // The plan's schedule, else CHB_SCHEDULE (static | dynamic), else the
+  // sweep's default.
+  static const char* sched = std::getenv("CHB_SCHEDULE");
+  bool want_static = prog->static_default;
+  if (sched && std::strcmp(sched, "static") == 0) want_static = true;
+  if (sched && std::strcmp(sched, "dynamic") == 0) want_static = false;
+  if (plan->schedule >= 0) want_static = plan->schedule == 1;
+  const bool dynamic = !want_static && prog->d_npend && prog->d_ready0;
+  if (dynamic) {
+    ra.dynamic = 1;
+    ra.nwords = (int)prog->ready0.size();
+    ra.nsumm = (int)prog->summ0.size();
+    ra.pend = (int*)(w + L.pend_off);
+    ra.ready = (unsigned long long*)(w + L.ready_off);
+    ra.summ = (unsigned long long*)(w + L.summ_off);
+    ra.wclaimed = (int*)(w + L.wcl_off);
+    ra.succ_off = prog->d_succ_off;
+    ra.succ = prog->d_succ;
+    ra.ctarget = prog->d_ctarget;
+    CUDA_TRY(cudaMemcpyAsync(ra.pend, prog->d_npend, prog->npend.size() * sizeof(int), cudaMemcpyDeviceToDevice,
+                             stream));
+    CUDA_TRY(cudaMemcpyAsync(ra.ready, prog->d_ready0, prog->ready0.size() * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToDevice, stream));
+    CUDA_TRY(cudaMemcpyAsync(ra.summ, prog->d_summ0, prog->summ0.size() * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToDevice, stream));
+  }
   int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
   CUDA_TRY(engine_launch(ra, grid, stream));
   return 0;
@@ -334,6 +391,39 @@ extern "C" int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, 
   if (tasks) std::memcpy(tasks, p->tasks.data(), p->tasks.size() * sizeof(Task));
   if (waits) std::memcpy(waits, p->waits.data(), p->waits.size() * sizeof(int2));
   if (fronts) std::memcpy(fronts, plan->fronts.data(), plan->fronts.size() * sizeof(FrontDesc));
+  return 0;
+}
+
+extern "C" int chb_program_schedule(chb_plan* plan, int op, int64_t k, int flags, int64_t* sizes, int32_t* npend,
+                                    int32_t* succ_off, int32_t* succ, int32_t* ctarget, uint64_t* ready0,
+                                    uint64_t* summ0) {
+  clear_error();
+  if (!plan || !sizes) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  sizes[0] = (int64_t)p->npend.size();
+  sizes[1] = (int64_t)p->succ_off.size();
+  sizes[2] = (int64_t)p->succ.size();
+  sizes[3] = (int64_t)p->ctarget.size();
+  sizes[4] = (int64_t)p->ready0.size();
+  sizes[5] = (int64_t)p->summ0.size();
+  auto cp = [](void* dst, const auto& v) {
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+  };
+  cp(npend, p->npend);
+  cp(succ_off, p->succ_off);
+  cp(succ, p->succ);
+  cp(ctarget, p->ctarget);
+  cp(ready0, p->ready0);
+  cp(summ0, p->summ0);
+  return 0;
+}
+
+extern "C" int chb_plan_set_schedule(chb_plan* plan, int mode) {
+  clear_error();
+  if (!plan) return set_error(-1, "null plan");
+  if (mode < -1 || mode > 1) return set_error(-2, "schedule mode must be -1, 0 or 1");
+  plan->schedule = mode;
   return 0;
 }
 

@@ -20,8 +20,20 @@ struct Program {
   int64_t ncounters = 0;   // tasks + groups
   int64_t ws_doubles = 0;  // doubles of workspace (update matrices + scratch)
   int smem_doubles = ENGINE_SMEM_BASE_DOUBLES;  // dynamic shared memory per CTA
+  bool static_default = false;  // list order unless the plan asks otherwise
   Task* d_tasks = nullptr;
   int2* d_waits = nullptr;
+  // dynamic scheduling data (filled by DagBuilder::finish)
+  std::vector<int> npend;                 // waits per task
+  std::vector<int> succ_off, succ;        // waiters per counter (CSR)
+  std::vector<int> ctarget;               // completion value per counter
+  std::vector<unsigned long long> ready0, summ0;  // initially ready tasks
+  int* d_npend = nullptr;
+  int* d_succ_off = nullptr;
+  int* d_succ = nullptr;
+  int* d_ctarget = nullptr;
+  unsigned long long* d_ready0 = nullptr;
+  unsigned long long* d_summ0 = nullptr;
   ~Program();
 };
 
@@ -31,6 +43,7 @@ struct Program {
 //   [dbl_off, ...)           doubles: update matrices, then program scratch
 struct WsLayout {
   size_t counters_off;
+  size_t pend_off, ready_off, summ_off, wcl_off;  // dynamic scheduling state
   size_t dbl_off;
   size_t total;
 };
@@ -66,6 +79,7 @@ struct chb_plan {
   std::vector<int64_t> seg;     // matrices of a merged plan: supernodes [seg[m], seg[m+1])
   int64_t* d_seg = nullptr;
   int grid = 0;                 // persistent grid size
+  int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;

@@ -96,6 +96,13 @@ class Plan(object):
         aligned = (base + 255) // 256 * 256
         return aligned, nbytes
 
+    def set_schedule(self, mode):
+        """Task scheduling of this plan's sweeps: "dynamic" (finished tasks
+        release their waiters), "static" (list order with waits) or None
+        (the default).  Results are bit-identical."""
+        code = {None: -1, "dynamic": 0, "static": 1}[mode]
+        N.check(N.plan_set_schedule(self.handle, code), "plan_set_schedule")
+
     def program_info(self, op, k=0, flags=0):
         info = (ctypes.c_int64 * 8)()
         N.check(N.program_info(self.handle, op, int(k), int(flags), info), "program_info")

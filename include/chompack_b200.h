@@ -103,6 +103,13 @@ int chb_workspace_size(const chb_plan* plan, int op, int64_t k, int flags, size_
  * the per-supernode descriptors into caller buffers of those sizes. */
 int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
 int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits, void* fronts);
+/* The dynamic-schedule data of a compiled sweep: sizes[0..5] = lengths of
+ * the pending counts per task, the successor offsets per counter (counters
+ * + 1), the successor list, the completion value per counter, the initial
+ * ready bitmap and its summary (64-bit words).  Array arguments may be NULL
+ * (sizes only). */
+int chb_program_schedule(chb_plan* plan, int op, int64_t k, int flags, int64_t* sizes, int32_t* npend,
+                         int32_t* succ_off, int32_t* succ, int32_t* ctarget, uint64_t* ready0, uint64_t* summ0);
 
 /* ------------------------------------------------------------------------ */
 /* Numeric sweeps.  All pointers are device pointers; calls are asynchronous */
@@ -182,6 +189,14 @@ int chb_dot_batch(chb_plan* plan, const double* x, const double* y, double* resu
  * global-timer ns at claim, start (dependencies met) and end, and the SM id
  * | task kind << 32.  Pass NULL to switch tracing off. */
 int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
+
+/* Task scheduling of the plan's sweeps: 0 dynamic (a finished task releases
+ * its waiters; CTAs claim ready tasks near the lowest list positions), 1
+ * static (CTAs take tasks in list order and wait for their dependencies),
+ * -1 the default (CHB_SCHEDULE=static|dynamic from the environment, else
+ * static for cholesky, llt and trsm and dynamic for the others).  Both give
+ * bit-identical results. */
+int chb_plan_set_schedule(chb_plan* plan, int mode);
 
 /* Allocation-free Cholesky.  No counterpart in the reference: an addition for
  * callers that cannot call cudaMalloc when they factor (code running under

@@ -41,6 +41,30 @@ N.lib.chb_program_export.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
 
 
+N.lib.chb_program_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int64)] + [ctypes.c_void_p] * 6
+
+
+class Schedule(object):
+    """The dynamic-schedule data of a program: pending counts, successors
+    per counter (CSR), completion values and the initial ready bitmaps."""
+
+    def __init__(self, plan_handle, op, k=0, flags=0):
+        sz = (ctypes.c_int64 * 6)()
+        args = (plan_handle, op, k, flags, sz)
+        N.check(N.lib.chb_program_schedule(*args, None, None, None, None, None, None), "program_schedule")
+        self.npend = np.zeros(sz[0], dtype=np.int32)
+        self.succ_off = np.zeros(sz[1], dtype=np.int32)
+        self.succ = np.zeros(sz[2], dtype=np.int32)
+        self.ctarget = np.zeros(sz[3], dtype=np.int32)
+        self.ready0 = np.zeros(sz[4], dtype=np.uint64)
+        self.summ0 = np.zeros(sz[5], dtype=np.uint64)
+        N.check(N.lib.chb_program_schedule(*args, self.npend.ctypes.data, self.succ_off.ctypes.data,
+                                           self.succ.ctypes.data, self.ctarget.ctypes.data,
+                                           self.ready0.ctypes.data, self.summ0.ctypes.data),
+                "program_schedule")
+
+
 class Program(object):
     def __init__(self, plan_handle, op, k=0, flags=0, nsn=0):
         info = (ctypes.c_int64 * 8)()
@@ -371,11 +395,15 @@ class VM(object):
                     v = buf[off + col * ld + row]
                 WS[up + q * Nc + i] = v
 
-    def run(self, order="list", seed=0):
+    def run(self, order="list", seed=0, schedule=None):
+        """order: "list", "random" (any order the waits allow) or "dynamic"
+        (the device's dynamic release rules applied to `schedule`)."""
         tasks = self.p.tasks
         nt = len(tasks)
         if order == "list":
             seq = range(nt)
+        elif order == "dynamic":
+            seq = dynamic_order(self.p, schedule, seed)
         else:
             seq = self._random_order(seed)
         for i in seq:
@@ -416,3 +444,47 @@ class VM(object):
                             ready.append(w)
         assert len(order) == nt, "task graph has unsatisfiable waits"
         return order
+
+
+def dynamic_order(prog, sch, seed=0, window=4):
+    """The task order of the dynamic device schedule: a finished task (and
+    the early signal of a look-ahead task) releases the waiters of its
+    counters; a group counter releases its waiters when it reaches its
+    completion value; the next task is one of the `window` ready tasks of
+    lowest list position (several CTAs claim at once), chosen at random."""
+    rng = np.random.default_rng(seed)
+    tasks = prog.tasks
+    nt = len(tasks)
+    pend = sch.npend.astype(np.int64).copy()
+    count = np.zeros(len(sch.ctarget), dtype=np.int64)
+    ready = sorted(int(i) for i in np.nonzero(pend == 0)[0])
+    bits = np.zeros(len(sch.ready0) * 64, dtype=bool)
+    bits[ready] = True
+    assert np.array_equal(np.packbits(bits, bitorder="little").view(np.uint64), sch.ready0)
+
+    def release(c, out):
+        for s in sch.succ[sch.succ_off[c]:sch.succ_off[c + 1]]:
+            pend[s] -= 1
+            assert pend[s] >= 0
+            if pend[s] == 0:
+                out.append(int(s))
+
+    order = []
+    while ready:
+        j = int(rng.integers(min(window, len(ready))))
+        i = ready.pop(j)
+        order.append(i)
+        new = []
+        early = int(tasks[i]["aux"][3]) - 1 if int(tasks[i]["op"]) == T_LA else -1
+        if early >= 0:
+            release(early, new)
+        release(i, new)
+        g = int(tasks[i]["group"])
+        if g >= 0:
+            count[g] += 1
+            assert count[g] <= sch.ctarget[g]
+            if count[g] == sch.ctarget[g]:
+                release(g, new)
+        ready = sorted(ready + new)
+    assert len(order) == nt, "dynamic schedule left tasks unreleased"
+    return order
