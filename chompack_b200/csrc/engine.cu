@@ -101,7 +101,6 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src) 
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
 }
 
-__device__ __forceinline__ void cp_async_commit_and_wait_later() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Releases the waiters listed in succ[b, e) (warp 0); the first 32 come
@@ -276,16 +275,39 @@ struct SmemLayout {
 
 constexpr int PER_THREAD = (TILE * KC) / NTHREADS;  // staged elements per thread
 
-// Element (r, k) of an operand, already known to be inside [0,rows) x [0,K).
+// Address of element (r, k) of an operand; ok is cleared outside the
+// triangle of OM_TRI_* operands (the caller sets it from the bounds).
 template <int MODE>
-__device__ __forceinline__ double op_elem(const double* __restrict__ X, int ld, int diag, int koff, int r, int k) {
-  if (MODE == OM_N) return __ldcg(X + (int64_t)k * ld + r);
-  if (MODE == OM_T) return __ldcg(X + (int64_t)r * ld + k);
-  if (MODE == OM_TRI_N) return (r + diag >= k) ? __ldcg(X + (int64_t)k * ld + r) : 0.0;
-  if (MODE == OM_TRI_T) return (k + diag >= r) ? __ldcg(X + (int64_t)r * ld + k) : 0.0;
+__device__ __forceinline__ const double* op_addr(const double* X, int ld, int diag, int koff, int r, int k, bool& ok) {
+  if (MODE == OM_N) return X + (int64_t)k * ld + r;
+  if (MODE == OM_T) return X + (int64_t)r * ld + k;
+  if (MODE == OM_TRI_N) {
+    ok = ok && r + diag >= k;
+    return X + (int64_t)k * ld + r;
+  }
+  if (MODE == OM_TRI_T) {
+    ok = ok && k + diag >= r;
+    return X + (int64_t)r * ld + k;
+  }
   // OM_SYM: element (r + diag, k + koff) of a symmetric matrix stored lower
-  int gr = r + diag, gc = k + koff;
-  return (gr >= gc) ? __ldcg(X + (int64_t)gc * ld + gr) : __ldcg(X + (int64_t)gr * ld + gc);
+  const int gr = r + diag, gc = k + koff;
+  return gr >= gc ? X + (int64_t)gc * ld + gr : X + (int64_t)gr * ld + gc;
+}
+
+// 8-byte asynchronous copy global -> shared; zeros when !ok (nothing is read).
+// Tiles written by other CTAs of the launch are read only after an acquire
+// that ordered their writes before this copy, so the L1-allocating form
+// sees them.
+__device__ __forceinline__ void cp_async8_zfill(double* dst, const double* src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Coordinates of the s-th staged element of this thread.  Operands read
@@ -304,25 +326,19 @@ __device__ __forceinline__ void stage_coord(int s, int& r, int& kk) {
   }
 }
 
+// Issues the copies of the operand's K chunk [k0, k0 + KC) into a stage:
+// S[kk*LDS + r] = op(r, k0 + kk), zero outside [0,rows) x [0,K).
 template <int MODE>
-__device__ __forceinline__ void load_chunk_t(const double* __restrict__ X, int ld, int diag, int koff, int rows,
-                                             int k0, int K, double (&v)[PER_THREAD]) {
+__device__ __forceinline__ void issue_chunk_t(const double* __restrict__ X, int ld, int diag, int koff, int rows,
+                                              int k0, int K, double* S) {
 #pragma unroll
   for (int s = 0; s < PER_THREAD; s++) {
     int r, kk;
     stage_coord<MODE>(s, r, kk);
     const int k = k0 + kk;
-    v[s] = (r < rows && k < K) ? op_elem<MODE>(X, ld, diag, koff, r, k) : 0.0;
-  }
-}
-
-template <int MODE>
-__device__ __forceinline__ void store_chunk_t(double* S, const double (&v)[PER_THREAD]) {
-#pragma unroll
-  for (int s = 0; s < PER_THREAD; s++) {
-    int r, kk;
-    stage_coord<MODE>(s, r, kk);
-    S[kk * LDS + r] = v[s];
+    bool ok = r < rows && k < K;
+    const double* src = op_addr<MODE>(X, ld, diag, koff, r, k, ok);
+    cp_async8_zfill(S + kk * LDS + r, ok ? src : X, ok);
   }
 }
 
@@ -342,19 +358,14 @@ __device__ __forceinline__ Opnd make_opnd(const RunArgs& ra, const Operand& o) {
   return p;
 }
 
-__device__ __forceinline__ void load_chunk(const Opnd& o, int rows, int k0, int K, double (&v)[PER_THREAD]) {
+__device__ __forceinline__ void issue_chunk(const Opnd& o, int rows, int k0, int K, double* S) {
   switch (o.mode) {
-    case OM_N: load_chunk_t<OM_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
-    case OM_T: load_chunk_t<OM_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
-    case OM_TRI_N: load_chunk_t<OM_TRI_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
-    case OM_TRI_T: load_chunk_t<OM_TRI_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
-    default: load_chunk_t<OM_SYM>(o.X, o.ld, o.diag, o.koff, rows, k0, K, v); break;
+    case OM_N: issue_chunk_t<OM_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, S); break;
+    case OM_T: issue_chunk_t<OM_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, S); break;
+    case OM_TRI_N: issue_chunk_t<OM_TRI_N>(o.X, o.ld, o.diag, o.koff, rows, k0, K, S); break;
+    case OM_TRI_T: issue_chunk_t<OM_TRI_T>(o.X, o.ld, o.diag, o.koff, rows, k0, K, S); break;
+    default: issue_chunk_t<OM_SYM>(o.X, o.ld, o.diag, o.koff, rows, k0, K, S); break;
   }
-}
-
-__device__ __forceinline__ void store_chunk(int mode, double* S, const double (&v)[PER_THREAD]) {
-  if (mode == OM_T || mode == OM_TRI_T) store_chunk_t<OM_T>(S, v);
-  else store_chunk_t<OM_N>(S, v);
 }
 
 // Double-precision tensor-core MMA, m16n8k4 (sm_90+):
@@ -414,28 +425,41 @@ __device__ __forceinline__ void zero_acc(Acc& acc) {
       for (int h = 0; h < 4; h++) acc[i][j][h] = 0.0;
 }
 
-// acc = opA * opB^T over K, with the next K chunk's global loads in flight
-// while the current chunk is multiplied.
+// acc = opA * opB^T over K through a GEMM_STAGES-deep ring of K chunks in
+// shared memory: the copies of chunk c + GEMM_STAGES - 1 are in flight while
+// chunk c is multiplied; one barrier per chunk.
+constexpr int GEMM_STAGES = 4;
+constexpr int STAGE_DOUBLES = 2 * KC * LDS;  // A chunk, then B chunk
+
 __device__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm, Acc& acc) {
   zero_acc(acc);
-  double va[PER_THREAD], vb[PER_THREAD];
-  if (K > 0) {
-    load_chunk(A, m, 0, K, va);
-    load_chunk(B, n, 0, K, vb);
-  }
-  for (int k0 = 0; k0 < K; k0 += KC) {
-    store_chunk(A.mode, sm.A, va);
-    store_chunk(B.mode, sm.B, vb);
-    __syncthreads();
-    if (k0 + KC < K) {
-      load_chunk(A, m, k0 + KC, K, va);
-      load_chunk(B, n, k0 + KC, K, vb);
+  const int nch = (K + KC - 1) / KC;
+  double* const ring = sm.A;
+#pragma unroll
+  for (int c = 0; c < GEMM_STAGES - 1; c++) {
+    if (c < nch) {
+      issue_chunk(A, m, c * KC, K, ring + c * STAGE_DOUBLES);
+      issue_chunk(B, n, c * KC, K, ring + c * STAGE_DOUBLES + KC * LDS);
     }
-    int kn = min(KC, K - k0);
-    kn = (kn + 3) & ~3;
-    mma_block(sm.A, sm.B, kn, acc);
-    __syncthreads();
+    cp_async_commit();
   }
+  for (int c = 0; c < nch; c++) {
+    cp_async_wait_group<GEMM_STAGES - 2>();  // this thread's copies of chunk c
+    __syncthreads();                         // everyone's; and chunk c - 1 is consumed
+    const int cn = c + GEMM_STAGES - 1;
+    if (cn < nch) {
+      double* d = ring + (cn % GEMM_STAGES) * STAGE_DOUBLES;
+      issue_chunk(A, m, cn * KC, K, d);
+      issue_chunk(B, n, cn * KC, K, d + KC * LDS);
+    }
+    cp_async_commit();
+    const double* st = ring + (c % GEMM_STAGES) * STAGE_DOUBLES;
+    int kn = min(KC, K - c * KC);
+    kn = (kn + 3) & ~3;
+    mma_block(st, st + KC * LDS, kn, acc);
+  }
+  cp_async_wait_group<0>();
+  __syncthreads();
 }
 
 // C = alpha*acc + beta*C (masked to m x n and, for lower, to r + cdiag >= c).
@@ -713,11 +737,12 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
       // broadcast and the other updates run beside it.
       double* colb = sT;  // free until the inverse assembly: 2 x 16 doubles
       double dn = a[0];
+      int first_bad = -1;  // first non-positive pivot, reported once after the loop
 #pragma unroll
       for (int jj = 0; jj < 16; jj++) {
         const double d = __shfl_sync(0xffffffffu, dn, jj);
         const bool bad = !(d > 0.0);
-        if (bad && lane == 0 && j0 + jj < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + jj + 1);
+        first_bad = (bad && first_bad < 0) ? jj : first_bad;
         const double x = bad ? 1.0 : d;
         const double rs = rsqrt(x);
         const double l = (il == jj) ? x * rs : a[jj] * rs;
@@ -732,6 +757,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
           if (il >= kk) a[kk] = fma(-l, lkj, a[kk]);
         }
       }
+      if (lane == 0 && first_bad >= 0 && j0 + first_bad < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + first_bad + 1);
       if (lane < 16) {
 #pragma unroll
         for (int c = 0; c < 16; c++)
@@ -1417,7 +1443,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
             s_succ[1] = e;
           }
           if (lane < e - b) cp_async4(&s_pre[lane], ra.succ + b + lane);
-          cp_async_commit_and_wait_later();
+          cp_async_commit();
           if (lane == 0 && ra.trace) {
             ra.trace[4 * (int64_t)c] = t0;
             ra.trace[4 * (int64_t)c + 1] = global_ns();
@@ -1501,6 +1527,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
 }
 
 static_assert(2 * TILE * LDS <= ENGINE_SMEM_BASE_DOUBLES, "GEMM staging exceeds the engine's shared memory");
+static_assert(GEMM_STAGES * STAGE_DOUBLES <= ENGINE_SMEM_BASE_DOUBLES, "GEMM ring exceeds the engine's shared memory");
 static_assert(POTRF_SMEM_DOUBLES <= ENGINE_SMEM_BASE_DOUBLES, "POTRF exceeds the engine's shared memory");
 
 size_t engine_smem_bytes() { return (size_t)ENGINE_SMEM_DOUBLES * sizeof(double); }
