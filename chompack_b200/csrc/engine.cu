@@ -11,9 +11,10 @@
 //
 // Dense FP64 tile arithmetic uses the double-precision tensor-core MMA
 // (mma.sync m16n8k4 f64): a 64x64 C tile is split over 4 warps, 32x32 each.
-// Operand tiles are staged through shared memory with L2-coherent loads
-// (__ldcg), since tiles produced by other CTAs in the same launch must not be
-// read from a stale L1 line.
+// GEMM operand tiles are staged through a ring of shared-memory K chunks by
+// cp.async; tiles produced by other CTAs in the same launch are read only
+// after an acquire that ordered their writes before the read.  The other
+// tasks read with L2-coherent loads (__ldcg).
 #include <cuda_runtime.h>
 #include <cstdint>
 
