@@ -85,6 +85,12 @@ sym_weight = _sig("chb_sym_weight", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_doubl
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
 set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 plan_set_schedule = _sig("chb_plan_set_schedule", ctypes.c_int, [PPLAN, ctypes.c_int])
+io_flags = _sig("chb_io_flags", ctypes.c_int, [ctypes.c_int, ctypes.c_int])
+io_overlap_available = _sig("chb_io_overlap_available", ctypes.c_int, [])
+cholesky_io = _sig("chb_cholesky_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
+projected_inverse_io = _sig("chb_projected_inverse_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
+llt_io = _sig("chb_llt_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
+program_io = _sig("chb_program_io", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64, vp, vp, vp, vp])
 
 OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)
 HESSIAN_MAX_U = 59   # U matrices per chb_hessian call (base slots 5..63)

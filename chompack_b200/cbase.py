@@ -4,10 +4,15 @@ C ABI of include/chompack_b200.h.
 
 Each call uploads nothing but what changed: the symbolic factorisation is
 uploaded once per `symbolic` object (its Plan), the task program of each
-sweep is compiled once, and the workspace is reused.  Values stay in the
-cspmatrix's CUDA float64 tensor, transformed in place.  Calls are
-synchronous like the reference's (they read the device status to raise
-ArithmeticError); the `*_async` variants in `chompack_b200.engine` skip that.
+sweep is compiled once, and the workspace is reused.  Calls are synchronous
+like the reference's (they read the device status to raise ArithmeticError).
+
+Values live either in a CUDA float64 tensor (transformed in place on the
+device) or, as in the reference, in host memory (a CPU float64 tensor,
+pinned for the copies to overlap).  Host values keep a device mirror on the
+cspmatrix: cholesky, projected_inverse and llt stream the values in while
+the sweep runs (unless the mirror already holds them) and each finished
+chunk of the result back out; the other sweeps copy in, run, copy out.
 """
 import ctypes
 
@@ -18,13 +23,73 @@ from . import _native as N
 __all__ = ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot"]
 
 
-def _values(X, name="X"):
+def _on_host(X):
     v = X.blkval
-    if not isinstance(v, torch.Tensor) or v.device.type != "cuda":
-        raise RuntimeError("%s.blkval must be a CUDA tensor: the sweeps run on the GPU only" % name)
+    return isinstance(v, torch.Tensor) and v.device.type == "cpu"
+
+
+def _values(X, name="X"):
+    """Device values of X: its CUDA tensor, or for host values the device
+    mirror, brought up to date with a copy if the host values changed."""
+    v = X.blkval
+    if not isinstance(v, torch.Tensor) or v.device.type not in ("cuda", "cpu"):
+        raise RuntimeError("%s.blkval must be a float64 tensor" % name)
     if v.dtype != torch.float64 or not v.is_contiguous():
         raise ValueError("%s.blkval must be a contiguous float64 tensor" % name)
-    return v
+    if v.device.type == "cuda":
+        return v
+    m = _mirror(X, X.symb.plan())
+    if not _synced(X):
+        m.copy_(v)
+        _mark_synced(X)
+    return m
+
+
+def _mirror(X, plan):
+    dev = torch.device("cuda", plan.device)
+    m = X.__dict__.get("_dev")
+    if m is None or m.device != dev or m.numel() != X.blkval.numel():
+        m = torch.empty(X.blkval.numel(), dtype=torch.float64, device=dev)
+        X._dev = m
+        X._dev_tag = None
+    return m
+
+
+def _synced(X):
+    v = X.blkval
+    return X.__dict__.get("_dev_tag") == (v.data_ptr(), v._version)
+
+
+def _mark_synced(X):
+    v = X.blkval
+    X._dev_tag = (v.data_ptr(), v._version)
+
+
+def _write_back(X):
+    """After an in-place sweep on the device mirror of host values."""
+    if _on_host(X):
+        X.blkval.copy_(X._dev)
+        _mark_synced(X)
+
+
+def _streamed(X, op, launch, name="X"):
+    """A streamed sweep on host values: chunks go in (unless the mirror
+    holds them) while the sweep runs, and come back out as they finish."""
+    v = X.blkval
+    if v.dtype != torch.float64 or not v.is_contiguous():
+        raise ValueError("%s.blkval must be a contiguous float64 tensor" % name)
+    plan = X.symb.plan()
+    m = _mirror(X, plan)
+    host_in = None if _synced(X) else v.data_ptr()
+    flags = N.io_flags(host_in is not None, 1)
+    dev = torch.device("cuda", plan.device)
+    ws, nbytes = plan.workspace(op, 0, flags)
+    s = _stream(dev)
+    _check(launch(plan.handle, host_in, v.data_ptr(), m.data_ptr(), ws, nbytes, s), "launch")
+    info = N.info(plan.handle, ws, s)
+    _check(info, "sweep")
+    _mark_synced(X)
+    return info
 
 
 def _stream(dev):
@@ -51,10 +116,13 @@ def cholesky(X):
     (cbase.c:176-284).  On exit X holds the factor and X.is_factor is True."""
     if X.is_factor is not False:
         raise ValueError("X must be a cspmatrix")
-    v = _values(X)
-    plan = X.symb.plan(v.device.index)
-    info = _run_and_status(plan, N.OP_CHOLESKY,
-                           lambda ws, nb, s: N.cholesky(plan.handle, v.data_ptr(), ws, nb, s))
+    if _on_host(X):
+        info = _streamed(X, N.OP_CHOLESKY, N.cholesky_io)
+    else:
+        v = _values(X)
+        plan = X.symb.plan(v.device.index)
+        info = _run_and_status(plan, N.OP_CHOLESKY,
+                               lambda ws, nb, s: N.cholesky(plan.handle, v.data_ptr(), ws, nb, s))
     X.is_factor = True
     if info:
         raise ArithmeticError("factorization failed")
@@ -65,10 +133,13 @@ def projected_inverse(L):
     (cbase.c:393-500).  On exit L holds Y and L.is_factor is False."""
     if L.is_factor is not True:
         raise ValueError("X must be a cspmatrix")
-    v = _values(L)
-    plan = L.symb.plan(v.device.index)
-    info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
-                           lambda ws, nb, s: N.projected_inverse(plan.handle, v.data_ptr(), ws, nb, s))
+    if _on_host(L):
+        info = _streamed(L, N.OP_PROJECTED_INVERSE, N.projected_inverse_io)
+    else:
+        v = _values(L)
+        plan = L.symb.plan(v.device.index)
+        info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
+                               lambda ws, nb, s: N.projected_inverse(plan.handle, v.data_ptr(), ws, nb, s))
     L.is_factor = False
     if info:
         raise ArithmeticError("partial inverse failed")
@@ -79,9 +150,12 @@ def llt(L):
     (cbase.c:287-390).  On exit L holds X and L.is_factor is False."""
     if L.is_factor is not True:
         raise ValueError("X must be a cspmatrix")
-    v = _values(L)
-    plan = L.symb.plan(v.device.index)
-    _run_and_status(plan, N.OP_LLT, lambda ws, nb, s: N.llt(plan.handle, v.data_ptr(), ws, nb, s))
+    if _on_host(L):
+        _streamed(L, N.OP_LLT, N.llt_io)
+    else:
+        v = _values(L)
+        plan = L.symb.plan(v.device.index)
+        _run_and_status(plan, N.OP_LLT, lambda ws, nb, s: N.llt(plan.handle, v.data_ptr(), ws, nb, s))
     L.is_factor = False
 
 
@@ -172,6 +246,7 @@ def completion(X, factored_updates=True):
     fu = 1 if factored_updates is True else 0
     info = _run_and_status(plan, N.OP_COMPLETION,
                            lambda ws, nb, s: N.completion(plan.handle, v.data_ptr(), fu, ws, nb, s), k=fu)
+    _write_back(X)
     X.is_factor = True
     if info:
         raise ArithmeticError("completion failed")
@@ -220,5 +295,7 @@ def hessian(L, Y, U, adj=False, inv=False, factored_updates=True):
                 plan, N.OP_HESSIAN,
                 lambda ws, nb, s: N.hessian(plan.handle, lv.data_ptr(), yv.data_ptr(), arr, len(chunk), a, inv_i,
                                             fu, ws, nb, s), k=len(chunk), flags=flags)
+    for u in Us:
+        _write_back(u)
     if info:
         raise ArithmeticError("hessian failed")

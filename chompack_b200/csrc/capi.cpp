@@ -28,7 +28,44 @@ int run_op(chb_plan* plan, int op, int64_t k, int flags, double* const* bases, i
   return run_program(plan, prog, work, work_bytes, bases, nbases, (cudaStream_t)stream, ldb, alpha);
 }
 
+// A sweep on values held in host memory (see chb_cholesky_io).
+int run_io(chb_plan* plan, int op, const double* host_in, double* host_out, double* dev_blkval, void* work,
+           size_t work_bytes, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  if (!dev_blkval) return set_error(-1, "null device values");
+  const int flags = (host_in ? PF_IO_IN : 0) | (host_out ? PF_IO_OUT : 0);
+  Program* prog = get_program(plan, op, 0, flags);
+  if (!prog) return -2;
+  double* bases[1] = {dev_blkval};
+  if (!flags) return run_program(plan, prog, work, work_bytes, bases, 1, (cudaStream_t)stream);
+  HostIo io;
+  io.host_in = host_in;
+  io.host_out = host_out;
+  return run_program(plan, prog, work, work_bytes, bases, 1, (cudaStream_t)stream, 0, 1.0, &io);
+}
+
 }  // namespace
+
+extern "C" int chb_io_flags(int host_in, int host_out) {
+  return (host_in ? PF_IO_IN : 0) | (host_out ? PF_IO_OUT : 0);
+}
+
+extern "C" int chb_cholesky_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval,
+                               void* work, size_t work_bytes, void* stream) {
+  return run_io(plan, CHB_OP_CHOLESKY, host_in, host_out, dev_blkval, work, work_bytes, stream);
+}
+
+extern "C" int chb_projected_inverse_io(chb_plan* plan, const double* host_in, double* host_out,
+                                        double* dev_blkval, void* work, size_t work_bytes, void* stream) {
+  return run_io(plan, CHB_OP_PROJECTED_INVERSE, host_in, host_out, dev_blkval, work, work_bytes, stream);
+}
+
+extern "C" int chb_llt_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval, void* work,
+                          size_t work_bytes, void* stream) {
+  return run_io(plan, CHB_OP_LLT, host_in, host_out, dev_blkval, work, work_bytes, stream);
+}
 
 extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
   double* bases[1] = {blkval};

@@ -92,6 +92,115 @@ struct DagBuilder {
     if (group >= 0) waits[task].push_back({group, -1, true});
   }
 
+  // Incoming chunks (whole supernodes) that a task reads or writes: those
+  // holding the start of each operand on the values (base B_X).
+  static void in_chunks(const Task& t, const IoSpec& io, std::vector<int>& out) {
+    out.clear();
+    if (t.op == T_NOP || t.op == T_SIGNAL || t.op == T_ARRIVAL) return;
+    auto add_off = [&](int64_t off) {
+      const int j = (int)(std::upper_bound(io.in_off.begin(), io.in_off.end(), off) - io.in_off.begin()) - 1;
+      if (j >= 0 && j + 1 < (int)io.in_off.size() && std::find(out.begin(), out.end(), j) == out.end())
+        out.push_back(j);
+    };
+    for (const Operand* o : {&t.a, &t.b, &t.c})
+      if (o->base == B_X && o->ld > 0) add_off(o->off);
+    if (t.op == T_MROW && t.aux[0] == B_X) add_off((int64_t)(uint32_t)t.aux[2] | ((int64_t)t.aux[3] << 32));
+  }
+
+  // Outgoing chunks that a task's writes to the values overlap.  A written
+  // tile of at most e rows and columns (e = max(m, n)) spans
+  // [off, off + (e-1)*ld + e); an extend-add writes the front's columns
+  // [aux[1], aux[2]).
+  static void out_chunks(const Task& t, const IoSpec& io, std::vector<int>& out) {
+    out.clear();
+    auto add_range = [&](int64_t lo, int64_t hi) {
+      const auto& v = io.out_off;
+      int j = (int)(std::upper_bound(v.begin(), v.end(), lo) - v.begin()) - 1;
+      for (j = std::max(j, 0); j + 1 < (int)v.size() && v[j] < hi; j++)
+        if (std::find(out.begin(), out.end(), j) == out.end()) out.push_back(j);
+    };
+    const int64_t e = std::max(std::max(t.m, t.n), 1);
+    auto tile = [&](const Operand& o) {
+      if (o.base == B_X && o.ld > 0) add_range(o.off, o.off + (e - 1) * o.ld + e);
+    };
+    switch (t.op) {
+      case T_NOP: case T_SIGNAL: case T_ARRIVAL: case T_EXTRACT: break;  // an extract writes the workspace
+      case T_GEMM: case T_MROW: case T_COPY: case T_SUM: tile(t.c); break;
+      case T_LA: tile(t.a); tile(t.c); break;
+      case T_POTRF: tile(t.a); if (t.aux[1]) tile(t.c); break;
+      case T_ASM:
+        if (t.a.base == B_X && t.a.ld > 0) add_range(t.a.off + (int64_t)t.aux[1] * t.a.ld, t.a.off + (int64_t)t.aux[2] * t.a.ld);
+        tile(t.c);
+        break;
+      default: tile(t.a); tile(t.b); tile(t.c); break;
+    }
+  }
+
+  // Streaming of the values (see IoSpec): per incoming chunk a T_ARRIVAL
+  // task (it waits for the host's copy, its estimated duration is the
+  // chunk's arrival time) that every task touching the chunk waits on; per
+  // outgoing chunk a fan-in of T_NOP tasks (at most 64 waits each, so that
+  // no single task walks a long wait list) under one T_SIGNAL.  Arrival
+  // tasks are created after the sweep's tasks, which breaks the creation
+  // order's topology; finish() ranks and orders them first.
+  std::vector<int> arrival_of_chunk;  // T_ARRIVAL task of each incoming chunk
+
+  void apply_io(const IoSpec& io, std::vector<int>& signal_of_chunk) {
+    signal_of_chunk.clear();
+    arrival_of_chunk.clear();
+    if (!io.in && !io.out) return;
+    const int nin = io.in ? (int)io.in_off.size() - 1 : 0;
+    const int nch = io.out ? (int)io.out_off.size() - 1 : 0;
+    const int nt0 = (int)tasks.size();
+    std::vector<int> arr(nin, -1);
+    if (io.in)
+      for (int j = 0; j < nin; j++) {
+        Task a;
+        std::memset(&a, 0, sizeof(a));
+        a.op = T_ARRIVAL;
+        a.aux[0] = j;
+        arr[j] = add(a, SchedKey{-1, 0, 0, 0, j, 0}, -1, io.arrive_us[j]);
+      }
+    arrival_of_chunk = arr;
+    std::vector<std::vector<int>> touch(nch);
+    std::vector<int> ch;
+    for (int t = 0; t < nt0; t++) {
+      if (io.in) {
+        in_chunks(tasks[t], io, ch);
+        for (int j : ch) wait_task(t, arr[j]);
+      }
+      if (io.out) {
+        out_chunks(tasks[t], io, ch);
+        for (int j : ch) touch[j].push_back(t);
+      }
+    }
+    if (!io.out) return;
+    signal_of_chunk.assign(nch, -1);
+    for (int j = 0; j < nch; j++) {
+      std::vector<int> level = touch[j];
+      SchedKey key{1 << 30, 0, 0, 0, j, 0};
+      while (level.size() > 64) {
+        std::vector<int> up;
+        for (size_t i = 0; i < level.size(); i += 64) {
+          Task n;
+          std::memset(&n, 0, sizeof(n));
+          n.op = T_NOP;
+          const int id = add(n, key, -1, 0.5);
+          for (size_t u = i; u < std::min(level.size(), i + 64); u++) wait_task(id, level[u]);
+          up.push_back(id);
+        }
+        level.swap(up);
+      }
+      Task sg;
+      std::memset(&sg, 0, sizeof(sg));
+      sg.op = T_SIGNAL;
+      sg.aux[0] = j;
+      const int id = add(sg, key, -1, 0.5);
+      for (int u : level) wait_task(id, u);
+      signal_of_chunk[j] = id;
+    }
+  }
+
   // Rough duration model of a task on one CTA (microseconds); only the
   // relative sizes matter for the priority order.
   static double estimate(const Task& t) {
@@ -118,29 +227,34 @@ struct DagBuilder {
   // device's CTAs, which claim tasks in list order, follow a schedule that
   // keeps the critical path moving while ready work fills the machine.
   int finish(Program& prog, int slots = 296) {
+    std::vector<int> signal_of_chunk;
+    apply_io(prog.io, signal_of_chunk);
     const int nt = (int)tasks.size();
     const int ng = (int)group_size.size();
     std::vector<std::vector<int>> members(ng);
     for (int t = 0; t < nt; t++)
       if (group_of[t] >= 0) members[group_of[t]].push_back(t);
-    std::vector<double> rank(nt, 0.0);
-    // creation order is topological (every wait names an earlier task)
-    for (int t = nt - 1; t >= 0; t--) {
-      rank[t] += cost[t];
-      for (const Wait& wt : waits[t]) {
-        if (wt.is_group) {
-          const int o = early_owner[wt.id];
-          if (o >= 0 && o < t) rank[o] = std::max(rank[o], rank[t] + early_at[o] - cost[o]);
-          for (int u : members[wt.id])
-            if (u < t) rank[u] = std::max(rank[u], rank[t]);
-        } else if (wt.id < t) {
-          rank[wt.id] = std::max(rank[wt.id], rank[t]);
+    std::vector<double> rank(nt, 0.0), start(nt, 0.0), extra(nt, 0.0);
+    auto compute_rank = [&]() {
+      std::fill(rank.begin(), rank.end(), 0.0);
+      // creation order is topological (every wait names an earlier task)
+      for (int t = nt - 1; t >= 0; t--) {
+        rank[t] += cost[t] + extra[t];
+        for (const Wait& wt : waits[t]) {
+          if (wt.is_group) {
+            const int o = early_owner[wt.id];
+            if (o >= 0 && o < t) rank[o] = std::max(rank[o], rank[t] + early_at[o] - cost[o]);
+            for (int u : members[wt.id])
+              if (u < t) rank[u] = std::max(rank[u], rank[t]);
+          } else if (wt.id < t) {
+            rank[wt.id] = std::max(rank[wt.id], rank[t]);
+          }
         }
       }
-    }
+    };
     // waiters of each task / group, and unmet wait counts
     std::vector<std::vector<int>> task_waiters(nt), group_waiters(ng);
-    std::vector<int> unmet(nt, 0);
+    std::vector<int> unmet0(nt, 0);
     for (int t = 0; t < nt; t++) {
       for (const Wait& wt : waits[t]) {
         if (wt.is_group) {
@@ -149,48 +263,101 @@ struct DagBuilder {
         } else {
           task_waiters[wt.id].push_back(t);
         }
-        unmet[t]++;
+        unmet0[t]++;
       }
     }
-    std::vector<int> group_left(group_size.begin(), group_size.end());
-    std::vector<double> start(nt, 0.0);
-    {
-      auto by_rank = [&](int a, int b) { return rank[a] < rank[b] || (rank[a] == rank[b] && b < a); };
-      std::priority_queue<int, std::vector<int>, decltype(by_rank)> ready(by_rank);
-      typedef std::pair<double, int> Ev;
-      std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
-      for (int t = 0; t < nt; t++)
-        if (unmet[t] == 0) ready.push(t);
-      int free_slots = std::max(slots, 1);
-      double now = 0.0;
-      int done = 0;
-      auto release = [&](int w) {
-        if (--unmet[w] == 0) ready.push(w);
-      };
-      while (done < nt) {
-        while (free_slots > 0 && !ready.empty()) {
-          int t = ready.top();
-          ready.pop();
-          start[t] = now;
-          running.push({now + std::max(cost[t], 1e-3), t});
-          if (early_of[t] >= 0) running.push({now + std::min(early_at[t], cost[t]), -1 - early_of[t]});
-          free_slots--;
+    auto simulate = [&]() -> int {
+      std::vector<int> unmet = unmet0;
+      std::vector<int> group_left(group_size.begin(), group_size.end());
+      {
+        auto by_rank = [&](int a, int b) { return rank[a] < rank[b] || (rank[a] == rank[b] && b < a); };
+        std::priority_queue<int, std::vector<int>, decltype(by_rank)> ready(by_rank);
+        typedef std::pair<double, int> Ev;
+        std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> running;
+        for (int t = 0; t < nt; t++)
+          if (unmet[t] == 0) ready.push(t);
+        int free_slots = std::max(slots, 1);
+        double now = 0.0;
+        int done = 0;
+        auto release = [&](int w) {
+          if (--unmet[w] == 0) ready.push(w);
+        };
+        while (done < nt) {
+          while (free_slots > 0 && !ready.empty()) {
+            int t = ready.top();
+            ready.pop();
+            start[t] = now;
+            running.push({now + std::max(cost[t], 1e-3), t});
+            if (early_of[t] >= 0) running.push({now + std::min(early_at[t], cost[t]), -1 - early_of[t]});
+            free_slots--;
+          }
+          if (running.empty()) return set_error(-23, "task graph: unsatisfiable waits");
+          Ev e = running.top();
+          running.pop();
+          now = e.first;
+          if (e.second < 0) {  // an early signal: release its waiters, no slot freed
+            for (int w : group_waiters[-1 - e.second]) release(w);
+            continue;
+          }
+          free_slots++;
+          done++;
+          const int t = e.second;
+          for (int w : task_waiters[t]) release(w);
+          if (group_of[t] >= 0 && --group_left[group_of[t]] == 0)
+            for (int w : group_waiters[group_of[t]]) release(w);
         }
-        if (running.empty()) return set_error(-23, "task graph: unsatisfiable waits");
-        Ev e = running.top();
-        running.pop();
-        now = e.first;
-        if (e.second < 0) {  // an early signal: release its waiters, no slot freed
-          for (int w : group_waiters[-1 - e.second]) release(w);
-          continue;
-        }
-        free_slots++;
-        done++;
-        const int t = e.second;
-        for (int w : task_waiters[t]) release(w);
-        if (group_of[t] >= 0 && --group_left[group_of[t]] == 0)
-          for (int w : group_waiters[group_of[t]]) release(w);
       }
+      return 0;
+    };
+    // Output signals: a signal's rank includes the copy time of its chunk
+    // and of every chunk signalled after it (at ~50 GB/s), so that the tasks
+    // that complete a chunk rank as if the copies were the rest of the sweep
+    // (otherwise nothing waits on them and the schedule leaves them last).
+    compute_rank();
+    if (simulate() != 0) return -23;
+    if (!arrival_of_chunk.empty()) {
+      // Incoming copies in earliest-deadline order: chunk j is due at the
+      // latest start (critical path minus upward rank) of the first task
+      // that touches it; each arrival task's duration becomes the time its
+      // chunk arrives in that order (~50 GB/s).
+      const int nin = (int)arrival_of_chunk.size();
+      double tend = 0.0;
+      for (int t = 0; t < nt; t++) tend = std::max(tend, rank[t]);
+      std::vector<double> due(nin, tend);
+      std::vector<int> chunk_of_arrival(nt, -1);
+      for (int j = 0; j < nin; j++) chunk_of_arrival[arrival_of_chunk[j]] = j;
+      for (int t = 0; t < nt; t++)
+        for (const Wait& wt : waits[t])
+          if (!wt.is_group && chunk_of_arrival[wt.id] >= 0) {
+            const int j = chunk_of_arrival[wt.id];
+            due[j] = std::min(due[j], tend - rank[t]);
+          }
+      std::vector<int>& ord = prog.io.in_order;
+      ord.resize(nin);
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return due[x] < due[y]; });
+      double at = 0.0;
+      for (int j : ord) {
+        at += (prog.io.in_off[j + 1] - prog.io.in_off[j]) * 8.0 / 5e4;
+        cost[arrival_of_chunk[j]] = at;
+      }
+      compute_rank();
+      if (simulate() != 0) return -23;
+    }
+    if (!signal_of_chunk.empty()) {
+      const int nch = (int)signal_of_chunk.size();
+      std::vector<int> ch(nch);
+      std::iota(ch.begin(), ch.end(), 0);
+      std::sort(ch.begin(), ch.end(),
+                [&](int x, int y) { return start[signal_of_chunk[x]] < start[signal_of_chunk[y]]; });
+      double tail = 0.0;
+      for (int i = nch - 1; i >= 0; i--) {
+        const int j = ch[i];
+        tail += (prog.io.out_off[j + 1] - prog.io.out_off[j]) * 8.0 / 5e4;
+        extra[signal_of_chunk[j]] = tail;
+      }
+      compute_rank();
+      if (simulate() != 0) return -23;
     }
     std::vector<int> order(nt);
     std::iota(order.begin(), order.end(), 0);
@@ -241,7 +408,14 @@ struct DagBuilder {
       prog.waits.insert(prog.waits.end(), w.begin(), w.end());
       prog.tasks[i] = tk;
     }
-    prog.ncounters = (int64_t)nt + (int64_t)group_size.size();
+    prog.ncounters = (int64_t)nt + (int64_t)ng;
+    prog.out_order.clear();
+    if (!signal_of_chunk.empty()) {
+      std::vector<int> ch(signal_of_chunk.size());
+      std::iota(ch.begin(), ch.end(), 0);
+      std::sort(ch.begin(), ch.end(), [&](int x, int y) { return pos[signal_of_chunk[x]] < pos[signal_of_chunk[y]]; });
+      prog.out_order = ch;
+    }
     // dynamic scheduling data: waits per task, waiters per counter, the
     // value at which each counter is complete, the initially ready tasks
     const int64_t nc = prog.ncounters;

@@ -35,6 +35,41 @@ __device__ __forceinline__ void red_release_add(int* p, int v) {
 
 __device__ __forceinline__ int ld_volatile(const int* p) { return *((const volatile int*)p); }
 
+__device__ __forceinline__ int ld_acquire_sys(const int* p) {
+  int v;
+  asm volatile("ld.acquire.sys.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until the copy of incoming chunk j has raised its flag (the host
+// stream copies the chunk, then the flag).  Bounded like every wait: on
+// timeout DE_TIMEOUT is recorded and the sweep leaves.
+__device__ void wait_arrival(const RunArgs& ra, int j) {
+  if (j < 0 || j >= ra.nio_in) {
+    atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
+    return;
+  }
+  int64_t spins = 0;
+  unsigned ns = 64;
+  while (ld_acquire_sys(ra.io_in + j) == 0) {
+    if (++spins > ra.spin_limit) {
+      atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+      atomicAdd(&ra.ctl[3], 1);
+      return;
+    }
+    if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) return;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
+}
+
+// Host-visible flag: the CTA's earlier writes (ordered by the caller's
+// __syncthreads) become visible to the copy engines before the flag.
+__device__ __forceinline__ void raise_io_flag(int* p) {
+  __threadfence_system();
+  asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(1) : "memory");
+}
+
 __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -1505,6 +1540,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_QL: run_ql(ra, t, smem); break;
       case T_NOP: break;
       case T_SUM: run_sum(ra, t); break;
+      case T_SIGNAL:
+        if (threadIdx.x == 0 && t.aux[0] >= 0 && t.aux[0] < ra.nio_out) raise_io_flag(ra.io_out + t.aux[0]);
+        break;
+      case T_ARRIVAL:
+        if (threadIdx.x == 0) wait_arrival(ra, t.aux[0]);
+        break;
       default:
         if (threadIdx.x == 0) atomicCAS(&ra.ctl[1], 0, DE_BAD_TASK);
         break;
@@ -1524,6 +1565,13 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       const int nx = finish_task(ra, ti, t.group, s_succ[0], s_succ[1], s_pre);
       if (threadIdx.x == 0) s_next = nx;
     }
+  }
+  if (ra.nio_out > 0) {
+    // the last CTA to leave raises every output flag (already raised after a
+    // complete sweep; after an aborted one the waiting copies still proceed)
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&ra.ctl[6], 1) == (int)gridDim.x - 1)
+      for (int j = 0; j < ra.nio_out; j++) raise_io_flag(ra.io_out + j);
   }
 }
 

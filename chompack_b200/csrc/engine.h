@@ -76,7 +76,9 @@ enum TaskOp : uint8_t {
   T_VEC = 9,      // vector ops for the triangular solve sweep
   T_NOP = 10,     // no work: joins dependencies
   T_LA = 11,      // Cholesky look-ahead: L = A21 M^T (early signal), A22 -= L L^T
-  T_SUM = 12      // C = alpha * sum of aux[0] partial tiles (stride aux[1]) + beta * C
+  T_SUM = 12,     // C = alpha * sum of aux[0] partial tiles (stride aux[1]) + beta * C
+  T_SIGNAL = 13,  // host-visible flag io_out[aux[0]] = 1 (a chunk of the values is final)
+  T_ARRIVAL = 14  // waits (bounded) until the host's copy raised io_in[aux[0]] (a chunk arrived)
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the
@@ -157,6 +159,13 @@ struct RunArgs {
   const int* succ_off;            // ncounters + 1
   const int* succ;
   const int* ctarget;             // value at which a counter is complete
+  // Streamed output: T_SIGNAL raises io_out[chunk] (system scope) when a
+  // chunk of the values is final; the last CTA to leave raises all nio_out
+  // flags, so that copies waiting on them never wait on an aborted sweep.
+  int* io_out;
+  int nio_out;
+  int nio_in;
+  int* io_in;    // arrival flags, raised by the copies of the incoming chunks
 };
 
 // Sub-operations of T_VEC (triangular solve sweep).

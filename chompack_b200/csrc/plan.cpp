@@ -70,11 +70,61 @@ static int upload_program(Program& prog) {
 
 // Builds the host side of a program only (no device upload); used by the
 // introspection entry points, which must work without a GPU.
+// Chunks of the values for streaming (at most 24 each way: the arrival
+// flags are control words 8..31, the output flags 32..55).  Incoming: cut at
+// the first supernode boundary after 1/24 of the values.  Outgoing: the
+// same, and a supernode larger than that is cut between 64-column tiles
+// (its block is column-major, so column ranges are contiguous).
+static IoSpec make_io_spec(const chb_plan& plan, bool in, bool out) {
+  IoSpec io;
+  io.in = in;
+  io.out = out;
+  const int64_t total = plan.blk_total;
+  auto cut = [&](int64_t target, bool split, std::vector<int64_t>& off) {
+    off.assign(1, 0);
+    for (int64_t k = 0; k < plan.nsn; k++) {
+      const chb::FrontDesc& f = plan.fronts[k];
+      const int64_t beg = f.blk, end = (k + 1 < plan.nsn) ? plan.fronts[k + 1].blk : total;
+      if (split && end - beg > target && f.nj > 0) {
+        const int64_t cols = std::max<int64_t>(64, (target / f.nj) / 64 * 64);
+        for (int64_t c = cols; c < f.nn; c += cols) {
+          const int64_t o = beg + c * f.nj;
+          if (o - off.back() >= target / 2) off.push_back(o);
+        }
+      }
+      if (end - off.back() >= target && end < total) off.push_back(end);
+    }
+    off.push_back(total);
+  };
+  const int64_t t0 = std::max<int64_t>(total / 24, 1);
+  cut(t0, false, io.in_off);
+  for (int64_t t = t0;; t += t0 / 4 + 1) {
+    cut(t, true, io.out_off);
+    if (io.out_off.size() <= 25) break;
+  }
+  // arrival estimates at ~50 GB/s (only the list order uses them)
+  for (size_t j = 0; j + 1 < io.in_off.size(); j++) io.arrive_us.push_back(io.in_off[j + 1] * 8.0 / 5e4);
+  return io;
+}
+
 Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   ProgKey key{op, k, flags};
   auto it = plan->progs.find(key);
   if (it != plan->progs.end()) return it->second.get();
   std::unique_ptr<Program> prog(new Program());
+  const int io = flags & (PF_IO_IN | PF_IO_OUT);
+  if (io) {
+    if (op != CHB_OP_CHOLESKY && op != CHB_OP_PROJECTED_INVERSE && op != CHB_OP_LLT) {
+      set_error(-2, "streamed values are available for cholesky, projected_inverse and llt");
+      return nullptr;
+    }
+    if (plan->blk_total <= 0) {
+      set_error(-2, "streamed values: empty factorisation");
+      return nullptr;
+    }
+    prog->io = make_io_spec(*plan, (io & PF_IO_IN) != 0, (io & PF_IO_OUT) != 0);
+    flags &= ~(PF_IO_IN | PF_IO_OUT);
+  }
   int rc;
   switch (op) {
     case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
@@ -111,8 +161,43 @@ Program* get_program(chb_plan* plan, int op, int64_t k, int flags) {
   return p;
 }
 
+// cuStreamWaitValue32 through the runtime's driver entry point (no link
+// against the driver library); null where the driver does not offer it.
+typedef int (*WaitValue32Fn)(cudaStream_t, void*, unsigned int, unsigned int);
+static WaitValue32Fn wait_value32() {
+  static WaitValue32Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuStreamWaitValue32", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return (WaitValue32Fn)p;
+  }();
+  return fn;
+}
+
+extern "C" int chb_io_overlap_available() { return wait_value32() != nullptr; }
+
+static int ensure_io_streams(chb_plan* plan) {
+  if (plan->io_in) return 0;
+  CUDA_TRY(cudaStreamCreateWithFlags(&plan->io_in, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&plan->ev_start, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventCreateWithFlags(&plan->ev_in, cudaEventDisableTiming));
+  for (int q = 0; q < chb_plan::IO_OUT_STREAMS; q++) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&plan->io_out[q], cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&plan->ev_out[q], cudaEventDisableTiming));
+  }
+  CUDA_TRY(cudaMallocHost(&plan->h_one, sizeof(int)));
+  *plan->h_one = 1;
+  return 0;
+}
+
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
-                cudaStream_t stream, int64_t run_ldb, double run_alpha) {
+                cudaStream_t stream, int64_t run_ldb, double run_alpha, const HostIo* io) {
+  const bool io_in = prog->io.in, io_out = prog->io.out;
+  if ((io_in || io_out) != (io != nullptr) || (io && (io_in != (io->host_in != nullptr) ||
+                                                     io_out != (io->host_out != nullptr))))
+    return set_error(-6, "streamed program and host buffers do not match");
   WsLayout L = ws_layout(*prog);
   if (work_bytes < L.total || (L.total > 0 && !work))
     return set_error(-4, "workspace too small: %zu bytes given, %zu needed", work_bytes, L.total);
@@ -164,8 +249,61 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
     CUDA_TRY(cudaMemcpyAsync(ra.summ, prog->d_summ0, prog->summ0.size() * sizeof(unsigned long long),
                              cudaMemcpyDeviceToDevice, stream));
   }
+  const int nin = (int)prog->io.in_off.size() - 1, nout = (int)prog->io.out_off.size() - 1;
+  if (io_in) {
+    ra.io_in = ra.ctl + 8;
+    ra.nio_in = nin;
+  }
+  if (io_out) {
+    ra.io_out = ra.ctl + 32;
+    ra.nio_out = nout;
+  }
+  double* x = bases[B_X];
+  if (io) {
+    const int rs = ensure_io_streams(plan);
+    if (rs) return rs;
+    CUDA_TRY(cudaEventRecord(plan->ev_start, stream));
+  }
   int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
   CUDA_TRY(engine_launch(ra, grid, stream));
+  if (!io) return 0;
+  if (io_in) {
+    // chunk j, then its arrival flag (copies on one stream run in order), in
+    // the order the task graph needs them
+    const std::vector<int64_t>& off = prog->io.in_off;
+    CUDA_TRY(cudaStreamWaitEvent(plan->io_in, plan->ev_start, 0));
+    for (int j : prog->io.in_order) {
+      CUDA_TRY(cudaMemcpyAsync(x + off[j], io->host_in + off[j], (off[j + 1] - off[j]) * sizeof(double),
+                               cudaMemcpyHostToDevice, plan->io_in));
+      CUDA_TRY(cudaMemcpyAsync(ra.io_in + j, plan->h_one, sizeof(int), cudaMemcpyHostToDevice, plan->io_in));
+    }
+    CUDA_TRY(cudaEventRecord(plan->ev_in, plan->io_in));
+    CUDA_TRY(cudaStreamWaitEvent(stream, plan->ev_in, 0));
+  }
+  if (io_out) {
+    const std::vector<int64_t>& off = prog->io.out_off;
+    WaitValue32Fn wv = wait_value32();
+    if (wv) {
+      // each chunk as soon as its flag is up, dealt over the output streams
+      // in the order the list finishes them
+      const int nq = std::min<int>(chb_plan::IO_OUT_STREAMS, nout);
+      for (int q = 0; q < nq; q++) CUDA_TRY(cudaStreamWaitEvent(plan->io_out[q], plan->ev_start, 0));
+      for (size_t i = 0; i < prog->out_order.size(); i++) {
+        const int j = prog->out_order[i];
+        cudaStream_t sq = plan->io_out[i % nq];
+        if (wv(sq, ra.io_out + j, 1u, 0u /* GEQ */) != 0) return set_error(-7, "cuStreamWaitValue32 failed");
+        CUDA_TRY(cudaMemcpyAsync(io->host_out + off[j], x + off[j], (off[j + 1] - off[j]) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, sq));
+      }
+      for (int q = 0; q < nq; q++) {
+        CUDA_TRY(cudaEventRecord(plan->ev_out[q], plan->io_out[q]));
+        CUDA_TRY(cudaStreamWaitEvent(stream, plan->ev_out[q], 0));
+      }
+    } else {
+      // no stream waits on this driver: copy after the sweep
+      CUDA_TRY(cudaMemcpyAsync(io->host_out, x, off[nout] * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+  }
   return 0;
 }
 
@@ -342,6 +480,14 @@ extern "C" int chb_plan_destroy(chb_plan* plan) {
   if (!plan) return 0;
   if (plan->device >= 0) cudaSetDevice(plan->device);
   plan->progs.clear();
+  if (plan->io_in) cudaStreamDestroy(plan->io_in);
+  if (plan->ev_start) cudaEventDestroy(plan->ev_start);
+  if (plan->ev_in) cudaEventDestroy(plan->ev_in);
+  for (int q = 0; q < chb_plan::IO_OUT_STREAMS; q++) {
+    if (plan->io_out[q]) cudaStreamDestroy(plan->io_out[q]);
+    if (plan->ev_out[q]) cudaEventDestroy(plan->ev_out[q]);
+  }
+  if (plan->h_one) cudaFreeHost(plan->h_one);
   if (plan->d_fronts) cudaFree(plan->d_fronts);
   if (plan->d_relidx) cudaFree(plan->d_relidx);
   if (plan->d_chidx) cudaFree(plan->d_chidx);
@@ -416,6 +562,23 @@ extern "C" int chb_program_schedule(chb_plan* plan, int op, int64_t k, int flags
   cp(ctarget, p->ctarget);
   cp(ready0, p->ready0);
   cp(summ0, p->summ0);
+  return 0;
+}
+
+extern "C" int chb_program_io(chb_plan* plan, int op, int64_t k, int flags, int64_t* counts, int64_t* in_off,
+                              int32_t* in_order, int64_t* out_off, int32_t* out_order) {
+  clear_error();
+  if (!plan || !counts) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  const int64_t nin = p->io.in ? (int64_t)p->io.in_off.size() - 1 : 0;
+  const int64_t nout = p->io.out ? (int64_t)p->io.out_off.size() - 1 : 0;
+  counts[0] = nin;
+  counts[1] = nout;
+  if (in_off && nin) std::memcpy(in_off, p->io.in_off.data(), (nin + 1) * sizeof(int64_t));
+  if (in_order && nin) std::memcpy(in_order, p->io.in_order.data(), nin * sizeof(int));
+  if (out_off && nout) std::memcpy(out_off, p->io.out_off.data(), (nout + 1) * sizeof(int64_t));
+  if (out_order && !p->out_order.empty()) std::memcpy(out_order, p->out_order.data(), p->out_order.size() * sizeof(int));
   return 0;
 }
 

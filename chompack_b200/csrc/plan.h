@@ -14,6 +14,22 @@ struct chb_plan;
 
 namespace chb {
 
+// Streaming of the values between host and device while a sweep runs.
+// With `in`, the values are copied in chunks of whole supernodes, and every
+// task that touches incoming chunk j waits for a T_ARRIVAL task that waits
+// for the flag the copy stream raises after the chunk's copy.  With `out`, a
+// T_SIGNAL task per outgoing chunk raises a host-visible flag once every
+// task whose writes overlap the chunk has finished; outgoing chunks may cut
+// a large supernode between tile columns, so that its leading columns go
+// out while the rest is still being computed.
+struct IoSpec {
+  bool in = false, out = false;
+  std::vector<int64_t> in_off;    // value offsets of the incoming chunks (chunks + 1): whole supernodes
+  std::vector<double> arrive_us;  // estimated arrival of each incoming chunk (list order only)
+  std::vector<int64_t> out_off;   // outgoing chunks: large supernodes split at 64-column boundaries
+  std::vector<int> in_order;      // order of the incoming copies (set by DagBuilder::finish)
+};
+
 struct Program {
   std::vector<Task> tasks;
   std::vector<int2> waits;
@@ -21,6 +37,8 @@ struct Program {
   int64_t ws_doubles = 0;  // doubles of workspace (update matrices + scratch)
   int smem_doubles = ENGINE_SMEM_BASE_DOUBLES;  // dynamic shared memory per CTA
   bool static_default = false;  // list order unless the plan asks otherwise
+  IoSpec io;                    // streaming of the values (set before building)
+  std::vector<int> out_order;   // chunks in the list order of their signals
   Task* d_tasks = nullptr;
   int2* d_waits = nullptr;
   // dynamic scheduling data (filled by DagBuilder::finish)
@@ -83,6 +101,13 @@ struct chb_plan {
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;
+  // streaming of the values to and from host memory (created on first use);
+  // outgoing chunks go round-robin over several streams, so that a chunk
+  // that finishes later than predicted holds up only its own stream
+  static constexpr int IO_OUT_STREAMS = 4;
+  cudaStream_t io_in = nullptr, io_out[IO_OUT_STREAMS] = {};
+  cudaEvent_t ev_start = nullptr, ev_in = nullptr, ev_out[IO_OUT_STREAMS] = {};
+  int* h_one = nullptr;  // pinned 1, copied into an arrival counter after its chunk
 };
 
 namespace chb {
@@ -92,9 +117,22 @@ Program* get_program(chb_plan* plan, int op, int64_t k, int flags);
 // Host side only (no device upload).
 Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags);
 
+// Host buffers of a streamed run (see IoSpec): host_in is copied into the
+// values (bases[B_X]) chunk by chunk while the sweep runs, and each chunk
+// of the result is copied to host_out as soon as it is final.
+struct HostIo {
+  const double* host_in = nullptr;
+  double* host_out = nullptr;
+};
+
+// Program flags selecting the streamed variants (bits above the sweeps' own
+// flags).
+constexpr int PF_IO_IN = 1 << 16;
+constexpr int PF_IO_OUT = 1 << 17;
+
 // Launch a program.  bases: MAX_BASES device pointers (unused slots null).
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
-                cudaStream_t stream, int64_t run_ldb = 0, double run_alpha = 1.0);
+                cudaStream_t stream, int64_t run_ldb = 0, double run_alpha = 1.0, const HostIo* io = nullptr);
 
 // Device entry points implemented in engine.cu.
 size_t engine_smem_bytes();

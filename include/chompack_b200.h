@@ -96,6 +96,37 @@ enum chb_op {
  * be 256-byte aligned. */
 int chb_workspace_size(const chb_plan* plan, int op, int64_t k, int flags, size_t* bytes);
 
+/* Sweeps on values held in host memory.  The reference's cspmatrix keeps
+ * its values on the host (cbase.c:176-284 reads and writes blkval in
+ * place); these entry points keep that calling pattern without serialising
+ * the copies.  The values are cut into at most 24 chunks at supernode
+ * boundaries.  With host_in, chunk j is copied into dev_blkval while the
+ * sweep runs and every task that touches it waits for its arrival; with
+ * host_out, chunk j is copied back as soon as every task that writes it
+ * has finished (outgoing chunks also cut large supernodes between 64-column
+ * tiles).  Either may be NULL (values already on the device / result
+ * left on the device); host buffers should be pinned for the copies to
+ * overlap.  The workspace is the one chb_workspace_size gives for `flags`
+ * = chb_io_flags(host_in != NULL, host_out != NULL).  The call returns when
+ * everything is enqueued on `stream`; the stream's completion includes the
+ * copies. */
+int chb_io_flags(int host_in, int host_out);
+/* 1 when the driver offers stream waits on device flags (the results then
+ * stream out while the sweep runs), 0 when they are copied after it. */
+int chb_io_overlap_available(void);
+int chb_cholesky_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval, void* work,
+                    size_t work_bytes, void* stream);
+int chb_projected_inverse_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval,
+                             void* work, size_t work_bytes, void* stream);
+int chb_llt_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval, void* work,
+               size_t work_bytes, void* stream);
+/* Introspection of a streamed program: counts[0..1] = incoming and
+ * outgoing chunks; the incoming chunks' value offsets (count + 1) and copy
+ * order; the outgoing chunks' value offsets (count + 1) and the order in
+ * which their signals are listed.  Array arguments may be NULL. */
+int chb_program_io(chb_plan* plan, int op, int64_t k, int flags, int64_t* counts, int64_t* in_off,
+                   int32_t* in_order, int64_t* out_off, int32_t* out_order);
+
 /* Introspection of a compiled sweep (works on a host-only plan, device < 0):
  * info[0..7] = tasks, waits, counters, workspace doubles, workspace bytes,
  * byte offset of the doubles, doubles of update matrices, sizeof(task).

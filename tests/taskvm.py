@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_QL, T_VEC, T_NOP, T_LA, T_SUM = 8, 9, 10, 11, 12
+T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL = 8, 9, 10, 11, 12, 13, 14
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -175,7 +175,7 @@ class VM(object):
             self._vec(t)
         elif op == T_QL:
             self._ql(t)
-        elif op == T_NOP:
+        elif op in (T_NOP, T_SIGNAL, T_ARRIVAL):
             pass
         elif op == T_SUM:  # C = alpha * sum_q P_q + beta * C (in order)
             m, n, p, stride = int(t["m"]), int(t["n"]), int(t["aux"][0]), int(t["aux"][1])
