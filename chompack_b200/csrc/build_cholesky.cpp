@@ -15,6 +15,8 @@
 // blk21 = S_k * M with M = L11^{-1} assembled block-row by block-row
 // (M(c, j) = -M_cc * sum_{l=j}^{c-1} L(c, l) M(l, j)), so no tile of it has a
 // sequential dependency on its neighbours.
+#include <cstdlib>
+
 #include "dag.h"
 
 namespace chb {
@@ -57,6 +59,14 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   };
   std::vector<int> last_top, last_bot, trsmb, last_mrow;
   std::vector<Dep> trsm_top, trsm_prev;
+  // Fused diagonal tasks wait mid task; under the dynamic schedule at most
+  // one per front can wait at a time, so fuse only while such fronts
+  // cannot hold half of the CTAs.
+  int64_t multi_block_fronts = 0;
+  for (int64_t k = 0; k < N; k++)
+    if (P.fronts[k].nn > T) multi_block_fronts++;
+  const int grid = P.grid > 0 ? P.grid : 296;
+  const bool fuse_la = 2 * multi_block_fronts < grid && std::getenv("CHB_NO_FUSED_LA") == nullptr;
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int nn = f.nn, na = f.na, nj = f.nj;
@@ -105,10 +115,19 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     trsmb.assign(std::max(NBb, 1), -1);
     last_mrow.assign(NBc, -1);
     int pot = -1;
+    int diag_end = -1;  // end group of the previous fused diagonal task
     for (int c = 0; c < NBc; c++) {
       const int bc = bw(c);
       const int cT = c * T;
-      // POTRF of the diagonal tile (+ M_cc when anything lies below it)
+      // POTRF of the diagonal tile (+ M_cc when anything lies below it).
+      // With fusion, the same task then publishes its counter (M_cc is
+      // stored: the solves below may start), waits (mid task) for the
+      // updates of tiles (c+1, c) and (c+1, c+1) from column c-1, computes
+      // L(c+1, c) = A(c+1, c) M_cc^T from M_cc in shared memory, raises an
+      // early signal, and applies A(c+1, c+1) -= L L^T; its end group
+      // releases POTRF(c+1), so consecutive diagonal tiles are consecutive
+      // tasks.
+      const bool fuse = fuse_la && c + 1 < NBc;
       {
         Task t = make_task(T_POTRF);
         t.m = t.n = bc;
@@ -117,17 +136,33 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         t.aux[0] = cT;
         t.aux[1] = inv ? 1 : 0;
         if (inv) t.c = opnd(B_WS, M + (int64_t)cT * nn + cT, nn);
-        pot = B.add(t, {lv, c, 0, (int)k, 0, 0});
+        if (fuse) t.k = bw(c + 1);
+        const int gend = fuse ? B.new_group() : -1;
+        pot = B.add(t, {lv, c, 0, (int)k, 0, 0}, gend);
         if (c == 0) B.wait_group(pot, asm_group);
+        else if (diag_end >= 0) B.wait_group(pot, diag_end);
         else B.wait_task(pot, last_top[(size_t)c * NBc + c]);
+        diag_end = gend;
       }
       const Operand Mcc = opnd(B_WS, M + (int64_t)cT * nn + cT, nn, OM_TRI_N, 0);
-      // TRSM of the top tiles below the diagonal: P(r,c) := P(r,c) * M_cc^T.
-      // The next diagonal block's tile goes through the look-ahead task,
-      // which also applies that tile's rank-64 update of the next diagonal
-      // tile, so the chain POTRF(c) -> POTRF(c+1) has one task between.
       for (int r = 0; r < NBc; r++) trsm_prev[r] = trsm_top[r];
-      if (c + 1 < NBc) {
+      if (fuse) {
+        const int r = c + 1;
+        B.split_task(pot, 9.0);
+        if (c > 0) {
+          B.wait_mid(pot, last_top[(size_t)r * NBc + c]);
+          B.wait_mid(pot, last_top[(size_t)r * NBc + r]);
+        }
+        trsm_top[r].id = B.early_signal(pot, B.cost[pot] + 5.0);
+        trsm_top[r].group = true;
+        last_top[(size_t)r * NBc + r] = pot;
+      }
+      // TRSM of the top tiles below the diagonal: P(r,c) := P(r,c) * M_cc^T.
+      // Without fusion, the next diagonal block's tile goes through the
+      // look-ahead task, which also applies that tile's rank-64 update of
+      // the next diagonal tile, so the chain POTRF(c) -> POTRF(c+1) has one
+      // task between.
+      if (!fuse && c + 1 < NBc) {
         const int r = c + 1, rT = r * T;
         Task t = make_task(T_LA);
         t.m = bw(r);

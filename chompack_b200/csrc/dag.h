@@ -46,7 +46,15 @@ struct DagBuilder {
   std::vector<std::vector<Wait>> waits;
   std::vector<int32_t> group_of;   // provisional group of each task (-1)
   std::vector<int32_t> group_size;
-  std::vector<double> cost;        // estimated duration (microseconds)
+  std::vector<double> cost;        // estimated duration (microseconds); of the first part for split tasks
+  // Split tasks: a task with post_cost > 0 runs its first part (cost),
+  // publishes its own counter (the waiters on the task need only the first
+  // part), waits for its mid waits and runs its second part (post_cost),
+  // whose end is published through the task's group.  On the device the
+  // waits after the first Task::cdiag ones are checked between the parts;
+  // the dynamic schedule releases the task on the first ones only.
+  std::vector<std::vector<int>> mid_waits;
+  std::vector<double> post_cost;
   // Early signals: a task may publish a one-member group part-way through
   // (the counter index goes to its aux[3] as index + 1), so that waiters on
   // its first result do not wait for all of it.
@@ -65,6 +73,8 @@ struct DagBuilder {
     keys.push_back(key);
     cost.push_back(est_us >= 0 ? est_us : estimate(t));
     waits.emplace_back();
+    mid_waits.emplace_back();
+    post_cost.push_back(0.0);
     group_of.push_back(group);
     early_of.push_back(-1);
     early_at.push_back(0.0);
@@ -86,6 +96,12 @@ struct DagBuilder {
   void wait_task(int task, int dep) {
     if (dep >= 0) waits[task].push_back({dep, 1, false});
   }
+  // A wait checked between the two parts of a split task (post_us: the
+  // estimated duration of its second part).
+  void wait_mid(int task, int dep) {
+    if (dep >= 0) mid_waits[task].push_back(dep);
+  }
+  void split_task(int task, double post_us) { post_cost[task] = post_us; }
   // Wait for all members of a group (the group must be complete when the
   // program is finished).
   void wait_group(int task, int group) {
@@ -239,15 +255,18 @@ struct DagBuilder {
       std::fill(rank.begin(), rank.end(), 0.0);
       // creation order is topological (every wait names an earlier task)
       for (int t = nt - 1; t >= 0; t--) {
-        rank[t] += cost[t] + extra[t];
+        rank[t] += cost[t] + post_cost[t] + extra[t];
+        for (int d : mid_waits[t])
+          if (d < t) rank[d] = std::max(rank[d], rank[t] - cost[t]);
         for (const Wait& wt : waits[t]) {
           if (wt.is_group) {
             const int o = early_owner[wt.id];
-            if (o >= 0 && o < t) rank[o] = std::max(rank[o], rank[t] + early_at[o] - cost[o]);
+            if (o >= 0 && o < t) rank[o] = std::max(rank[o], rank[t] + early_at[o] - cost[o] - post_cost[o]);
             for (int u : members[wt.id])
               if (u < t) rank[u] = std::max(rank[u], rank[t]);
           } else if (wt.id < t) {
-            rank[wt.id] = std::max(rank[wt.id], rank[t]);
+            // a split task's own waiters follow its first part only
+            rank[wt.id] = std::max(rank[wt.id], rank[t] - post_cost[wt.id]);
           }
         }
       }
@@ -266,8 +285,16 @@ struct DagBuilder {
         unmet0[t]++;
       }
     }
+    std::vector<std::vector<int>> mid_waiters(nt);
+    std::vector<int> mid_unmet0(nt, 0);
+    for (int t = 0; t < nt; t++)
+      for (int d : mid_waits[t]) {
+        mid_waiters[d].push_back(t);
+        mid_unmet0[t]++;
+      }
     auto simulate = [&]() -> int {
-      std::vector<int> unmet = unmet0;
+      std::vector<int> unmet = unmet0, mid_unmet = mid_unmet0;
+      std::vector<char> first_done(nt, 0);
       std::vector<int> group_left(group_size.begin(), group_size.end());
       {
         auto by_rank = [&](int a, int b) { return rank[a] < rank[b] || (rank[a] == rank[b] && b < a); };
@@ -282,19 +309,36 @@ struct DagBuilder {
         auto release = [&](int w) {
           if (--unmet[w] == 0) ready.push(w);
         };
+        // second part of a split task: its end, and its early signal (its
+        // estimate counts from the task's start as if it never waited)
+        auto second_part = [&](int t) {
+          running.push({now + std::max(post_cost[t], 1e-3), t});
+          if (early_of[t] >= 0) running.push({now + std::max(early_at[t] - cost[t], 0.0), -1 - early_of[t]});
+        };
         while (done < nt) {
           while (free_slots > 0 && !ready.empty()) {
             int t = ready.top();
             ready.pop();
             start[t] = now;
-            running.push({now + std::max(cost[t], 1e-3), t});
-            if (early_of[t] >= 0) running.push({now + std::min(early_at[t], cost[t]), -1 - early_of[t]});
+            if (post_cost[t] > 0.0) {
+              running.push({now + std::max(cost[t], 1e-3), -1 - ng - t});
+            } else {
+              running.push({now + std::max(cost[t], 1e-3), t});
+              if (early_of[t] >= 0) running.push({now + std::min(early_at[t], cost[t]), -1 - early_of[t]});
+            }
             free_slots--;
           }
           if (running.empty()) return set_error(-23, "task graph: unsatisfiable waits");
           Ev e = running.top();
           running.pop();
           now = e.first;
+          if (e.second < -ng) {  // first part of a split task done: its own waiters go
+            const int t = -1 - ng - e.second;
+            first_done[t] = 1;
+            for (int w : task_waiters[t]) release(w);
+            if (mid_unmet[t] == 0) second_part(t);
+            continue;
+          }
           if (e.second < 0) {  // an early signal: release its waiters, no slot freed
             for (int w : group_waiters[-1 - e.second]) release(w);
             continue;
@@ -302,7 +346,10 @@ struct DagBuilder {
           free_slots++;
           done++;
           const int t = e.second;
-          for (int w : task_waiters[t]) release(w);
+          if (post_cost[t] <= 0.0)
+            for (int w : task_waiters[t]) release(w);
+          for (int w : mid_waiters[t])
+            if (--mid_unmet[w] == 0 && first_done[w]) second_part(w);
           if (group_of[t] >= 0 && --group_left[group_of[t]] == 0)
             for (int w : group_waiters[group_of[t]]) release(w);
         }
@@ -401,6 +448,22 @@ struct DagBuilder {
           if (x.x == e.x) { dup = true; break; }
         if (!dup) w.push_back(e);
       }
+      if (!mid_waits[t].empty() || post_cost[t] > 0.0) {
+        // Mid waits may point forwards in the list: every task that needs
+        // this one starts (in the simulated schedule that gives the list
+        // order) after its second part, hence after each mid wait, so the
+        // list order stays deadlock-free for tasks claimed in order.
+        tk.cdiag = (int32_t)w.size();
+        for (int d : mid_waits[t]) {
+          int2 e;
+          e.x = pos[d];
+          e.y = 1;
+          bool dup = false;
+          for (const int2& x : w)
+            if (x.x == e.x) { dup = true; break; }
+          if (!dup) w.push_back(e);
+        }
+      }
       if (w.size() > 65535) return set_error(-22, "task graph: too many waits");
       tk.nwait = (uint16_t)w.size();
       tk.group = group_of[t] >= 0 ? nt + group_of[t] : -1;
@@ -423,10 +486,11 @@ struct DagBuilder {
     prog.succ_off.assign(nc + 1, 0);
     prog.ctarget.assign(nc, 1);
     for (size_t g = 0; g < group_size.size(); g++) prog.ctarget[nt + g] = std::max(group_size[g], 1);
+    auto npre = [](const Task& tk) { return (tk.op == T_POTRF && tk.k > 0) ? (int)tk.cdiag : (int)tk.nwait; };
     for (int i = 0; i < nt; i++) {
       const Task& tk = prog.tasks[i];
-      prog.npend[i] = tk.nwait;
-      for (int w = 0; w < tk.nwait; w++) prog.succ_off[prog.waits[tk.wait_off + w].x + 1]++;
+      prog.npend[i] = npre(tk);
+      for (int w = 0; w < npre(tk); w++) prog.succ_off[prog.waits[tk.wait_off + w].x + 1]++;
     }
     for (int64_t c = 0; c < nc; c++) prog.succ_off[c + 1] += prog.succ_off[c];
     prog.succ.assign(prog.succ_off[nc], 0);
@@ -434,7 +498,7 @@ struct DagBuilder {
       std::vector<int> fill(prog.succ_off.begin(), prog.succ_off.end() - 1);
       for (int i = 0; i < nt; i++) {
         const Task& tk = prog.tasks[i];
-        for (int w = 0; w < tk.nwait; w++) prog.succ[fill[prog.waits[tk.wait_off + w].x]++] = i;
+        for (int w = 0; w < npre(tk); w++) prog.succ[fill[prog.waits[tk.wait_off + w].x]++] = i;
       }
     }
     const int nwords = (nt + 63) / 64, nsumm = (nwords + 63) / 64;

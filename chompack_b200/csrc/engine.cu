@@ -267,19 +267,22 @@ __device__ __forceinline__ int claim_task(const RunArgs& ra, int* lo) {
 }
 
 // After task ti (warp 0, the CTA's writes ordered before by __syncthreads):
-// releases the waiters of the task (the first 32 prefetched into pre) and,
+// releases the waiters of the task (the first 32 prefetched into pre;
+// already done mid task by a split task: own_released) and,
 // when the task completes its group, of the group; counts the task into its
 // bitmap word's finished tasks and the finished count.  Returns the released
 // waiter this CTA runs next, or -1 (also when a device error is set).
-__device__ __forceinline__ int finish_task(const RunArgs& ra, int ti, int group, int sb, int se, const int* pre) {
+__device__ __forceinline__ int finish_task(const RunArgs& ra, int ti, int group, int sb, int se, const int* pre,
+                                           bool own_released) {
   const int lane = threadIdx.x & 31;
   int next = 0x7fffffff;
   int gdone = 0, filled = 0, err = 0;
   if (lane == 0 && group >= 0) gdone = atom_add_acq_rel(ra.counters + group, 1) + 1 == __ldg(ra.ctarget + group);
   if (lane == 1) filled = atomicAdd(ra.wclaimed + (ti >> 6), 1) + 1 == min(64, ra.ntasks - (ti & ~63));
   if (lane == 2) err = ld_volatile(&ra.ctl[1]);
+  if (lane == 3) red_release_add(ra.counters + ti, 1);  // for the mid waits of split tasks
   cp_async_wait_all();
-  release_list(ra, sb, se, pre, true, &next);
+  if (!own_released) release_list(ra, sb, se, pre, true, &next);
   if (__shfl_sync(0xffffffffu, gdone, 0))
     release_list(ra, __ldg(ra.succ_off + group), __ldg(ra.succ_off + group + 1), nullptr, true, &next);
   if (lane == 1 && filled) advance_frontier(ra);
@@ -428,16 +431,18 @@ __device__ __forceinline__ void acc_coord(int i, int j, int h, int& r, int& c) {
   c = (warp & 1) * 32 + 8 * j + 2 * q + (h & 1);
 }
 
-// acc += A(:, 0:kn) * B(:, 0:kn)^T from staged tiles (kn multiple of 4).
-__device__ __forceinline__ void mma_block(const double* sA, const double* sB, int kn, Acc& acc) {
+// acc += A(:, 0:kn) * B(:, 0:kn)^T from tiles in shared memory, A(r, k) at
+// sA[k*LA + r] and B(c, k) at sB[k*LB + c] (kn multiple of 4).
+template <int LA, int LB>
+__device__ __forceinline__ void mma_block_ld(const double* sA, const double* sB, int kn, Acc& acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int r0 = (warp >> 1) * 32 + g, c0 = (warp & 1) * 32 + g;
 #pragma unroll 4
   for (int kk = 0; kk < kn; kk += 4) {
     double a[2][2], b[4];
-    const double* ak = sA + (kk + q) * LDS + r0;
-    const double* bk = sB + (kk + q) * LDS + c0;
+    const double* ak = sA + (kk + q) * LA + r0;
+    const double* bk = sB + (kk + q) * LB + c0;
 #pragma unroll
     for (int i = 0; i < 2; i++) {
       a[i][0] = ak[16 * i];
@@ -450,6 +455,11 @@ __device__ __forceinline__ void mma_block(const double* sA, const double* sB, in
 #pragma unroll
       for (int j = 0; j < 4; j++) dmma16(acc[i][j], a[i][0], a[i][1], b[j]);
   }
+}
+
+// The GEMM stages (leading dimension LDS).
+__device__ __forceinline__ void mma_block(const double* sA, const double* sB, int kn, Acc& acc) {
+  mma_block_ld<LDS, LDS>(sA, sB, kn, acc);
 }
 
 __device__ __forceinline__ void zero_acc(Acc& acc) {
@@ -708,7 +718,98 @@ __device__ __forceinline__ void warp_mma_16x8(double (&acc)[4], const double* pa
   }
 }
 
-__device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
+// Look-ahead part of a fused diagonal task (T_POTRF with k = m2 > 0, run
+// after the factorisation of the b = 64 tile; sL holds L_cc and sM holds
+// M = L_cc^{-1}, both with leading dimension POTRF_LD):
+//   1. wait for the task's mid waits (waits [cdiag, nwait): the updates of
+//      tiles (c+1, c) and (c+1, c+1) from the previous column block);
+//   2. L' = A(c+1, c) M^T  (m2 x b; A staged into sL), stored in place and
+//      kept in sL;
+//   3. early signal aux[3] - 1 (the readers of L');
+//   4. A(c+1, c+1) -= L' L'^T (lower part, m2 x m2).
+// The tiles lie at a.off + b (panel) and a.off + b*lda + b (diagonal).
+__device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t, double* smem) {
+  __shared__ int s_la_abort;
+  constexpr int LD = POTRF_LD;
+  double* sL = smem;
+  const double* sM = smem + TILE * LD;
+  const int b = t.m, m2 = t.k, lda = t.a.ld;
+  double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ P = X + b;
+  double* __restrict__ D = X + (int64_t)b * lda + b;
+  const int tid = threadIdx.x;
+  __syncthreads();
+  if (tid == 0) {
+    int abort = 0;
+    for (int w = t.cdiag; w < t.nwait && !abort; w++) {
+      const int2 wt = ra.waits[t.wait_off + w];
+      int64_t spins = 0;
+      unsigned ns = 16;
+      while (ld_acquire(ra.counters + wt.x) < wt.y) {
+        if (++spins > ra.spin_limit) {
+          atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+          atomicAdd(&ra.ctl[3], 1);
+          abort = 1;
+          break;
+        }
+        if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
+        __nanosleep(ns);
+        if (ns < 128) ns <<= 1;
+      }
+    }
+    s_la_abort = abort;
+  }
+  __syncthreads();
+  if (s_la_abort) return;
+  // A(c+1, c) into sL (rows >= m2 zero)
+  {
+    double v[TILE * TILE / NTHREADS];
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = tid + s2 * NTHREADS;
+      const int r = idx % TILE, c = idx / TILE;
+      v[s2] = (r < m2 && c < b) ? __ldcg(P + (int64_t)c * lda + r) : 0.0;
+    }
+#pragma unroll
+    for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
+      const int idx = tid + s2 * NTHREADS;
+      sL[(idx / TILE) * LD + idx % TILE] = v[s2];
+    }
+  }
+  __syncthreads();
+  Acc acc;
+  zero_acc(acc);
+  mma_block_ld<LD, LD>(sL, sM, b, acc);
+  __syncthreads();
+  // L' into sL and in place
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        int r, c;
+        acc_coord(i, j, h, r, c);
+        const double v = (r < m2) ? acc[i][j][h] : 0.0;
+        sL[c * LD + r] = v;
+        if (r < m2 && c < b) P[(int64_t)c * lda + r] = v;
+      }
+  __syncthreads();
+  if (t.aux[3] > 0) {
+    if (ra.dynamic) {
+      const int c = t.aux[3] - 1;
+      if (tid < 32) release_list(ra, __ldg(ra.succ_off + c), __ldg(ra.succ_off + c + 1), nullptr, false, nullptr);
+    } else if (tid == 0) {
+      __threadfence();
+      red_release_add(ra.counters + (t.aux[3] - 1), 1);
+    }
+  }
+  zero_acc(acc);
+  mma_block_ld<LD, LD>(sL, sL, b, acc);
+  store_acc(D, lda, m2, m2, true, 0, -1.0, 1.0, acc);
+}
+
+__device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti) {
   const int b = t.m;
   const int LD = POTRF_LD;
   double* sL = smem;               // [col][row], lower; upper part zero
@@ -918,6 +1019,17 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem) {
     if (r < b && cc < b) Mout[(int64_t)cc * ldm + r] = sM[cc * LD + r];
   }
   POTRF_STAMP(7);
+  if (t.k > 0) {
+    // first part done: L_cc and M_cc are stored; the task's own waiters go
+    __syncthreads();
+    if (ra.dynamic) {
+      if (tid < 32) release_list(ra, __ldg(ra.succ_off + ti), __ldg(ra.succ_off + ti + 1), nullptr, false, nullptr);
+    } else if (tid == 0) {
+      __threadfence();
+      red_release_add(ra.counters + ti, 1);
+    }
+    potrf_lookahead(ra, t, smem);
+  }
 }
 
 // ------------------------------------------------------------ assembly
@@ -1503,7 +1615,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       if (threadIdx.x == 0) {
         if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
         int abort = 0;
-        for (int w = 0; w < s_t.nwait && !abort; w++) {
+        const int npre = (s_t.op == T_POTRF && s_t.k > 0) ? (int)s_t.cdiag : (int)s_t.nwait;
+        for (int w = 0; w < npre && !abort; w++) {
           const int2 wt = ra.waits[s_t.wait_off + w];
           int64_t spins = 0;
           unsigned ns = 16;
@@ -1532,7 +1645,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_GEMM:
       case T_LA: run_gemm_or_la(ra, t, sm); break;
       case T_MROW: run_mrow(ra, t, sm); break;
-      case T_POTRF: run_potrf(ra, t, smem); break;
+      case T_POTRF: run_potrf(ra, t, smem, ti); break;
       case T_ASM: run_asm(ra, t); break;
       case T_EXTRACT: run_extract(ra, t); break;
       case T_COPY: run_copy(ra, t); break;
@@ -1562,7 +1675,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
         if (t.group >= 0) red_release_add(ra.counters + t.group, 1);
       }
     } else if (threadIdx.x < 32) {
-      const int nx = finish_task(ra, ti, t.group, s_succ[0], s_succ[1], s_pre);
+      const int nx = finish_task(ra, ti, t.group, s_succ[0], s_succ[1], s_pre, t.op == T_POTRF && t.k > 0);
       if (threadIdx.x == 0) s_next = nx;
     }
   }

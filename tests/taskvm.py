@@ -79,6 +79,15 @@ class Program(object):
                                          self.waits.ctypes.data, self.fronts.ctypes.data), "program_export")
 
 
+def _early_counter(t):
+    """The early-signal counter of a look-ahead task or a fused diagonal
+    task (aux[3] = counter + 1), or -1."""
+    op = int(t["op"])
+    if op == T_LA or (op == T_POTRF and int(t["k"]) > 0):
+        return int(t["aux"][3]) - 1
+    return -1
+
+
 def _operand(buf, o, rows, K):
     r = np.arange(rows)[:, None]
     k = np.arange(K)[None, :]
@@ -167,6 +176,16 @@ class VM(object):
             if int(t["aux"][1]):
                 M = np.linalg.inv(L)
                 _store(self.bases[int(t["c"]["base"])], t["c"], b, b, np.tril(M), False, 0, 0.0)
+            m2 = int(t["k"])
+            if m2 > 0:   # fused look-ahead: next panel tile and next diagonal tile
+                r2 = np.arange(m2)[:, None]
+                pidx = off + b + c * ld + r2                   # tile (c+1, c): m2 x b
+                L2 = X[pidx] @ np.tril(np.linalg.inv(L)).T
+                X[pidx] = L2
+                c2 = np.arange(m2)[None, :]
+                didx = off + b * ld + b + c2 * ld + r2         # tile (c+1, c+1): m2 x m2
+                low = r2 >= c2
+                X[didx[low]] = (X[didx] - L2 @ L2.T)[low]
         elif op == T_ASM:
             self._asm(t)
         elif op == T_EXTRACT:
@@ -432,7 +451,7 @@ class VM(object):
             ready[j] = ready[-1]
             ready.pop()
             order.append(i)
-            early = int(tasks[i]["aux"][3]) - 1 if int(tasks[i]["op"]) == T_LA else -1
+            early = _early_counter(tasks[i])
             for cid in (i, int(tasks[i]["group"]), early):
                 if cid < 0:
                     continue
@@ -469,13 +488,34 @@ def dynamic_order(prog, sch, seed=0, window=4):
             if pend[s] == 0:
                 out.append(int(s))
 
+    # split tasks (a fused diagonal task) wait for their mid waits too: the
+    # device runs them in two parts, this interpreter in one
+    done = np.zeros(nt, dtype=bool)
+
+    def mid_deps(i):
+        t = tasks[i]
+        if int(t["op"]) != T_POTRF or int(t["k"]) == 0:
+            return []
+        w0, nw, npre = int(t["wait_off"]), int(t["nwait"]), int(t["cdiag"])
+        return [int(c) for c, _ in prog.waits[w0 + npre:w0 + nw]]
+
     order = []
-    while ready:
+    stalled = []
+    while ready or stalled:
+        still = [i for i in stalled if not all(done[d] for d in mid_deps(i))]
+        ready = sorted(ready + [i for i in stalled if i not in still])
+        stalled = still
+        if not ready:
+            raise AssertionError("dynamic schedule: split tasks wait on tasks that never run")
         j = int(rng.integers(min(window, len(ready))))
         i = ready.pop(j)
+        if not all(done[d] for d in mid_deps(i)):
+            stalled.append(i)
+            continue
+        done[i] = True
         order.append(i)
         new = []
-        early = int(tasks[i]["aux"][3]) - 1 if int(tasks[i]["op"]) == T_LA else -1
+        early = _early_counter(tasks[i])
         if early >= 0:
             release(early, new)
         release(i, new)

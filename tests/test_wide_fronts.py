@@ -1,0 +1,74 @@
+"""Task programs of problems whose fronts span several 64-column blocks, on
+the CPU: the fused diagonal task of cholesky (factor the diagonal tile, then
+wait mid task for the next tiles' updates and do the look-ahead) and the
+separate look-ahead task it replaces, executed by the task interpreter in
+random orders allowed by the waits and under the dynamic release rules,
+against the oracle's C restatement of the reference's sweeps."""
+import os
+
+import numpy as np
+import pytest
+
+import chompack_b200 as cp
+from chompack_b200 import _native as N
+from chompack_b200.plan import Plan
+from helpers import problem, assert_blocks_close
+from oracle import oracle
+import taskvm
+
+CASES = [("grid3d", (10,), (32, 32)), ("grid2d", (70,), (64, 64))]
+
+
+def _setup(kind, args, merge, fused):
+    old = os.environ.pop("CHB_NO_FUSED_LA", None)
+    if not fused:
+        os.environ["CHB_NO_FUSED_LA"] = "1"
+    try:
+        A, s = problem(kind, *args, merge=merge, seed=3)
+        pl = Plan(s, device=-1)
+        prog = taskvm.Program(pl.handle, N.OP_CHOLESKY, nsn=s.Nsn)
+        sch = taskvm.Schedule(pl.handle, N.OP_CHOLESKY)
+    finally:
+        os.environ.pop("CHB_NO_FUSED_LA", None)
+        if old is not None:
+            os.environ["CHB_NO_FUSED_LA"] = old
+    return A, s, pl, prog, sch
+
+
+@pytest.mark.parametrize("kind,args,merge", CASES)
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("order,seed", [("random", 0), ("random", 1), ("dynamic", 2)])
+def test_wide_front_cholesky(kind, args, merge, fused, order, seed):
+    A, s, pl, prog, sch = _setup(kind, args, merge, fused)
+    ops = prog.tasks["op"]
+    n_fused = int(np.sum((ops == taskvm.T_POTRF) & (prog.tasks["k"] > 0)))
+    n_la = int(np.sum(ops == taskvm.T_LA))
+    assert int(np.max(np.diff(s.snptr))) > 64
+    assert (n_fused > 0 and n_la == 0) if fused else (n_fused == 0 and n_la > 0)
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    ref = x0.copy()
+    assert oracle.cholesky(s, ref) == 0
+    x = x0.copy()
+    bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, x, ref)
+
+
+def test_fused_task_waits():
+    """The fused task's first Task::cdiag waits gate its start (and its
+    pending count in the dynamic schedule); the rest are mid-task waits on
+    the updates of the next panel and diagonal tiles."""
+    A, s, pl, prog, sch = _setup("grid3d", (10,), (32, 32), True)
+    seen_mid = 0
+    for i, t in enumerate(prog.tasks):
+        if int(t["op"]) != taskvm.T_POTRF or int(t["k"]) == 0:
+            continue
+        npre, nw = int(t["cdiag"]), int(t["nwait"])
+        assert 0 <= npre <= nw
+        assert sch.npend[i] == npre
+        w0 = int(t["wait_off"])
+        for cid, _ in prog.waits[w0 + npre:w0 + nw]:
+            assert cid < prog.ntasks and int(prog.tasks[cid]["op"]) == taskvm.T_GEMM
+            seen_mid += 1
+        assert int(t["aux"][3]) > 0     # the early signal of the next panel tile
+    assert seen_mid > 0
