@@ -366,18 +366,46 @@ __device__ __forceinline__ void stage_coord(int s, int& r, int& kk) {
 }
 
 // Issues the copies of the operand's K chunk [k0, k0 + KC) into a stage:
-// S[kk*LDS + r] = op(r, k0 + kk), zero outside [0,rows) x [0,K).
+// S[kk*LDS + r] = op(r, k0 + kk), zero outside [0,rows) x [0,K).  For the
+// plain and triangular modes a thread's elements lie at fixed strides from
+// one base pointer (the coordinates of stage_coord with the thread count a
+// multiple of TILE and of KC), which saves the per-element address
+// arithmetic.
+static_assert(NTHREADS % TILE == 0 && NTHREADS % KC == 0, "stage coordinates assume whole rows / columns");
 template <int MODE>
 __device__ __forceinline__ void issue_chunk_t(const double* __restrict__ X, int ld, int diag, int koff, int rows,
                                               int k0, int K, double* S) {
+  const int tid = threadIdx.x;
+  if (MODE == OM_N || MODE == OM_TRI_N) {
+    constexpr int KSTEP = NTHREADS / TILE;  // k rows per element step
+    const int r = tid % TILE, kb = tid / TILE;
+    const double* p = X + (int64_t)(k0 + kb) * ld + r;
 #pragma unroll
-  for (int s = 0; s < PER_THREAD; s++) {
-    int r, kk;
-    stage_coord<MODE>(s, r, kk);
-    const int k = k0 + kk;
-    bool ok = r < rows && k < K;
-    const double* src = op_addr<MODE>(X, ld, diag, koff, r, k, ok);
-    cp_async8_zfill(S + kk * LDS + r, ok ? src : X, ok);
+    for (int s = 0; s < PER_THREAD; s++) {
+      const int kk = kb + KSTEP * s, k = k0 + kk;
+      const bool ok = r < rows && k < K && (MODE == OM_N || r + diag >= k);
+      cp_async8_zfill(S + kk * LDS + r, ok ? p + (int64_t)(KSTEP * s) * ld : X, ok);
+    }
+  } else if (MODE == OM_T || MODE == OM_TRI_T) {
+    constexpr int RSTEP = NTHREADS / KC;  // rows per element step
+    const int kk = tid % KC, rb = tid / KC, k = k0 + kk;
+    const double* p = X + (int64_t)rb * ld + k;
+#pragma unroll
+    for (int s = 0; s < PER_THREAD; s++) {
+      const int r = rb + RSTEP * s;
+      const bool ok = r < rows && k < K && (MODE == OM_T || k + diag >= r);
+      cp_async8_zfill(S + kk * LDS + r, ok ? p + (int64_t)(RSTEP * s) * ld : X, ok);
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < PER_THREAD; s++) {
+      int r, kk;
+      stage_coord<MODE>(s, r, kk);
+      const int k = k0 + kk;
+      bool ok = r < rows && k < K;
+      const double* src = op_addr<MODE>(X, ld, diag, koff, r, k, ok);
+      cp_async8_zfill(S + kk * LDS + r, ok ? src : X, ok);
+    }
   }
 }
 
