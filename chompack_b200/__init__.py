@@ -23,5 +23,6 @@ __all__ = ["spmatrix", "tril", "triu", "symmetrize", "perm", "eye", "symbolic", 
 from .cbase import cholesky, llt, projected_inverse, completion, hessian, trsm, dot  # noqa: E402,F401
 from . import autograd  # noqa: E402,F401
 from .batch import batch  # noqa: E402,F401
+from . import mixed  # noqa: E402,F401
 
 __all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot", "autograd", "batch"]

@@ -87,6 +87,12 @@ set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 plan_set_schedule = _sig("chb_plan_set_schedule", ctypes.c_int, [PPLAN, ctypes.c_int])
 io_flags = _sig("chb_io_flags", ctypes.c_int, [ctypes.c_int, ctypes.c_int])
 io_overlap_available = _sig("chb_io_overlap_available", ctypes.c_int, [])
+precision_flags = _sig("chb_precision_flags", ctypes.c_int, [ctypes.c_int])
+cholesky_prec = _sig("chb_cholesky_prec", ctypes.c_int, [PPLAN, ctypes.c_int, vp, vp, vp, vp, ctypes.c_size_t, vp])
+projected_inverse_prec = _sig("chb_projected_inverse_prec", ctypes.c_int,
+                              [PPLAN, ctypes.c_int, vp, vp, vp, vp, ctypes.c_size_t, vp])
+symv = _sig("chb_symv", ctypes.c_int, [PPLAN, vp, vp, vp, vp, vp, i64, i64, ctypes.c_double, vp])
+PREC = {"fp64": 0, "tf32": 1, "tf32x3": 2}
 cholesky_io = _sig("chb_cholesky_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 projected_inverse_io = _sig("chb_projected_inverse_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 llt_io = _sig("chb_llt_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])

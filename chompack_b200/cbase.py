@@ -72,7 +72,13 @@ def _write_back(X):
         _mark_synced(X)
 
 
-def _streamed(X, op, launch, name="X"):
+def _precision(precision):
+    if precision not in N.PREC:
+        raise ValueError("precision must be one of %s" % ", ".join(sorted(N.PREC)))
+    return N.PREC[precision]
+
+
+def _streamed(X, op, launch, name="X", prec=0):
     """A streamed sweep on host values: chunks go in (unless the mirror
     holds them) while the sweep runs, and come back out as they finish."""
     v = X.blkval
@@ -81,7 +87,7 @@ def _streamed(X, op, launch, name="X"):
     plan = X.symb.plan()
     m = _mirror(X, plan)
     host_in = None if _synced(X) else v.data_ptr()
-    flags = N.io_flags(host_in is not None, 1)
+    flags = N.io_flags(host_in is not None, 1) | N.precision_flags(prec)
     dev = torch.device("cuda", plan.device)
     ws, nbytes = plan.workspace(op, 0, flags)
     s = _stream(dev)
@@ -111,35 +117,57 @@ def _run_and_status(plan, op, launch, k=0, flags=0):
     return info
 
 
-def cholesky(X):
+def cholesky(X, precision="fp64"):
     """Supernodal multifrontal Cholesky factorisation X = L L^T, in place
-    (cbase.c:176-284).  On exit X holds the factor and X.is_factor is True."""
+    (cbase.c:176-284).  On exit X holds the factor and X.is_factor is True.
+
+    precision (an addition; the reference is FP64 only): "tf32" or "tf32x3"
+    run the GEMM tiles (Schur updates, panel solves) on TF32 tensor cores
+    with FP32 accumulation, the diagonal tiles in FP64 (see
+    chompack_b200.mixed for refined solves and error reports)."""
     if X.is_factor is not False:
         raise ValueError("X must be a cspmatrix")
+    prec = _precision(precision)
     if _on_host(X):
-        info = _streamed(X, N.OP_CHOLESKY, N.cholesky_io)
+        info = _streamed(X, N.OP_CHOLESKY,
+                         lambda h, hi, ho, d, ws, nb, s: N.cholesky_prec(h, prec, hi, ho, d, ws, nb, s), prec=prec)
     else:
         v = _values(X)
         plan = X.symb.plan(v.device.index)
-        info = _run_and_status(plan, N.OP_CHOLESKY,
-                               lambda ws, nb, s: N.cholesky(plan.handle, v.data_ptr(), ws, nb, s))
+        if prec:
+            info = _run_and_status(plan, N.OP_CHOLESKY,
+                                   lambda ws, nb, s: N.cholesky_prec(plan.handle, prec, None, None, v.data_ptr(),
+                                                                     ws, nb, s), flags=N.precision_flags(prec))
+        else:
+            info = _run_and_status(plan, N.OP_CHOLESKY,
+                                   lambda ws, nb, s: N.cholesky(plan.handle, v.data_ptr(), ws, nb, s))
     X.is_factor = True
     if info:
         raise ArithmeticError("factorization failed")
 
 
-def projected_inverse(L):
+def projected_inverse(L, precision="fp64"):
     """Supernodal multifrontal projected inverse Y = P(L^{-T} L^{-1}), in place
-    (cbase.c:393-500).  On exit L holds Y and L.is_factor is False."""
+    (cbase.c:393-500).  On exit L holds Y and L.is_factor is False.
+    precision: as for cholesky (its GEMM tiles on TF32 tensor cores)."""
     if L.is_factor is not True:
         raise ValueError("X must be a cspmatrix")
+    prec = _precision(precision)
     if _on_host(L):
-        info = _streamed(L, N.OP_PROJECTED_INVERSE, N.projected_inverse_io)
+        info = _streamed(L, N.OP_PROJECTED_INVERSE,
+                         lambda h, hi, ho, d, ws, nb, s: N.projected_inverse_prec(h, prec, hi, ho, d, ws, nb, s),
+                         prec=prec)
     else:
         v = _values(L)
         plan = L.symb.plan(v.device.index)
-        info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
-                               lambda ws, nb, s: N.projected_inverse(plan.handle, v.data_ptr(), ws, nb, s))
+        if prec:
+            info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
+                                   lambda ws, nb, s: N.projected_inverse_prec(plan.handle, prec, None, None,
+                                                                              v.data_ptr(), ws, nb, s),
+                                   flags=N.precision_flags(prec))
+        else:
+            info = _run_and_status(plan, N.OP_PROJECTED_INVERSE,
+                                   lambda ws, nb, s: N.projected_inverse(plan.handle, v.data_ptr(), ws, nb, s))
     L.is_factor = False
     if info:
         raise ArithmeticError("partial inverse failed")

@@ -28,18 +28,23 @@ int run_op(chb_plan* plan, int op, int64_t k, int flags, double* const* bases, i
   return run_program(plan, prog, work, work_bytes, bases, nbases, (cudaStream_t)stream, ldb, alpha);
 }
 
+int precision_flags(int precision) {
+  return precision == CHB_PREC_TF32 ? PF_TF32 : precision == CHB_PREC_TF32X3 ? PF_TF32X3 : 0;
+}
+
 // A sweep on values held in host memory (see chb_cholesky_io).
 int run_io(chb_plan* plan, int op, const double* host_in, double* host_out, double* dev_blkval, void* work,
-           size_t work_bytes, void* stream) {
+           size_t work_bytes, void* stream, int precision = CHB_PREC_FP64) {
   clear_error();
   int rc = check_plan(plan);
   if (rc) return rc;
   if (!dev_blkval) return set_error(-1, "null device values");
-  const int flags = (host_in ? PF_IO_IN : 0) | (host_out ? PF_IO_OUT : 0);
+  if (precision < CHB_PREC_FP64 || precision > CHB_PREC_TF32X3) return set_error(-1, "unknown precision %d", precision);
+  const int flags = (host_in ? PF_IO_IN : 0) | (host_out ? PF_IO_OUT : 0) | precision_flags(precision);
   Program* prog = get_program(plan, op, 0, flags);
   if (!prog) return -2;
   double* bases[1] = {dev_blkval};
-  if (!flags) return run_program(plan, prog, work, work_bytes, bases, 1, (cudaStream_t)stream);
+  if (!host_in && !host_out) return run_program(plan, prog, work, work_bytes, bases, 1, (cudaStream_t)stream);
   HostIo io;
   io.host_in = host_in;
   io.host_out = host_out;
@@ -65,6 +70,18 @@ extern "C" int chb_projected_inverse_io(chb_plan* plan, const double* host_in, d
 extern "C" int chb_llt_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval, void* work,
                           size_t work_bytes, void* stream) {
   return run_io(plan, CHB_OP_LLT, host_in, host_out, dev_blkval, work, work_bytes, stream);
+}
+
+extern "C" int chb_precision_flags(int precision) { return precision_flags(precision); }
+
+extern "C" int chb_cholesky_prec(chb_plan* plan, int precision, const double* host_in, double* host_out,
+                                 double* dev_blkval, void* work, size_t work_bytes, void* stream) {
+  return run_io(plan, CHB_OP_CHOLESKY, host_in, host_out, dev_blkval, work, work_bytes, stream, precision);
+}
+
+extern "C" int chb_projected_inverse_prec(chb_plan* plan, int precision, const double* host_in, double* host_out,
+                                          double* dev_blkval, void* work, size_t work_bytes, void* stream) {
+  return run_io(plan, CHB_OP_PROJECTED_INVERSE, host_in, host_out, dev_blkval, work, work_bytes, stream, precision);
 }
 
 extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
@@ -180,6 +197,19 @@ extern "C" int chb_sym_weight(chb_plan* plan, const double* x, double* y, double
   if (rc) return rc;
   cudaError_t e = symw_launch(x, y, alpha, plan->d_fronts, (int)plan->nsn, (cudaStream_t)stream);
   if (e != cudaSuccess) return set_error(-100 - (int)e, "sym_weight launch failed: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+extern "C" int chb_symv(chb_plan* plan, const double* blkval, const int64_t* sncolptr, const int64_t* snrowidx,
+                        const double* x, double* y, int64_t nrhs, int64_t ld, double alpha, void* stream) {
+  clear_error();
+  int rc = check_plan(plan);
+  if (rc) return rc;
+  if (!blkval || !sncolptr || !snrowidx || !x || !y) return set_error(-1, "null argument");
+  if (nrhs < 0 || ld < plan->n) return set_error(-1, "symv: nrhs >= 0 and ld >= n required");
+  cudaError_t e = symv_launch(blkval, plan->d_fronts, sncolptr, snrowidx, plan->d_perm, x, y, (int)plan->nsn,
+                              (int)nrhs, ld, alpha, (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_error(-100 - (int)e, "symv launch failed: %s", cudaGetErrorString(e));
   return 0;
 }
 

@@ -97,7 +97,45 @@ __global__ void __launch_bounds__(DOT_THREADS) seg_final(const double* __restric
     __syncthreads();
   }
 }
+// y += alpha X x for the symmetric chordal matrix X in blkval (lower
+// trapezoid of each supernode block; both triangles applied), nrhs columns
+// of leading dimension ld, rows in the original order through perm.  One
+// CTA per supernode; the scattered additions are atomic, so the summation
+// order (and the last bits) of y depend on the schedule.
+__global__ void __launch_bounds__(DOT_THREADS) symv_blocks(const double* __restrict__ blkval,
+                                                           const FrontDesc* __restrict__ fronts,
+                                                           const int64_t* __restrict__ sncolptr,
+                                                           const int64_t* __restrict__ snrowidx,
+                                                           const int64_t* __restrict__ perm, const double* __restrict__ x,
+                                                           double* __restrict__ y, int nsn, int nrhs, int64_t ld,
+                                                           double alpha) {
+  for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
+    const FrontDesc f = fronts[k];
+    const int64_t* __restrict__ rows = snrowidx + sncolptr[k];
+    const double* __restrict__ b = blkval + f.blk;
+    const int64_t count = (int64_t)f.nj * f.nn;
+    for (int64_t e = threadIdx.x; e < count; e += DOT_THREADS) {
+      const int j = (int)(e / f.nj), i = (int)(e % f.nj);
+      if (i < j) continue;  // strict upper part of the diagonal block
+      const double v = alpha * b[e];
+      const int64_t R = perm[rows[i]], C = perm[rows[j]];
+      for (int r = 0; r < nrhs; r++) {
+        atomicAdd(y + R + r * ld, v * x[C + r * ld]);
+        if (i != j) atomicAdd(y + C + r * ld, v * x[R + r * ld]);
+      }
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int64_t* sncolptr,
+                        const int64_t* snrowidx, const int64_t* perm, const double* x, double* y, int nsn, int nrhs,
+                        int64_t ld, double alpha, cudaStream_t stream) {
+  if (nsn <= 0 || nrhs <= 0) return cudaSuccess;
+  symv_blocks<<<nsn, DOT_THREADS, 0, stream>>>(blkval, fronts, sncolptr, snrowidx, perm, x, y, nsn, nrhs, ld, alpha);
+  return cudaGetLastError();
+}
 
 cudaError_t segment_sums(const double* partial, const int64_t* seg, int count, double* out, cudaStream_t stream) {
   if (count > 0) seg_final<<<count < 4096 ? count : 4096, DOT_THREADS, 0, stream>>>(partial, seg, count, out);

@@ -499,13 +499,96 @@ __device__ __forceinline__ void zero_acc(Acc& acc) {
       for (int h = 0; h < 4; h++) acc[i][j][h] = 0.0;
 }
 
+// ------------------------------------------------------------ TF32 path
+__device__ __forceinline__ uint32_t to_tf32(float f) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return r;
+}
+
+// TF32 MMA m16n8k8 with FP32 accumulation:
+//   A 16x8 row-major: a0 = A(g, q), a1 = A(g+8, q), a2 = A(g, q+4), a3 = A(g+8, q+4)
+//   B 8x8 col-major:  b0 = B(q, g), b1 = B(q+4, g)
+//   C 16x8: as the FP64 MMA (c0,c1 row g, c2,c3 row g+8; columns 2q, 2q+1)
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+typedef float AccF[2][4][4];
+
+// High and low TF32 parts of an FP64 value (x ~ hi + lo to about 22 bits).
+__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
+  const float f = (float)x;
+  hi = to_tf32(f);
+  lo = to_tf32((float)(x - (double)__uint_as_float(hi)));
+}
+
+// accf += A(:, 0:kn) B(:, 0:kn)^T from FP64 stages (kn a multiple of 8; the
+// stage is zero past K).  X3: three products (hi*hi + hi*lo + lo*hi).
+template <bool X3>
+__device__ __forceinline__ void mma_block_tf32(const double* sA, const double* sB, int kn, AccF& acc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int r0 = (warp >> 1) * 32 + g, c0 = (warp & 1) * 32 + g;
+#pragma unroll 2
+  for (int kk = 0; kk < kn; kk += 8) {
+    uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+    const double* ak0 = sA + (kk + q) * LDS + r0;
+    const double* ak4 = sA + (kk + q + 4) * LDS + r0;
+    const double* bk0 = sB + (kk + q) * LDS + c0;
+    const double* bk4 = sB + (kk + q + 4) * LDS + c0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const double v[4] = {ak0[16 * i], ak0[16 * i + 8], ak4[16 * i], ak4[16 * i + 8]};
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        if (X3) split_tf32(v[e], ah[i][e], al[i][e]);
+        else ah[i][e] = to_tf32((float)v[e]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double v0 = bk0[8 * j], v1 = bk4[8 * j];
+      if (X3) {
+        split_tf32(v0, bh[j][0], bl[j][0]);
+        split_tf32(v1, bh[j][1], bl[j][1]);
+      } else {
+        bh[j][0] = to_tf32((float)v0);
+        bh[j][1] = to_tf32((float)v1);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (X3) {
+          mma_tf32(acc[i][j], al[i], bh[j][0], bh[j][1]);
+          mma_tf32(acc[i][j], ah[i], bl[j][0], bl[j][1]);
+        }
+        mma_tf32(acc[i][j], ah[i], bh[j][0], bh[j][1]);
+      }
+  }
+}
+
 // acc = opA * opB^T over K through a GEMM_STAGES-deep ring of K chunks in
 // shared memory: the copies of chunk c + GEMM_STAGES - 1 are in flight while
 // chunk c is multiplied; one barrier per chunk.
 constexpr int GEMM_STAGES = 4;
 constexpr int STAGE_DOUBLES = 2 * KC * LDS;  // A chunk, then B chunk
 
-__device__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm, Acc& acc) {
+template <int PREC>
+__device__ void gemm_acc_p(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm, Acc& acc) {
+  AccF accf;
+  if (PREC != PREC_FP64) {
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int h = 0; h < 4; h++) accf[i][j][h] = 0.f;
+  }
   zero_acc(acc);
   const int nch = (K + KC - 1) / KC;
   double* const ring = sm.A;
@@ -529,11 +612,29 @@ __device__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, cons
     cp_async_commit();
     const double* st = ring + (c % GEMM_STAGES) * STAGE_DOUBLES;
     int kn = min(KC, K - c * KC);
-    kn = (kn + 3) & ~3;
-    mma_block(st, st + KC * LDS, kn, acc);
+    if (PREC == PREC_FP64) {
+      kn = (kn + 3) & ~3;
+      mma_block(st, st + KC * LDS, kn, acc);
+    } else {
+      kn = (kn + 7) & ~7;
+      mma_block_tf32<PREC == PREC_TF32X3>(st, st + KC * LDS, kn, accf);
+    }
   }
   cp_async_wait_group<0>();
   __syncthreads();
+  if (PREC != PREC_FP64) {
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int h = 0; h < 4; h++) acc[i][j][h] = (double)accf[i][j][h];
+  }
+}
+
+__device__ __forceinline__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm,
+                                         Acc& acc) {
+  gemm_acc_p<PREC_FP64>(A, B, m, n, K, sm, acc);
 }
 
 // C = alpha*acc + beta*C (masked to m x n and, for lower, to r + cdiag >= c).
@@ -594,7 +695,9 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
     const double alpha = la ? (ph == 0 ? 1.0 : -1.0) : t.alpha;
     const double beta = la ? (ph == 0 ? 0.0 : 1.0) : t.beta;
     Acc acc;
-    gemm_acc(A, B, m, n, K, sm, acc);
+    if (la || t.c.prec == PREC_FP64) gemm_acc_p<PREC_FP64>(A, B, m, n, K, sm, acc);
+    else if (t.c.prec == PREC_TF32) gemm_acc_p<PREC_TF32>(A, B, m, n, K, sm, acc);
+    else gemm_acc_p<PREC_TF32X3>(A, B, m, n, K, sm, acc);
     store_acc(ra.bases[oc.base] + oc.off, oc.ld, m, n, lower, cdiag, alpha, beta, acc);
     if (la && ph == 0) {
       __syncthreads();

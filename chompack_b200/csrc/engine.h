@@ -88,12 +88,18 @@ enum QlOp : int {
   QL_PANEL = 1    // Householder reflections of the panel; W' and T factor
 };
 
+// Product precision of a GEMM task (its C operand's prec): FP64 tensor
+// cores, or TF32 tensor cores with FP32 accumulation from the FP64 operands
+// (one product, or three with a high/low split of each operand, which
+// carries about 22 bits); the result is added to C in FP64.
+enum Precision : int16_t { PREC_FP64 = 0, PREC_TF32 = 1, PREC_TF32X3 = 2 };
+
 struct Operand {
   int64_t off;    // element offset from the base pointer
   int32_t ld;     // leading dimension
   uint8_t base;   // Base slot
   uint8_t mode;   // OpMode
-  int16_t pad;
+  int16_t prec;   // C operand of T_GEMM: product precision (Precision); else 0
   int32_t diag;   // diagonal offset for OM_TRI_* / OM_SYM
   int32_t pad2;   // OM_SYM: column offset of k = 0
 };

@@ -125,6 +125,14 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     prog->io = make_io_spec(*plan, (io & PF_IO_IN) != 0, (io & PF_IO_OUT) != 0);
     flags &= ~(PF_IO_IN | PF_IO_OUT);
   }
+  const int16_t prec = (flags & PF_TF32X3) ? PREC_TF32X3 : (flags & PF_TF32) ? PREC_TF32 : PREC_FP64;
+  if (prec != PREC_FP64) {
+    if (op != CHB_OP_CHOLESKY && op != CHB_OP_PROJECTED_INVERSE) {
+      set_error(-2, "mixed precision is available for cholesky and projected_inverse");
+      return nullptr;
+    }
+    flags &= ~(PF_TF32 | PF_TF32X3);
+  }
   int rc;
   switch (op) {
     case CHB_OP_CHOLESKY: rc = build_cholesky(*plan, *prog); break;
@@ -136,6 +144,9 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;
+  if (prec != PREC_FP64)
+    for (Task& t : prog->tasks)
+      if (t.op == T_GEMM) t.c.prec = prec;
   for (const Task& t : prog->tasks)
     if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
   // Default schedule per sweep, by measurement on a 3-D grid of 64,000

@@ -129,6 +129,11 @@ struct HostIo {
 // flags).
 constexpr int PF_IO_IN = 1 << 16;
 constexpr int PF_IO_OUT = 1 << 17;
+// Program flags selecting the mixed-precision variants of cholesky and
+// projected_inverse: every GEMM task's product in TF32 (or 3xTF32) with
+// FP32 accumulation; diagonal tiles, look-ahead steps and sums stay FP64.
+constexpr int PF_TF32 = 1 << 18;
+constexpr int PF_TF32X3 = 1 << 19;
 
 // Launch a program.  bases: MAX_BASES device pointers (unused slots null).
 int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, double* const* bases, int nbases,
@@ -143,6 +148,9 @@ cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, dou
 cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,
                         cudaStream_t stream);
 cudaError_t segment_sums(const double* partial, const int64_t* seg, int count, double* out, cudaStream_t stream);
+cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int64_t* sncolptr,
+                        const int64_t* snrowidx, const int64_t* perm, const double* x, double* y, int nsn, int nrhs,
+                        int64_t ld, double alpha, cudaStream_t stream);
 cudaError_t logdet_partials(const double* l, const FrontDesc* fronts, int nsn, double* partial, cudaStream_t stream);
 cudaError_t dot_partials(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
                          cudaStream_t stream);

@@ -120,6 +120,31 @@ int chb_projected_inverse_io(chb_plan* plan, const double* host_in, double* host
                              void* work, size_t work_bytes, void* stream);
 int chb_llt_io(chb_plan* plan, const double* host_in, double* host_out, double* dev_blkval, void* work,
                size_t work_bytes, void* stream);
+/* Mixed precision (no counterpart in the reference).  Every GEMM task of
+ * the sweep (Schur-complement updates, panel solves through the explicit
+ * inverse of the diagonal tile, the products of the projected inverse)
+ * runs on TF32 tensor cores with FP32 accumulation from the FP64 operands
+ * (CHB_PREC_TF32: one product, about 11 bits per operand; CHB_PREC_TF32X3:
+ * high/low splits and three products, about 22 bits); results are added in
+ * FP64.  Diagonal-tile factorisations and inverses, the look-ahead steps,
+ * split-K sums, assembly and extraction stay FP64.  host_in / host_out as
+ * for chb_cholesky_io (NULL: device values only).  Workspace: the flags
+ * chb_precision_flags(precision) | chb_io_flags(...). */
+enum { CHB_PREC_FP64 = 0, CHB_PREC_TF32 = 1, CHB_PREC_TF32X3 = 2 };
+
+/* y += alpha X x for the symmetric chordal matrix in blkval (FP64; the
+ * residual of iterative refinement): x, y are n x nrhs column-major with
+ * leading dimension ld, rows in the original order; sncolptr / snrowidx
+ * are the symbolic's arrays on the device (int64).  No counterpart in the
+ * reference's C code (its Python solves build the residual with cvxopt). */
+int chb_symv(chb_plan* plan, const double* blkval, const int64_t* sncolptr, const int64_t* snrowidx, const double* x,
+             double* y, int64_t nrhs, int64_t ld, double alpha, void* stream);
+int chb_precision_flags(int precision);
+int chb_cholesky_prec(chb_plan* plan, int precision, const double* host_in, double* host_out, double* dev_blkval,
+                      void* work, size_t work_bytes, void* stream);
+int chb_projected_inverse_prec(chb_plan* plan, int precision, const double* host_in, double* host_out,
+                               double* dev_blkval, void* work, size_t work_bytes, void* stream);
+
 /* Introspection of a streamed program: counts[0..1] = incoming and
  * outgoing chunks; the incoming chunks' value offsets (count + 1) and copy
  * order; the outgoing chunks' value offsets (count + 1) and the order in

@@ -15,7 +15,7 @@ import numpy as np
 
 from chompack_b200 import _native as N
 
-OPERAND = np.dtype([("off", "<i8"), ("ld", "<i4"), ("base", "u1"), ("mode", "u1"), ("pad", "<i2"),
+OPERAND = np.dtype([("off", "<i8"), ("ld", "<i4"), ("base", "u1"), ("mode", "u1"), ("prec", "<i2"),
                     ("diag", "<i4"), ("pad2", "<i4")])
 TASK = np.dtype({
     "names": ["op", "cmode", "nwait", "wait_off", "group", "m", "n", "k", "cdiag", "aux", "alpha", "beta",
