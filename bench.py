@@ -257,6 +257,58 @@ def cpu_baseline(s, A, budget_s=15.0):
     return out
 
 
+def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
+    """Mixed-precision form (GEMM tiles on TF32 tensor cores, FP64 diagonal
+    tiles): log det forward + backward (cholesky + projected_inverse) on the
+    3-D 7-point grid side^3 with merge_size_fill(merge), timed in FP64,
+    TF32 and 3xTF32, with the errors of log det, its gradient and the factor
+    against the FP64 path, and an nrhs solve refined with FP64 residuals to
+    a normwise relative residual of 1e-12."""
+    import torch
+    import chompack_b200 as cp
+    from chompack_b200 import mixed
+    A, s = build_problem(side=side, merge=merge)
+    fl = sweep_flops(s)
+    flops = fl["cholesky"] + fl["projected_inverse"]
+    X0 = cp.cspmatrix(s, device=dev) + A
+    out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d); log det forward + backward "
+                       "(cholesky + projected_inverse)" % (side, s.n, merge[0], merge[1]),
+           "flops": flops}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for prec in ("fp64", "tf32", "tf32x3"):
+        X = cp.cspmatrix(s, blkval=X0.blkval.clone())
+        times = []
+        for it in range(reps + 2):
+            X.blkval.copy_(X0.blkval)
+            X.is_factor = False
+            torch.cuda.synchronize(dev)
+            ev0.record()
+            cp.cholesky(X, precision=prec)
+            cp.projected_inverse(X, precision=prec)
+            ev1.record()
+            torch.cuda.synchronize(dev)
+            if it >= 2:
+                times.append(ev0.elapsed_time(ev1))
+        ms = float(np.median(times))
+        entry = {"ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1)}
+        if prec != "fp64":
+            ld, Y, rep = mixed.logdet_and_gradient(X0, precision=prec)
+            entry.update({k: rep[k] for k in ("logdet_rel_error", "gradient_rel_error", "factor_rel_error")})
+            L = cp.cspmatrix(s, blkval=X0.blkval.clone())
+            cp.cholesky(L, precision=prec)
+            B = torch.from_numpy(np.asfortranarray(np.random.default_rng(11).standard_normal((s.n, nrhs)))).to(dev)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            x, srep = mixed.solve(X0, L, B, tol=1e-12, maxiter=40)
+            torch.cuda.synchronize(dev)
+            entry["solve"] = {"nrhs": nrhs, "iterations": srep["iterations"],
+                              "residual": srep["residuals"][-1], "ms": round((time.perf_counter() - t0) * 1e3, 2)}
+        out[prec] = entry
+    out["speedup_tf32"] = round(out["fp64"]["ms"] / out["tf32"]["ms"], 3)
+    out["speedup_tf32x3"] = round(out["fp64"]["ms"] / out["tf32x3"]["ms"], 3)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -266,6 +318,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the timings of the other sweeps")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section (48^3)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -469,6 +522,11 @@ def main():
             out["clocks"] = clocks
         if e2e:
             out["e2e"] = e2e
+        if not args.no_mixed and not args.no_other:
+            try:
+                out["mixed_precision"] = mixed_precision_section(dev)
+            except Exception as exc:  # reported beside the headline, never required
+                out["mixed_precision"] = {"unavailable": str(exc)}
         if not args.no_cpu:
             try:
                 out["cpu_baseline"] = cpu_baseline(s, A)

@@ -100,8 +100,13 @@ __global__ void __launch_bounds__(DOT_THREADS) seg_final(const double* __restric
 // y += alpha X x for the symmetric chordal matrix X in blkval (lower
 // trapezoid of each supernode block; both triangles applied), nrhs columns
 // of leading dimension ld, rows in the original order through perm.  One
-// CTA per supernode; the scattered additions are atomic, so the summation
-// order (and the last bits) of y depend on the schedule.
+// CTA per supernode k (nn columns, nj rows):
+//   rows: y[row i] += sum_j X(i, j) x[col j] with one thread per row (the
+//         diagonal block read symmetrically), one atomic per row;
+//   columns: y[col j] += sum_{i >= nn} X(i, j) x[row i] for the rows below
+//         the diagonal block, one warp per column, one atomic per column.
+// The atomics make the last bits of y depend on the schedule.
+constexpr int SYMV_RHS = 8;  // right-hand sides per pass
 __global__ void __launch_bounds__(DOT_THREADS) symv_blocks(const double* __restrict__ blkval,
                                                            const FrontDesc* __restrict__ fronts,
                                                            const int64_t* __restrict__ sncolptr,
@@ -109,19 +114,54 @@ __global__ void __launch_bounds__(DOT_THREADS) symv_blocks(const double* __restr
                                                            const int64_t* __restrict__ perm, const double* __restrict__ x,
                                                            double* __restrict__ y, int nsn, int nrhs, int64_t ld,
                                                            double alpha) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
     const FrontDesc f = fronts[k];
+    const int nn = f.nn, nj = f.nj;
     const int64_t* __restrict__ rows = snrowidx + sncolptr[k];
     const double* __restrict__ b = blkval + f.blk;
-    const int64_t count = (int64_t)f.nj * f.nn;
-    for (int64_t e = threadIdx.x; e < count; e += DOT_THREADS) {
-      const int j = (int)(e / f.nj), i = (int)(e % f.nj);
-      if (i < j) continue;  // strict upper part of the diagonal block
-      const double v = alpha * b[e];
-      const int64_t R = perm[rows[i]], C = perm[rows[j]];
-      for (int r = 0; r < nrhs; r++) {
-        atomicAdd(y + R + r * ld, v * x[C + r * ld]);
-        if (i != j) atomicAdd(y + C + r * ld, v * x[R + r * ld]);
+    for (int r0 = 0; r0 < nrhs; r0 += SYMV_RHS) {
+      const int nr = min(SYMV_RHS, nrhs - r0);
+      // rows
+      for (int i = threadIdx.x; i < nj; i += DOT_THREADS) {
+        double acc[SYMV_RHS];
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++) acc[r] = 0.0;
+        for (int j = 0; j < nn; j++) {
+          const double v = (i >= j) ? b[(int64_t)j * nj + i] : b[(int64_t)i * nj + j];
+          const int64_t C = perm[rows[j]];
+#pragma unroll
+          for (int r = 0; r < SYMV_RHS; r++)
+            if (r < nr) acc[r] = fma(v, x[C + (r0 + r) * ld], acc[r]);
+        }
+        const int64_t R = perm[rows[i]];
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++)
+          if (r < nr) atomicAdd(y + R + (r0 + r) * ld, alpha * acc[r]);
+      }
+      // columns, from the rows below the diagonal block
+      for (int j = warp; j < nn; j += DOT_THREADS / 32) {
+        double acc[SYMV_RHS];
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++) acc[r] = 0.0;
+        for (int i = nn + lane; i < nj; i += 32) {
+          const double v = b[(int64_t)j * nj + i];
+          const int64_t R = perm[rows[i]];
+#pragma unroll
+          for (int r = 0; r < SYMV_RHS; r++)
+            if (r < nr) acc[r] = fma(v, x[R + (r0 + r) * ld], acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        }
+        if (lane == 0) {
+          const int64_t C = perm[rows[j]];
+#pragma unroll
+          for (int r = 0; r < SYMV_RHS; r++)
+            if (r < nr) atomicAdd(y + C + (r0 + r) * ld, alpha * acc[r]);
+        }
       }
     }
   }
