@@ -1173,7 +1173,21 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
 // F(i, j) is the front panel (operand a: nj rows, ld a.ld) for j < nn, else
 // the update block U_k (operand c, ld c.ld).  One warp per child column;
 // children are applied one after the other.
-__device__ void run_asm(const RunArgs& ra, const Task& t) {
+// A child's relative indices, staged in shared memory once per child when
+// they fit (one coalesced pass), so that each scattered access costs one
+// round trip instead of two; otherwise read from global memory.
+constexpr int RIDX_SMEM_MAX = ENGINE_SMEM_BASE_DOUBLES * 2;  // int32 entries in the base shared memory
+__device__ __forceinline__ const int32_t* stage_ridx(const int32_t* __restrict__ r, int N, double* smem) {
+  if (N > RIDX_SMEM_MAX) return r;
+  int32_t* sr = reinterpret_cast<int32_t*>(smem);
+  for (int i = threadIdx.x; i < N; i += NTHREADS) sr[i] = __ldg(r + i);
+  __syncthreads();
+  return sr;
+}
+
+constexpr int GATHER_INFLIGHT = 8;  // scattered elements in flight per lane
+
+__device__ void run_asm(const RunArgs& ra, const Task& t, double* smem) {
   const FrontDesc f = ra.fronts[t.aux[0]];
   const int j0 = t.aux[1], j1 = t.aux[2];
   const bool zero_u = (t.aux[3] & 1) != 0;
@@ -1192,33 +1206,32 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
   for (int l = f.chend - 1; l >= f.chbeg; l--) {
     const FrontDesc ch = ra.fronts[ra.chidx[l]];
     const int N = ch.na;
-    const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+    const int32_t* r = stage_ridx(ra.relidx + ch.relptr, N, smem);
     const double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
     // child columns with r[q] in [j0, j1): r is strictly increasing
     int lo = 0, hi = N;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < j0) lo = mid + 1; else hi = mid; }
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (r[mid] < j0) lo = mid + 1; else hi = mid; }
     const int q0 = lo;
     hi = N;
-    while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(r + mid) < j1) lo = mid + 1; else hi = mid; }
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (r[mid] < j1) lo = mid + 1; else hi = mid; }
     const int q1 = lo;
     for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
-      const int col = __ldg(r + q);
+      const int col = r[q];
       double* __restrict__ dst =
           (col < f.nn) ? P + (int64_t)col * ldp : Uk + (int64_t)(col - f.nn) * ldu - f.nn;
       const double* __restrict__ src = Uc + (int64_t)q * N;
-      for (int i0 = q; i0 < N; i0 += 4 * 32) {
-        int ri[4];
-        double u[4], d[4];
+      for (int i0 = q; i0 < N; i0 += GATHER_INFLIGHT * 32) {
+        int ri[GATHER_INFLIGHT];
+        double u[GATHER_INFLIGHT], d[GATHER_INFLIGHT];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
+        for (int e = 0; e < GATHER_INFLIGHT; e++) {
           const int i = i0 + lane + 32 * e;
-          ri[e] = (i < N) ? __ldg(r + i) : -1;
+          ri[e] = (i < N) ? r[i] : -1;
           u[e] = (i < N) ? __ldcg(src + i) : 0.0;
+          d[e] = (i < N) ? __ldcg(dst + ri[e]) : 0.0;
         }
 #pragma unroll
-        for (int e = 0; e < 4; e++) d[e] = (ri[e] >= 0) ? __ldcg(dst + ri[e]) : 0.0;
-#pragma unroll
-        for (int e = 0; e < 4; e++)
+        for (int e = 0; e < GATHER_INFLIGHT; e++)
           if (ri[e] >= 0) dst[ri[e]] = d[e] + u[e];
       }
     }
@@ -1233,12 +1246,12 @@ __device__ void run_asm(const RunArgs& ra, const Task& t) {
 //   operand a (rows < nn, ld a.ld) when row < nn,
 //   operand b (rows >= nn, row nn at offset 0, ld b.ld) when col < nn <= row,
 //   operand c (update block, ld c.ld) when col >= nn.
-__device__ void run_extract(const RunArgs& ra, const Task& t) {
+__device__ void run_extract(const RunArgs& ra, const Task& t, double* smem) {
   const FrontDesc ch = ra.fronts[t.aux[0]];
   const FrontDesc f = ra.fronts[ch.parent];
   const int q0 = t.aux[1], q1 = t.aux[2];
   const int N = ch.na, nn = f.nn;
-  const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+  const int32_t* r = stage_ridx(ra.relidx + ch.relptr, N, smem);
   const double* __restrict__ F11 = ra.bases[t.a.base] + t.a.off;
   const double* __restrict__ F21 = ra.bases[t.b.base] + t.b.off;
   const double* __restrict__ F22 = ra.bases[t.c.base] + t.c.off;
@@ -1246,15 +1259,13 @@ __device__ void run_extract(const RunArgs& ra, const Task& t) {
   double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int q = q0 + warp; q < q1; q += NTHREADS / 32) {
-    const int col = __ldg(r + q);
-    for (int i0 = q; i0 < N; i0 += 4 * 32) {
-      double v[4];
-      int idx[4];
+    const int col = r[q];
+    for (int i0 = q; i0 < N; i0 += GATHER_INFLIGHT * 32) {
+      double v[GATHER_INFLIGHT];
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
+      for (int e = 0; e < GATHER_INFLIGHT; e++) {
         const int i = i0 + lane + 32 * e;
-        idx[e] = i;
-        const int row = (i < N) ? __ldg(r + i) : 0;
+        const int row = (i < N) ? r[i] : 0;
         const double* src;
         if (col >= nn) src = F22 + (int64_t)(col - nn) * ld22 + (row - nn);
         else if (row >= nn) src = F21 + (int64_t)col * ld21 + (row - nn);
@@ -1262,8 +1273,10 @@ __device__ void run_extract(const RunArgs& ra, const Task& t) {
         v[e] = (i < N) ? __ldcg(src) : 0.0;
       }
 #pragma unroll
-      for (int e = 0; e < 4; e++)
-        if (idx[e] < N) Uc[(int64_t)q * N + idx[e]] = v[e];
+      for (int e = 0; e < GATHER_INFLIGHT; e++) {
+        const int i = i0 + lane + 32 * e;
+        if (i < N) Uc[(int64_t)q * N + i] = v[e];
+      }
     }
   }
 }
@@ -1777,8 +1790,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_LA: run_gemm_or_la(ra, t, sm); break;
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem, ti); break;
-      case T_ASM: run_asm(ra, t); break;
-      case T_EXTRACT: run_extract(ra, t); break;
+      case T_ASM: run_asm(ra, t, smem); break;
+      case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;
       case T_QL: run_ql(ra, t, smem); break;
