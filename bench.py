@@ -26,6 +26,7 @@ import sys
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+OUT_DIR = os.environ.get("CHB_OUT_DIR", "gpurun_out")  # the folder whose files are kept after a run
 sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
@@ -61,7 +62,7 @@ def build_problem(side=40, merge=(32, 32), seed=0):
 class ClockSampler(object):
     """SM clock and clock-event-reason sampling during the timed region, by
     NVML polling from a thread (every 2 ms; read-only queries).  The samples
-    are also written to gpurun_out/clocks_bench_<pid>.csv."""
+    are also written as CSV beside the run's other outputs (OUT_DIR)."""
 
     # NVML clocks-event-reason bits
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
@@ -71,7 +72,7 @@ class ClockSampler(object):
         self.dev = dev
         self.thread = None
         self.samples = []
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % os.getpid())
+        self.path = os.path.join(ROOT, OUT_DIR, "clocks_bench_%d.csv" % os.getpid())
 
     def _handle(self):
         import pynvml
