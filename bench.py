@@ -310,6 +310,112 @@ def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
     return out
 
 
+def _event_ms(dev, fn, reps):
+    """Median CUDA-event time of fn() over reps runs after two warm-ups."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for it in range(reps + 2):
+        torch.cuda.synchronize(dev)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        if it >= 2:
+            times.append(e0.elapsed_time(e1))
+    return float(np.median(times))
+
+
+def batch_section(dev, count=256, value_sets=64, reps=5):
+    """Batched FP64 factorisation: `count` independent 2-D 5-point grids
+    (side uniform in 20..120, each node with 2 extra random neighbours
+    within grid distance 5, AMD ordering), and `value_sets` value sets on
+    one 64x64 grid pattern.  Each batch is one merged plan: cholesky and
+    projected_inverse of all its matrices take one launch each."""
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    out = {}
+    rng = np.random.default_rng(2024)
+    sides = rng.integers(20, 121, size=count)
+    As, symbs = [], []
+    for i, sd in enumerate(sides):
+        A = grids.grid2d_extra(int(sd), seed=1000 + i)
+        As.append(A)
+        symbs.append(cp.symbolic(A, p=cp.amd.order(A)))
+    for name, Bs, Xs in (("uneven_grids", symbs, As), ("value_sets_64x64", None, None)):
+        if Bs is None:
+            A0 = grids.grid2d(64, seed=7)
+            s0 = cp.symbolic(A0, p=cp.amd.order(A0))
+            Bs = [s0] * value_sets
+            Xs = [grids.grid2d(64, seed=7 + v) for v in range(value_sets)]
+        B = cp.batch(Bs, device=dev.index)
+        x0 = B.assemble(Xs)
+        x = x0.clone()
+
+        def step():
+            x.copy_(x0)
+            B.cholesky(x)
+            B.projected_inverse(x)
+        ms = _event_ms(dev, step, reps)
+        flops = sum(sweep_flops(sb)["cholesky"] + sweep_flops(sb)["projected_inverse"] for sb in Bs)
+        out[name] = {"matrices": len(Bs), "n_total": int(sum(sb.n for sb in Bs)), "values": int(B.size),
+                     "launches_per_step": 2, "ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1),
+                     "matrices_per_s": round(len(Bs) / ms * 1e3, 1), "step": "cholesky + projected_inverse (copy of "
+                     "the values included)"}
+    return out
+
+
+def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
+    """Differentiation: log det and its gradient (the projected inverse) for
+    `value_sets` value sets on the 3-D 7-point grid side^3 in one batch
+    (forward + backward = two launches), a central finite-difference check
+    of the gradient and of the second derivative (hessian) along a random
+    symmetric direction on the pattern, for the first value set."""
+    import torch
+    import chompack_b200 as cp
+    from chompack_b200 import grids, autograd
+    A0 = grids.grid3d(side, seed=0)
+    s = cp.symbolic(A0, p=cp.amd.order(A0), merge_function=cp.merge_size_fill(32, 32))
+    B = cp.batch([s] * value_sets, device=dev.index)
+    x0 = B.assemble([grids.grid3d(side, seed=v) for v in range(value_sets)])
+    x = x0.clone()
+    res = {}
+
+    def fwd_bwd():
+        x.copy_(x0)
+        B.cholesky(x)
+        res["ld"] = B.logdet(x)
+        B.projected_inverse(x)
+    ms = _event_ms(dev, fwd_bwd, reps)
+    fl = sweep_flops(s)
+    flops = value_sets * (fl["cholesky"] + fl["projected_inverse"])
+    # checks on value set 0
+    X = cp.cspmatrix(s, blkval=x0[:int(s.blkptr[-1])].clone())
+    rng = np.random.default_rng(5)
+    U = cp.cspmatrix(s, blkval=torch.from_numpy(rng.standard_normal(int(s.blkptr[-1]))).to(dev))
+
+    def ld_at(t):
+        return float(autograd.logdet_values(X.blkval + t * U.blkval, s))
+    Y = autograd.logdet_gradient(X)
+    g = cp.dot(Y, U)
+    fd = (ld_at(h) - ld_at(-h)) / (2 * h)
+    L = cp.cspmatrix(s, blkval=X.blkval.clone())
+    cp.cholesky(L)
+    HU = autograd.logdet_hvp(L, Y, U)
+    second = cp.dot(U, HU)
+
+    def g_at(t):
+        Xt = cp.cspmatrix(s, blkval=X.blkval + t * U.blkval)
+        return cp.dot(autograd.logdet_gradient(Xt), U)
+    fd2 = (g_at(1e-4) - g_at(-1e-4)) / 2e-4
+    return {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(32,32), %d value sets in one batch"
+                        % (side, s.n, value_sets),
+            "fwd_bwd_ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1), "launches": 2,
+            "gradient_fd_rel_error": abs(g - fd) / max(abs(fd), 1e-300),
+            "hvp_fd_rel_error": abs(second - fd2) / max(abs(fd2), 1e-300),
+            "fd_steps": [h, 1e-4]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,6 +426,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-other", action="store_true", help="skip the timings of the other sweeps")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision section (48^3)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch and autograd sections")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -528,6 +635,12 @@ def main():
                 out["mixed_precision"] = mixed_precision_section(dev)
             except Exception as exc:  # reported beside the headline, never required
                 out["mixed_precision"] = {"unavailable": str(exc)}
+        if not args.no_batch and not args.no_other:
+            for key, fn in (("batch", batch_section), ("autograd", autograd_section)):
+                try:
+                    out[key] = fn(dev)
+                except Exception as exc:  # reported beside the headline, never required
+                    out[key] = {"unavailable": str(exc)}
         if not args.no_cpu:
             try:
                 out["cpu_baseline"] = cpu_baseline(s, A)

@@ -63,16 +63,20 @@ def grid2d_extra(side, seed=0, extra=2, radius=5):
     offs = np.array(offs, dtype=np.int64)
     xs = np.arange(n) % side
     ys = np.arange(n) // side
-    ei, ej = [], []
-    for v in range(n):
-        cx, cy = xs[v] + offs[:, 0], ys[v] + offs[:, 1]
-        ok = (cx >= 0) & (cx < side) & (cy >= 0) & (cy < side)
-        cand = (cx[ok] + side * cy[ok])
-        pick = rng.choice(cand, size=min(extra, cand.size), replace=False)
-        for u in pick:
-            a, b = (v, int(u)) if v > u else (int(u), v)
-            ei.append(a)
-            ej.append(b)
+    # every node draws `extra` distinct candidates uniformly: random keys on
+    # its candidate offsets, invalid ones pushed last, the smallest keys win
+    cx = xs[:, None] + offs[None, :, 0]
+    cy = ys[:, None] + offs[None, :, 1]
+    ok = (cx >= 0) & (cx < side) & (cy >= 0) & (cy < side)
+    keys = np.where(ok, rng.random(ok.shape), 2.0)
+    k = min(extra, offs.shape[0])
+    pick = np.argpartition(keys, k - 1, axis=1)[:, :k] if k > 0 else np.zeros((n, 0), dtype=np.int64)
+    rows = np.arange(n)[:, None]
+    valid = ok[rows, pick]
+    u = (cx[rows, pick] + side * cy[rows, pick])[valid]
+    v = np.broadcast_to(rows, pick.shape)[valid]
+    ei = np.maximum(u, v)
+    ej = np.minimum(u, v)
     I.append(np.asarray(ei, dtype=np.int64))
     J.append(np.asarray(ej, dtype=np.int64))
     seed_vals = int(rng.integers(0, 2**31 - 1)) ^ seed
