@@ -186,40 +186,47 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       }
     }
     // copy back into blkval (all readers of the factor block are done once
-    // the final Y11 tiles are: they wait on every M tile and S21 tile)
-    for (int i = 0; i < NBc; i++) {
-      for (int j = 0; j <= i; j++) {
-        const int iT = i * T, jT = j * T;
+    // the final Y11 tiles are: they wait on every M tile and S21 tile), one
+    // task per column strip and part: the diagonal tile (lower part, zeros
+    // above), the rows below it in Y11, the strict upper part (zeros, as
+    // projected_inverse.c:36-38 leaves it) and the rows of S21
+    for (int j = 0; j < NBc; j++) {
+      const int jT = j * T;
+      {
         Task t = make_task(T_COPY);
-        t.m = bw(i);
+        t.m = bw(j);
         t.n = bw(j);
-        t.a = opnd(B_WS, Y + (int64_t)jT * nn + iT, nn);
-        t.c = opnd(B_X, blk + (int64_t)jT * nj + iT, nj);
-        t.aux[0] = (i == j) ? 3 : 0;
-        int id = B.add(t, {lv, 6, 0, (int)k, j, i});
+        t.a = opnd(B_WS, Y + (int64_t)jT * nn + jT, nn);
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + jT, nj);
+        t.aux[0] = 3;
+        int id = B.add(t, {lv, 6, 0, (int)k, j, j});
         B.wait_group(id, yfinal);
       }
-      // strict upper tiles of the diagonal block are zeroed too
-      for (int j = i + 1; j < NBc; j++) {
-        const int iT = i * T, jT = j * T;
+      if (jT + T < nn) {
         Task t = make_task(T_COPY);
-        t.m = bw(i);
+        t.m = nn - (jT + T);
+        t.n = bw(j);
+        t.a = opnd(B_WS, Y + (int64_t)jT * nn + jT + T, nn);
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + jT + T, nj);
+        int id = B.add(t, {lv, 6, 0, (int)k, j, j + 1}, -1, 3.0 + (double)t.m * t.n / 4096.0);
+        B.wait_group(id, yfinal);
+      }
+      if (jT > 0) {
+        Task t = make_task(T_COPY);
+        t.m = jT;
         t.n = bw(j);
         t.aux[0] = 4;  // zeros
-        t.c = opnd(B_X, blk + (int64_t)jT * nj + iT, nj);
-        int id = B.add(t, {lv, 6, 1, (int)k, j, i});
+        t.c = opnd(B_X, blk + (int64_t)jT * nj, nj);
+        int id = B.add(t, {lv, 6, 1, (int)k, j, 0}, -1, 3.0 + (double)t.m * t.n / 8192.0);
         B.wait_group(id, yfinal);
       }
-    }
-    for (int i = 0; i < NBb; i++) {
-      for (int j = 0; j < NBc; j++) {
-        const int iT = i * T, jT = j * T;
+      if (na > 0) {
         Task t = make_task(T_COPY);
-        t.m = bh(i);
+        t.m = na;
         t.n = bw(j);
-        t.a = opnd(B_WS, S + (int64_t)jT * na + iT, na);
-        t.c = opnd(B_X, blk + (int64_t)jT * nj + nn + iT, nj);
-        int id = B.add(t, {lv, 6, 2, (int)k, j, i});
+        t.a = opnd(B_WS, S + (int64_t)jT * na, na);
+        t.c = opnd(B_X, blk + (int64_t)jT * nj + nn, nj);
+        int id = B.add(t, {lv, 6, 2, (int)k, j, 0}, -1, 3.0 + (double)t.m * t.n / 4096.0);
         B.wait_group(id, yfinal);
       }
     }

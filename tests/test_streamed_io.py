@@ -52,7 +52,8 @@ def _in_chunks(t, off):
 
 def _written_ranges(t):
     """Value ranges [lo, hi) a task writes (a tile of at most e = max(m, n)
-    rows and columns, or an extend-add's front columns)."""
+    rows and columns, a plain copy's m x n strip, or an extend-add's front
+    columns)."""
     op = int(t["op"])
     e = max(int(t["m"]), int(t["n"]), 1)
 
@@ -62,6 +63,11 @@ def _written_ranges(t):
             return [(int(o["off"]), int(o["off"]) + (e - 1) * int(o["ld"]) + e)]
         return []
     if op in (taskvm.T_NOP, taskvm.T_SIGNAL, taskvm.T_ARRIVAL, taskvm.T_EXTRACT):
+        return []
+    if op == taskvm.T_COPY and int(t["aux"][0]) & 24 == 0:
+        o = t["c"]
+        if int(o["base"]) == 0 and int(o["ld"]) > 0:
+            return [(int(o["off"]), int(o["off"]) + (max(int(t["n"]), 1) - 1) * int(o["ld"]) + max(int(t["m"]), 1))]
         return []
     if op in (taskvm.T_GEMM, taskvm.T_MROW, taskvm.T_COPY, taskvm.T_SUM):
         return tile("c")
