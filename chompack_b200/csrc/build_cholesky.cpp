@@ -33,6 +33,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int NBc = ceil_div(f.nn, T);
+    if (f.nj <= T) continue;  // a small front needs no scratch (one shared-memory task)
     if (f.na > 0) {
       scrS[k] = ws;
       ws += (int64_t)f.na * f.nn;
@@ -75,6 +76,21 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     const int64_t blk = f.blk, upd = f.upd, S = scrS[k], M = scrM[k];
     auto bw = [&](int c) { return std::min(T, nn - c * T); };  // column block width
     auto bh = [&](int i) { return std::min(T, na - i * T); };  // bottom tile height
+
+    // A front that fits one tile is one task: extend-add, partial Cholesky
+    // and Schur complement in shared memory (cholesky.c:33-72 for one node).
+    if (nj <= T) {
+      Task t = make_task(T_FRONT);
+      t.m = nj;
+      t.n = nn;
+      t.aux[0] = (int32_t)k;
+      t.a = opnd(B_X, blk, nj);
+      t.c = opnd(B_WS, upd, std::max(na, 1));
+      const double est = 3.0 + 0.02 * nn * (double)nj + 0.002 * (double)nj * nj;
+      int id = B.add(t, {lv, -1, 0, (int)k, 0, 0}, uc_group[k], est);
+      for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
+      continue;
+    }
 
     // --- extend-add (cholesky.c:33-52), split into column chunks of about
     // equal work (children's update entries landing in the chunk)

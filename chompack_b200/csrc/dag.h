@@ -125,8 +125,8 @@ struct DagBuilder {
 
   // Outgoing chunks that a task's writes to the values overlap.  A written
   // tile of at most e rows and columns (e = max(m, n)) spans
-  // [off, off + (e-1)*ld + e); a plain copy its m x n strip; an extend-add
-  // writes the front's columns [aux[1], aux[2]).
+  // [off, off + (e-1)*ld + e); a plain copy its m x n strip; a small front
+  // its block; an extend-add writes the front's columns [aux[1], aux[2]).
   static void out_chunks(const Task& t, const IoSpec& io, std::vector<int>& out) {
     out.clear();
     auto add_range = [&](int64_t lo, int64_t hi) {
@@ -141,6 +141,9 @@ struct DagBuilder {
     };
     switch (t.op) {
       case T_NOP: case T_SIGNAL: case T_ARRIVAL: case T_EXTRACT: break;  // an extract writes the workspace
+      case T_FRONT:  // the front's whole nj x nn block (and its update matrix, workspace)
+        if (t.a.base == B_X && t.a.ld > 0) add_range(t.a.off, t.a.off + (int64_t)t.m * t.n);
+        break;
       case T_COPY:
         // a plain copy writes its m x n strip; the (anti-)transposing ones a square
         if ((t.aux[0] & 24) == 0 && t.c.base == B_X && t.c.ld > 0)

@@ -1239,6 +1239,73 @@ __device__ void run_asm(const RunArgs& ra, const Task& t, double* smem) {
   }
 }
 
+// A whole small cholesky front (T_FRONT, nj <= TILE; cholesky.c:33-72 for
+// one node) in shared memory, F(r, c) at F[c*FLD + r], lower part:
+//   1. F = the block's lower trapezoid (columns < nn), zero elsewhere;
+//   2. the children's update matrices added, last child first;
+//   3. the first nn columns eliminated (right-looking: pivot, column scaled,
+//      trailing lower part updated, a warp per column), which leaves L11,
+//      L21 and the Schur complement F22 - L21 L21^T;
+//   4. the rows below replaced by W = L21 L11^{-1} (the reference's layout
+//      of the off-diagonal block), one row per thread;
+//   5. the block and the update matrix (operand c) written back.
+// A non-positive pivot records ctl[2] = j + 1 and continues with 1.
+constexpr int FLD = TILE + 1;
+static_assert(TILE * FLD <= ENGINE_SMEM_BASE_DOUBLES, "small front exceeds the engine's shared memory");
+
+__device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
+  const FrontDesc f = ra.fronts[t.aux[0]];
+  const int nn = f.nn, na = f.na, nj = f.nj;
+  double* F = smem;
+  double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ U = ra.bases[t.c.base] + t.c.off;
+  const int ldu = t.c.ld;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = NTHREADS / 32;
+  for (int c = warp; c < nj; c += NW)
+    for (int r = lane; r < nj; r += 32)
+      F[c * FLD + r] = (c < nn && r >= c) ? __ldcg(X + (int64_t)c * nj + r) : 0.0;
+  __syncthreads();
+  for (int l = f.chend - 1; l >= f.chbeg; l--) {
+    const FrontDesc ch = ra.fronts[ra.chidx[l]];
+    const int Nc = ch.na;
+    const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
+    const double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
+    for (int q = warp; q < Nc; q += NW) {
+      const int col = __ldg(rr + q);
+      for (int i = q + lane; i < Nc; i += 32) F[col * FLD + __ldg(rr + i)] += __ldcg(Uc + (int64_t)q * Nc + i);
+    }
+    __syncthreads();
+  }
+  int first_bad = -1;
+  for (int j = 0; j < nn; j++) {
+    const double d = F[j * FLD + j];
+    const bool bad = !(d > 0.0);
+    if (bad && first_bad < 0) first_bad = j;
+    const double lj = sqrt(bad ? 1.0 : d), rl = 1.0 / lj;
+    for (int i = j + 1 + tid; i < nj; i += NTHREADS) F[j * FLD + i] *= rl;
+    __syncthreads();
+    if (tid == 0) F[j * FLD + j] = lj;  // nobody reads it in the update below
+    for (int c = j + 1 + warp; c < nj; c += NW) {
+      const double fc = F[j * FLD + c];
+      for (int i = c + lane; i < nj; i += 32) F[c * FLD + i] -= F[j * FLD + i] * fc;
+    }
+    __syncthreads();
+  }
+  if (tid == 0 && first_bad >= 0) atomicCAS(&ra.ctl[2], 0, first_bad + 1);
+  for (int i = nn + tid; i < nj; i += NTHREADS)
+    for (int j = nn - 1; j >= 0; j--) {
+      double v = F[j * FLD + i];
+      for (int l2 = j + 1; l2 < nn; l2++) v -= F[l2 * FLD + i] * F[j * FLD + l2];
+      F[j * FLD + i] = v / F[j * FLD + j];
+    }
+  __syncthreads();
+  for (int c = warp; c < nn; c += NW)
+    for (int r = c + lane; r < nj; r += 32) X[(int64_t)c * nj + r] = F[c * FLD + r];
+  for (int q = warp; q < na; q += NW)
+    for (int i = q + lane; i < na; i += 32) U[(int64_t)q * ldu + i] = F[(nn + q) * FLD + nn + i];
+}
+
 // Gather of a child's update matrix out of its parent's front
 // (projected_inverse.c:62-71, completion.c:61-66): for child c = aux[0] and
 // child columns q in [aux[1], aux[2]), U_c(i, q) = F(r[i], r[q]) for i >= q,
@@ -1791,6 +1858,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem, ti); break;
       case T_ASM: run_asm(ra, t, smem); break;
+      case T_FRONT: run_front(ra, t, smem); break;
       case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;

@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL = 8, 9, 10, 11, 12, 13, 14
+T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL, T_FRONT = 8, 9, 10, 11, 12, 13, 14, 15
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -188,6 +188,8 @@ class VM(object):
                 X[didx[low]] = (X[didx] - L2 @ L2.T)[low]
         elif op == T_ASM:
             self._asm(t)
+        elif op == T_FRONT:
+            self._front(t)
         elif op == T_EXTRACT:
             self._extract(t)
         elif op == T_VEC:
@@ -274,6 +276,46 @@ class VM(object):
                     Pb[Pof + col * ldp + rows] += v
                 else:
                     Ub[Uof + (col - nn) * ldu + (rows - nn)] += v
+
+    def _front(self, t):
+        """A whole small cholesky front: extend-add of the children (last
+        to first), partial Cholesky of the nj x nj front, the Schur
+        complement into the update matrix, and the off-diagonal block
+        stored as L21 L11^{-1} (the reference's layout)."""
+        f = self.p.fronts[int(t["aux"][0])]
+        nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
+        WS = self.bases[B_WS]
+        X, off = self.bases[int(t["a"]["base"])], int(t["a"]["off"])
+        r = np.arange(nj)[:, None]
+        c = np.arange(nn)[None, :]
+        F = np.zeros((nj, nj))
+        F[:, :nn] = np.where(r >= c, X[off + c * nj + r], 0.0)
+        for l in range(int(f["chend"]) - 1, int(f["chbeg"]) - 1, -1):
+            ch = self.p.fronts[self.chidx[l]]
+            Nc = int(ch["na"])
+            rr = np.asarray(self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc], dtype=np.int64)
+            Uc = WS[int(ch["upd"]): int(ch["upd"]) + Nc * Nc].reshape((Nc, Nc), order="F")
+            for q in range(Nc):
+                F[rr[q:], rr[q]] += Uc[q:, q]
+        S = np.tril(F) + np.tril(F, -1).T
+        try:
+            L11 = np.linalg.cholesky(S[:nn, :nn])
+        except np.linalg.LinAlgError:
+            if self.info == 0:
+                self.info = 1
+            return
+        Li = np.linalg.inv(L11)
+        L21 = S[nn:, :nn] @ Li.T
+        blk = np.vstack([L11, L21 @ Li])              # nj x nn
+        low = np.broadcast_to(r >= c, blk.shape)
+        X[(off + c * nj + r)[low]] = blk[low]
+        if na > 0:
+            U = S[nn:, nn:] - L21 @ L21.T
+            Ub, Uof, ldu = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
+            ri = np.arange(na)[:, None]
+            ci = np.arange(na)[None, :]
+            lw = ri >= ci
+            Ub[(Uof + ci * ldu + ri)[lw]] = U[lw]
 
     def _vec(self, t):
         mode, nrhs = int(t["aux"][0]), int(t["n"])

@@ -52,8 +52,8 @@ def _in_chunks(t, off):
 
 def _written_ranges(t):
     """Value ranges [lo, hi) a task writes (a tile of at most e = max(m, n)
-    rows and columns, a plain copy's m x n strip, or an extend-add's front
-    columns)."""
+    rows and columns, a plain copy's m x n strip, a small front's block, or
+    an extend-add's front columns)."""
     op = int(t["op"])
     e = max(int(t["m"]), int(t["n"]), 1)
 
@@ -64,6 +64,9 @@ def _written_ranges(t):
         return []
     if op in (taskvm.T_NOP, taskvm.T_SIGNAL, taskvm.T_ARRIVAL, taskvm.T_EXTRACT):
         return []
+    if op == taskvm.T_FRONT:
+        o = t["a"]
+        return [(int(o["off"]), int(o["off"]) + int(t["m"]) * int(t["n"]))] if int(o["base"]) == 0 else []
     if op == taskvm.T_COPY and int(t["aux"][0]) & 24 == 0:
         o = t["c"]
         if int(o["base"]) == 0 and int(o["ld"]) > 0:
