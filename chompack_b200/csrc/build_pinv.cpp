@@ -30,6 +30,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
   std::vector<int64_t> scrM(N), scrY(N), scrS(N, -1);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
+    if (f.nj <= T) continue;  // a small front needs no scratch (one shared-memory task)
     scrM[k] = ws;
     ws += (int64_t)f.nn * f.nn;
     scrY[k] = ws;
@@ -49,10 +50,16 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     return o;
   };
 
-  // group: the parent's extract tasks that produce V_k (k non-root)
+  // group: the parent's extract tasks that produce V_k (k non-root); the
+  // parent's own task when the parent is a small front
   std::vector<int> vready(N, -1);
   for (int64_t k = 0; k < N; k++)
     if (P.fronts[k].na > 0) vready[k] = B.new_group();
+  std::vector<int> vtask(N, -1);
+  auto wait_v = [&](int id, int64_t k) {
+    if (vtask[k] >= 0) B.wait_task(id, vtask[k]);
+    else B.wait_group(id, vready[k]);
+  };
 
   const int maxlv = P.nlevels;
   std::vector<int> inv, last_mrow;
@@ -64,6 +71,24 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     const int64_t blk = f.blk, upd = f.upd, M = scrM[k], Y = scrY[k], S = scrS[k];
     auto bw = [&](int c) { return std::min(T, nn - c * T); };
     auto bh = [&](int i) { return std::min(T, na - i * T); };
+
+    // A front that fits one tile is one task: the whole node of
+    // projected_inverse.c:33-73 in shared memory, including the children's
+    // updates, which its children then wait for.
+    if (nj <= T) {
+      Task t = make_task(T_PFRONT);
+      t.m = nj;
+      t.n = nn;
+      t.aux[0] = (int32_t)k;
+      t.a = opnd(B_X, blk, nj);
+      t.c = opnd(B_WS, upd, std::max(na, 1));
+      double est = 4.0 + 0.03 * (double)nj * nj;
+      for (int l = f.chbeg; l < f.chend; l++) est += 0.001 * P.fronts[P.chidx[l]].na * (double)P.fronts[P.chidx[l]].na;
+      int id = B.add(t, {lv, 0, 0, (int)k, 0, 0}, -1, est);
+      if (na > 0) wait_v(id, k);
+      for (int l = f.chbeg; l < f.chend; l++) vtask[P.chidx[l]] = id;
+      continue;
+    }
 
     // M = L^{-1}: diagonal tiles
     inv.assign(NBc, -1);
@@ -143,7 +168,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           Operand c = opnd(B_WS, S + (int64_t)jT * na + iT, na);
           Task t = gemm(bh(i), bw(j), na, -1.0, a, b, 0.0, c);
           SplitTask st = add_split_gemm(B, t, KSPLIT, scratch(t.k, KSPLIT), {lv, 3, 0, (int)k, j, i}, sgroup);
-          for (int id : st.parts) B.wait_group(id, vready[k]);
+          for (int id : st.parts) wait_v(id, k);
         }
       }
       // Y11 -= S21^T W (long K split)

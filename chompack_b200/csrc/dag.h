@@ -141,7 +141,8 @@ struct DagBuilder {
     };
     switch (t.op) {
       case T_NOP: case T_SIGNAL: case T_ARRIVAL: case T_EXTRACT: break;  // an extract writes the workspace
-      case T_FRONT:  // the front's whole nj x nn block (and its update matrix, workspace)
+      case T_FRONT:  // the front's whole nj x nn block (its update matrices are workspace)
+      case T_PFRONT:
         if (t.a.base == B_X && t.a.ld > 0) add_range(t.a.off, t.a.off + (int64_t)t.m * t.n);
         break;
       case T_COPY:

@@ -1251,7 +1251,7 @@ __device__ void run_asm(const RunArgs& ra, const Task& t, double* smem) {
 //   5. the block and the update matrix (operand c) written back.
 // A non-positive pivot records ctl[2] = j + 1 and continues with 1.
 constexpr int FLD = TILE + 1;
-static_assert(TILE * FLD <= ENGINE_SMEM_BASE_DOUBLES, "small front exceeds the engine's shared memory");
+static_assert(2 * TILE * FLD <= ENGINE_SMEM_BASE_DOUBLES, "small fronts exceed the engine's shared memory");
 
 __device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
   const FrontDesc f = ra.fronts[t.aux[0]];
@@ -1304,6 +1304,94 @@ __device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
     for (int r = c + lane; r < nj; r += 32) X[(int64_t)c * nj + r] = F[c * FLD + r];
   for (int q = warp; q < na; q += NW)
     for (int i = q + lane; i < na; i += 32) U[(int64_t)q * ldu + i] = F[(nn + q) * FLD + nn + i];
+}
+
+// A whole small projected-inverse front (T_PFRONT, nj <= TILE;
+// projected_inverse.c:33-73 for one node) in two shared-memory buffers of
+// leading dimension FLD: G holds L11, then M = L11^{-1} (inverted in place,
+// columns last to first, as LAPACK's unblocked triangular inverse does),
+// then S21; F holds the front: W and V_k (operand c) first, then
+// [Y11; S21 | V_k].
+//   Y11 = M^T M;  S21 = -V_k W;  Y11 -= S21^T W;
+//   U_c = F(r_c, r_c) for every child c (lower parts);
+//   the block <- [Y11 (strict upper part zeroed); S21].
+// A zero diagonal entry records ctl[2] = j + 1 and is taken as 1.
+__device__ void run_pfront(const RunArgs& ra, const Task& t, double* smem) {
+  const FrontDesc f = ra.fronts[t.aux[0]];
+  const int nn = f.nn, na = f.na, nj = f.nj;
+  double* G = smem;
+  double* F = smem + TILE * FLD;
+  double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
+  const double* __restrict__ V = ra.bases[t.c.base] + t.c.off;
+  const int ldv = t.c.ld;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = NTHREADS / 32;
+  for (int c = warp; c < nn; c += NW)
+    for (int r = lane; r < nj; r += 32) {
+      const double v = __ldcg(X + (int64_t)c * nj + r);
+      if (r < nn) G[c * FLD + r] = (r >= c) ? v : 0.0;
+      else F[c * FLD + r] = v;
+    }
+  for (int q = warp; q < na; q += NW)
+    for (int i = q + lane; i < na; i += 32) F[(nn + q) * FLD + nn + i] = __ldcg(V + (int64_t)q * ldv + i);
+  __syncthreads();
+  int first_bad = -1;
+  for (int j = nn - 1; j >= 0; j--) {
+    const double d = G[j * FLD + j];
+    if (d == 0.0 && first_bad < 0) first_bad = j;
+    const double ajj = 1.0 / (d == 0.0 ? 1.0 : d);
+    const int i = j + 1 + tid;
+    double ti = 0.0;
+    if (i < nn)
+      for (int l = j + 1; l <= i; l++) ti = fma(G[l * FLD + i], G[j * FLD + l], ti);
+    __syncthreads();
+    if (i < nn) G[j * FLD + i] = -ajj * ti;
+    if (tid == 0) G[j * FLD + j] = ajj;
+    __syncthreads();
+  }
+  if (tid == 0 && first_bad >= 0) atomicCAS(&ra.ctl[2], 0, first_bad + 1);
+  for (int j = warp; j < nn; j += NW)
+    for (int i = j + lane; i < nn; i += 32) {
+      double v = 0.0;
+      for (int l = i; l < nn; l++) v = fma(G[i * FLD + l], G[j * FLD + l], v);
+      F[j * FLD + i] = v;
+    }
+  __syncthreads();
+  if (na > 0) {
+    for (int j = warp; j < nn; j += NW)
+      for (int i = lane; i < na; i += 32) {
+        double v = 0.0;
+        for (int l = 0; l < na; l++) {
+          const double vil = (i >= l) ? F[(nn + l) * FLD + nn + i] : F[(nn + i) * FLD + nn + l];
+          v = fma(vil, F[j * FLD + nn + l], v);
+        }
+        G[j * FLD + i] = -v;
+      }
+    __syncthreads();
+    for (int j = warp; j < nn; j += NW)
+      for (int i = j + lane; i < nn; i += 32) {
+        double v = 0.0;
+        for (int l = 0; l < na; l++) v = fma(G[i * FLD + l], F[j * FLD + nn + l], v);
+        F[j * FLD + i] -= v;
+      }
+    __syncthreads();
+    for (int j = warp; j < nn; j += NW)
+      for (int i = lane; i < na; i += 32) F[j * FLD + nn + i] = G[j * FLD + i];
+    __syncthreads();
+  }
+  for (int l = f.chbeg; l < f.chend; l++) {
+    const FrontDesc ch = ra.fronts[ra.chidx[l]];
+    const int Nc = ch.na;
+    const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
+    double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
+    for (int q = warp; q < Nc; q += NW) {
+      const int col = __ldg(rr + q);
+      for (int i = q + lane; i < Nc; i += 32) Uc[(int64_t)q * Nc + i] = F[col * FLD + __ldg(rr + i)];
+    }
+  }
+  for (int c = warp; c < nn; c += NW)
+    for (int r = lane; r < nj; r += 32)
+      X[(int64_t)c * nj + r] = (r < nn && r < c) ? 0.0 : F[c * FLD + r];
 }
 
 // Gather of a child's update matrix out of its parent's front
@@ -1859,6 +1947,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_POTRF: run_potrf(ra, t, smem, ti); break;
       case T_ASM: run_asm(ra, t, smem); break;
       case T_FRONT: run_front(ra, t, smem); break;
+      case T_PFRONT: run_pfront(ra, t, smem); break;
       case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;

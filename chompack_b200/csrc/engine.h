@@ -79,7 +79,8 @@ enum TaskOp : uint8_t {
   T_SUM = 12,     // C = alpha * sum of aux[0] partial tiles (stride aux[1]) + beta * C
   T_SIGNAL = 13,  // host-visible flag io_out[aux[0]] = 1 (a chunk of the values is final)
   T_ARRIVAL = 14, // waits (bounded) until the host's copy raised io_in[aux[0]] (a chunk arrived)
-  T_FRONT = 15    // a whole small cholesky front (nj <= TILE) in shared memory (front aux[0])
+  T_FRONT = 15,   // a whole small cholesky front (nj <= TILE) in shared memory (front aux[0])
+  T_PFRONT = 16   // a whole small projected-inverse front (nj <= TILE) in shared memory (front aux[0])
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the

@@ -31,7 +31,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
-T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL, T_FRONT = 8, 9, 10, 11, 12, 13, 14, 15
+T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL, T_FRONT, T_PFRONT = 8, 9, 10, 11, 12, 13, 14, 15, 16
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -190,6 +190,8 @@ class VM(object):
             self._asm(t)
         elif op == T_FRONT:
             self._front(t)
+        elif op == T_PFRONT:
+            self._pfront(t)
         elif op == T_EXTRACT:
             self._extract(t)
         elif op == T_VEC:
@@ -316,6 +318,48 @@ class VM(object):
             ci = np.arange(na)[None, :]
             lw = ri >= ci
             Ub[(Uof + ci * ldu + ri)[lw]] = U[lw]
+
+    def _pfront(self, t):
+        """A whole small projected-inverse front: M = L11^{-1}, Y11 = M^T M,
+        S21 = -V W, Y11 -= S21^T W, the children's updates extracted from
+        the front [Y11, S21^T; S21, V], the block written back as [Y11
+        (strict upper part zeroed); S21]."""
+        f = self.p.fronts[int(t["aux"][0])]
+        nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
+        WS = self.bases[B_WS]
+        X, off = self.bases[int(t["a"]["base"])], int(t["a"]["off"])
+        r = np.arange(nj)[:, None]
+        c = np.arange(nn)[None, :]
+        blk = X[off + c * nj + r]
+        L11 = np.tril(blk[:nn])
+        if np.any(np.diag(L11) == 0.0) and self.info == 0:
+            self.info = 1
+        M = np.linalg.inv(L11)
+        Y11 = M.T @ M
+        F = np.zeros((nj, nj))
+        if na > 0:
+            Ub, Uof, ldu = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
+            ri = np.arange(na)[:, None]
+            ci = np.arange(na)[None, :]
+            Vl = np.where(ri >= ci, Ub[Uof + ci * ldu + ri], 0.0)
+            V = Vl + np.tril(Vl, -1).T
+            W = blk[nn:]
+            S = -V @ W
+            Y11 = Y11 - S.T @ W
+            F[nn:, :nn] = S
+            F[nn:, nn:] = V
+        F[:nn, :nn] = Y11
+        for l in range(int(f["chbeg"]), int(f["chend"])):
+            ch = self.p.fronts[self.chidx[l]]
+            Nc = int(ch["na"])
+            rr = np.asarray(self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc], dtype=np.int64)
+            q = np.arange(Nc)[None, :]
+            i = np.arange(Nc)[:, None]
+            low = i >= q
+            vals = F[rr[:, None], rr[None, :]]
+            WS[(int(ch["upd"]) + q * Nc + i)[low]] = vals[low]
+        out = np.vstack([np.where(r[:nn] >= c, Y11, 0.0), F[nn:, :nn]])
+        X[off + c * nj + r] = out
 
     def _vec(self, t):
         mode, nrhs = int(t["aux"][0]), int(t["n"])

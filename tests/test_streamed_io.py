@@ -64,7 +64,7 @@ def _written_ranges(t):
         return []
     if op in (taskvm.T_NOP, taskvm.T_SIGNAL, taskvm.T_ARRIVAL, taskvm.T_EXTRACT):
         return []
-    if op == taskvm.T_FRONT:
+    if op in (taskvm.T_FRONT, taskvm.T_PFRONT):
         o = t["a"]
         return [(int(o["off"]), int(o["off"]) + int(t["m"]) * int(t["n"]))] if int(o["base"]) == 0 else []
     if op == taskvm.T_COPY and int(t["aux"][0]) & 24 == 0:

@@ -1,8 +1,9 @@
 """Task programs of problems whose fronts span several 64-column blocks, on
 the CPU: the fused diagonal task of cholesky (factor the diagonal tile, then
 wait mid task for the next tiles' updates and do the look-ahead) and the
-separate look-ahead task it replaces, executed by the task interpreter in
-random orders allowed by the waits and under the dynamic release rules,
+separate look-ahead task it replaces, and projected_inverse with small
+fronts (one task each) next to tiled ones, executed by the task interpreter
+in random orders allowed by the waits and under the dynamic release rules,
 against the oracle's C restatement of the reference's sweeps."""
 import os
 
@@ -72,3 +73,24 @@ def test_fused_task_waits():
             seen_mid += 1
         assert int(t["aux"][3]) > 0     # the early signal of the next panel tile
     assert seen_mid > 0
+
+
+@pytest.mark.parametrize("kind,args,merge", CASES)
+@pytest.mark.parametrize("order,seed", [("random", 3), ("dynamic", 4)])
+def test_wide_front_projected_inverse(kind, args, merge, order, seed):
+    A, s = problem(kind, *args, merge=merge, seed=3)
+    pl = Plan(s, device=-1)
+    prog = taskvm.Program(pl.handle, N.OP_PROJECTED_INVERSE, nsn=s.Nsn)
+    sch = taskvm.Schedule(pl.handle, N.OP_PROJECTED_INVERSE)
+    nj = np.diff(np.asarray(s.sncolptr))
+    small = int(np.sum(prog.tasks["op"] == taskvm.T_PFRONT))
+    assert small == int(np.sum(nj <= 64))
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    L = x0.copy()
+    assert oracle.cholesky(s, L) == 0
+    ref = L.copy()
+    assert oracle.projected_inverse(s, ref) == 0
+    y = L.copy()
+    bases = {0: y, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, y, ref)
