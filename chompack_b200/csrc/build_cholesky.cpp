@@ -23,6 +23,7 @@ namespace chb {
 
 int build_cholesky(const chb_plan& P, Program& prog) {
   const int T = TILE;
+  const int small_nj = small_front_nj();
   const int CH = 64;  // at most this many front columns per extend-add task
   const int64_t N = P.nsn;
   DagBuilder B;
@@ -33,7 +34,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int NBc = ceil_div(f.nn, T);
-    if (f.nj <= T) continue;  // a small front needs no scratch (one shared-memory task)
+    if (f.nj <= small_nj) continue;  // a small front needs no scratch (one shared-memory task)
     if (f.na > 0) {
       scrS[k] = ws;
       ws += (int64_t)f.na * f.nn;
@@ -79,7 +80,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
 
     // A front that fits one tile is one task: extend-add, partial Cholesky
     // and Schur complement in shared memory (cholesky.c:33-72 for one node).
-    if (nj <= T) {
+    if (nj <= small_nj) {
       Task t = make_task(T_FRONT);
       t.m = nj;
       t.n = nn;

@@ -22,6 +22,7 @@ namespace chb {
 
 int build_projected_inverse(const chb_plan& P, Program& prog) {
   const int T = TILE;
+  const int small_nj = small_front_nj();
   const int CH = 16;  // child columns per extract task
   const int64_t N = P.nsn;
   DagBuilder B;
@@ -30,7 +31,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
   std::vector<int64_t> scrM(N), scrY(N), scrS(N, -1);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
-    if (f.nj <= T) continue;  // a small front needs no scratch (one shared-memory task)
+    if (f.nj <= small_nj) continue;  // a small front needs no scratch (one shared-memory task)
     scrM[k] = ws;
     ws += (int64_t)f.nn * f.nn;
     scrY[k] = ws;
@@ -75,7 +76,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     // A front that fits one tile is one task: the whole node of
     // projected_inverse.c:33-73 in shared memory, including the children's
     // updates, which its children then wait for.
-    if (nj <= T) {
+    if (nj <= small_nj) {
       Task t = make_task(T_PFRONT);
       t.m = nj;
       t.n = nn;

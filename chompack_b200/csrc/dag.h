@@ -7,6 +7,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <queue>
@@ -523,6 +524,16 @@ struct DagBuilder {
     return 0;
   }
 };
+
+// Largest front order (nj) that a sweep runs as one shared-memory task
+// (cholesky, projected_inverse): TILE, or CHB_SMALL_FRONT_NJ when set
+// (0 turns the small-front tasks off).
+inline int small_front_nj() {
+  const char* e = std::getenv("CHB_SMALL_FRONT_NJ");
+  if (!e) return TILE;
+  const int v = std::atoi(e);
+  return v < 0 ? 0 : (v > TILE ? TILE : v);
+}
 
 // An operand advanced by k0 along its K dimension.
 inline Operand shift_k(Operand o, int k0) {
