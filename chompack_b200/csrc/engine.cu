@@ -808,15 +808,23 @@ __device__ void run_mrow(const RunArgs& ra, const Task& t, const SmemLayout& sm)
 // The tile is padded to 64 x 64 with an identity block (which factors and
 // inverts to itself and does not couple to the leading b x b part), then
 // processed in four 16-column blocks J:
-//   (a) warp 0 factors the 16x16 diagonal block in registers (lane i holds
-//       row i, right-looking, pivots and multipliers broadcast by shuffles)
-//       and inverts it (lane c holds column c of Minv_JJ);
+//   (a) the 16x16 diagonal block is factored in registers (lane i holds
+//       row i, right-looking) and inverted (lane c holds column c of
+//       Minv_JJ);
 //   (b) panel below: L(r, J) = A(r, J) Minv_JJ^T            (DMMA)
 //   (c) trailing lower triangle: A(r, c) -= L(r, J) L(c, J)^T (DMMA)
-// then the inverse of the whole tile block row by block row:
+// and the inverse of the whole tile block row by block row:
 //   M(I, :I) = -Minv_II (L(I, :I) M(:I, :I))                (DMMA)
+// Warp 0 carries the dependent chain: in step J it computes the panel rows
+// of block J (from block J-1), updates the diagonal block J, factors and
+// inverts it.  Warps 1-3 meanwhile compute the other panel rows, update the
+// trailing rows below block J (after a named barrier on warp 0's panel
+// rows) and assemble block row J-1 of the inverse.  One block-wide barrier
+// per step; only block row 3 of the inverse follows the last step.
 constexpr int POTRF_LD = TILE + 1;
-constexpr int POTRF_SMEM_DOUBLES = 2 * TILE * POTRF_LD + TILE + 16 * TILE;
+// sL, sM, 1 / L(j, j), the pivot-column broadcast (2 x 16), per-warp 16 x 8
+// staging of the inverse assembly (16 x 64 in all)
+constexpr int POTRF_SMEM_DOUBLES = 2 * TILE * POTRF_LD + TILE + 32 + 16 * TILE;
 
 // Phase timing for development builds (-DCHB_PROFILE_POTRF); compiled out
 // otherwise.
@@ -846,6 +854,131 @@ __device__ __forceinline__ void warp_mma_16x8(double (&acc)[4], const double* pa
     const double a1 = sgn * pa[g + 8 + (k + q) * lda];
     const double b0 = pb[(k + q) * ksb + g * nsb];
     dmma16(acc, a0, a1, b0);
+  }
+}
+
+// Named barriers (id 0 is __syncthreads): bar.arrive publishes the
+// caller's shared-memory writes to the threads that bar.sync on the id.
+__device__ __forceinline__ void named_bar_arrive(int id, int nthreads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Panel rows [r0, r0 + 16) of the 16-column block at jp, in place:
+// L(r, jp + n) = sum_k A(r, jp + k) Minv(n, k), both 16x8 halves by the
+// calling warp (sL, sM: [col][row], leading dimension POTRF_LD).
+__device__ __forceinline__ void potrf_panel_rows(double* sL, const double* sM, int jp, int r0) {
+  constexpr int LD = POTRF_LD;
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  double a0[4] = {0.0, 0.0, 0.0, 0.0}, a1[4] = {0.0, 0.0, 0.0, 0.0};
+  warp_mma_16x8(a0, sL + jp * LD + r0, LD, sM + jp * LD + jp, LD, 1, 16, false);
+  warp_mma_16x8(a1, sL + jp * LD + r0, LD, sM + jp * LD + jp + 8, LD, 1, 16, false);
+  __syncwarp();
+  const int r = r0 + g, c0 = jp + 2 * q, c1 = c0 + 8;
+  sL[c0 * LD + r] = a0[0];
+  sL[(c0 + 1) * LD + r] = a0[1];
+  sL[c0 * LD + r + 8] = a0[2];
+  sL[(c0 + 1) * LD + r + 8] = a0[3];
+  sL[c1 * LD + r] = a1[0];
+  sL[(c1 + 1) * LD + r] = a1[1];
+  sL[c1 * LD + r + 8] = a1[2];
+  sL[(c1 + 1) * LD + r + 8] = a1[3];
+  __syncwarp();
+}
+
+// Lower-triangle part of the 16x8 tile at (r0, c0) minus the rank-16
+// product of the panel block at jp: A(r, c) -= sum_k L(r, jp + k) L(c, jp + k).
+__device__ __forceinline__ void potrf_syrk_tile(double* sL, int jp, int r0, int c0) {
+  constexpr int LD = POTRF_LD;
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int r = r0 + g, c = c0 + 2 * q;
+  double ac[4] = {sL[c * LD + r], sL[(c + 1) * LD + r], sL[c * LD + r + 8], sL[(c + 1) * LD + r + 8]};
+  warp_mma_16x8(ac, sL + jp * LD + r0, LD, sL + jp * LD + c0, LD, 1, 16, true);
+  if (r >= c) sL[c * LD + r] = ac[0];
+  if (r >= c + 1) sL[(c + 1) * LD + r] = ac[1];
+  if (r + 8 >= c) sL[c * LD + r + 8] = ac[2];
+  if (r + 8 >= c + 1) sL[(c + 1) * LD + r + 8] = ac[3];
+}
+
+// Block row I of the inverse, column tiles tj = first, first + stride, ...
+// of 8 columns: T = L(I, :I) M(:I, :I) (K = 16 I) staged in the warp's own
+// 16x8 area sTw, then M(I, tile) = -Minv_II T.
+__device__ __forceinline__ void potrf_inv_row(const double* sL, double* sM, double* sTw, int I, int first,
+                                              int stride) {
+  constexpr int LD = POTRF_LD;
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int i0 = 16 * I, ntj = i0 / 8;
+  for (int tj = first; tj < ntj; tj += stride) {
+    double ac[4] = {0.0, 0.0, 0.0, 0.0};
+    warp_mma_16x8(ac, sL + i0, LD, sM + (8 * tj) * LD, 1, LD, i0, false);
+    const int c = 2 * q;
+    sTw[g + 16 * c] = ac[0];
+    sTw[g + 16 * (c + 1)] = ac[1];
+    sTw[g + 8 + 16 * c] = ac[2];
+    sTw[g + 8 + 16 * (c + 1)] = ac[3];
+    __syncwarp();
+    double am[4] = {0.0, 0.0, 0.0, 0.0};
+    warp_mma_16x8(am, sM + i0 * LD + i0, LD, sTw, 1, 16, 16, true);
+    __syncwarp();
+    const int c0 = 8 * tj + 2 * q, r0 = i0 + g;
+    sM[c0 * LD + r0] = am[0];
+    sM[(c0 + 1) * LD + r0] = am[1];
+    sM[c0 * LD + r0 + 8] = am[2];
+    sM[(c0 + 1) * LD + r0 + 8] = am[3];
+  }
+}
+
+// acc[j] += A(16w : 16w + 16, :) B(8j : 8j + 8, :)^T for the calling warp w
+// (rows of the 64x64 product by 16-row block, all eight 8-column tiles),
+// A(r, k) at sA[k * POTRF_LD + r], B(c, k) at sB[k * POTRF_LD + c], B lower
+// triangular: tile j takes only k < 8 (j + 1), so every warp issues 72 of
+// the 128 MMAs of a full 64-deep product.
+__device__ __forceinline__ void mma_rows_lower_b(const double* sA, const double* sB, double (&acc)[8][4]) {
+  constexpr int LD = POTRF_LD;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+  const int r0 = 16 * warp + g;
+#pragma unroll 1
+  for (int kb = 0; kb < TILE / 8; kb++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int k = 8 * kb + 4 * h + q;
+      const double a0 = sA[k * LD + r0], a1 = sA[k * LD + r0 + 8];
+#pragma unroll
+      for (int j = 0; j < TILE / 8; j++)
+        if (j >= kb) dmma16(acc[j], a0, a1, sB[k * LD + 8 * j + g]);
+    }
+  }
+}
+
+// The 20 16x8 tiles on or below the diagonal of a 64x64 product, five per
+// warp: tile t lies in 16-row block rb and 8-column block j, listed by row
+// block 3, 2, 1, 0 (8, 6, 4 and 2 tiles).
+__device__ __forceinline__ void lower_tile(int t, int& rb, int& j) {
+  rb = t < 8 ? 3 : (t < 14 ? 2 : (t < 18 ? 1 : 0));
+  j = t - (t < 8 ? 0 : (t < 14 ? 8 : (t < 18 ? 14 : 18)));
+}
+
+// acc[i] += A(rows of tile i) A(columns of tile i)^T over k < kn for the
+// calling warp's five lower tiles (tile 5 w + i), A(r, k) at
+// sA[k * POTRF_LD + r]: 80 MMAs per warp instead of 128 for the full square.
+__device__ __forceinline__ void mma_lower_tiles(const double* sA, int kn, double (&acc)[5][4]) {
+  constexpr int LD = POTRF_LD;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+  int ro[5], co[5];
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    int rb, j;
+    lower_tile(5 * warp + i, rb, j);
+    ro[i] = 16 * rb + g;
+    co[i] = 8 * j + g;
+  }
+#pragma unroll 4
+  for (int kk = 0; kk < kn; kk += 4) {
+    const double* ak = sA + (kk + q) * LD;
+#pragma unroll
+    for (int i = 0; i < 5; i++) dmma16(acc[i], ak[ro[i]], ak[ro[i] + 8], ak[co[i]]);
   }
 }
 
@@ -908,23 +1041,24 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
     }
   }
   __syncthreads();
-  Acc acc;
-  zero_acc(acc);
-  mma_block_ld<LD, LD>(sL, sM, b, acc);
-  __syncthreads();
-  // L' into sL and in place
+  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+  {
+    double acc[TILE / 8][4];
 #pragma unroll
-  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < TILE / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+    mma_rows_lower_b(sL, sM, acc);  // b = TILE: only the last block column of a front has b < TILE
+    __syncthreads();
+    // L' into sL and in place
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+    for (int j = 0; j < TILE / 8; j++)
 #pragma unroll
       for (int h = 0; h < 4; h++) {
-        int r, c;
-        acc_coord(i, j, h, r, c);
-        const double v = (r < m2) ? acc[i][j][h] : 0.0;
+        const int r = 16 * warp + g + ((h & 2) ? 8 : 0), c = 8 * j + 2 * q + (h & 1);
+        const double v = (r < m2) ? acc[j][h] : 0.0;
         sL[c * LD + r] = v;
         if (r < m2 && c < b) P[(int64_t)c * lda + r] = v;
       }
+  }
   __syncthreads();
   if (t.aux[3] > 0) {
     if (ra.dynamic) {
@@ -935,9 +1069,32 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
       red_release_add(ra.counters + (t.aux[3] - 1), 1);
     }
   }
-  zero_acc(acc);
-  mma_block_ld<LD, LD>(sL, sL, b, acc);
-  store_acc(D, lda, m2, m2, true, 0, -1.0, 1.0, acc);
+  // D -= L' L'^T on and below the diagonal
+  double acc[5][4];
+#pragma unroll
+  for (int i = 0; i < 5; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
+  mma_lower_tiles(sL, b, acc);
+  double old[5][4];
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    int rb, j;
+    lower_tile(5 * warp + i, rb, j);
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int r = 16 * rb + g + ((h & 2) ? 8 : 0), c = 8 * j + 2 * q + (h & 1);
+      old[i][h] = (r < m2 && r >= c) ? __ldcg(D + (int64_t)c * lda + r) : 0.0;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    int rb, j;
+    lower_tile(5 * warp + i, rb, j);
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int r = 16 * rb + g + ((h & 2) ? 8 : 0), c = 8 * j + 2 * q + (h & 1);
+      if (r < m2 && r >= c) D[(int64_t)c * lda + r] = old[i][h] - acc[i][h];
+    }
+  }
 }
 
 __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti) {
@@ -946,7 +1103,8 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   double* sL = smem;               // [col][row], lower; upper part zero
   double* sM = sL + TILE * LD;     // inverse, upper part zero
   double* rdiag = sM + TILE * LD;  // 1 / L(j,j)
-  double* sT = rdiag + TILE;       // [16 x 64] scratch, T(r, c) at sT[r + 16 c]
+  double* colb = rdiag + TILE;     // pivot-column broadcast, 2 x 16
+  double* sT = colb + 32;          // per-warp 16 x 8 staging (warp w at 128 w)
   double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
   const int lda = t.a.ld;
   const int info_base = t.aux[0];
@@ -978,132 +1136,111 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   POTRF_STAMP(0);
 #pragma unroll 1
   for (int J = 0; J < 4; J++) {
-    const int j0 = 16 * J, j1 = j0 + 16;
-    if (warp == 0 && !factor) {
-      // invert-only: reciprocals of the diagonal (a zero pivot is singular)
-      const int il = lane & 15;
-      const double d = sL[(j0 + il) * LD + j0 + il];
-      if (lane < 16) {
-        if (d == 0.0 && j0 + il < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + il + 1);
-        rdiag[j0 + il] = 1.0 / (d == 0.0 ? 1.0 : d);
-      }
-      __syncwarp();
-    }
+    const int j0 = 16 * J, j1 = j0 + 16, jp = j0 - 16;
+    const bool panel = factor && J > 0;  // panel of block J-1 and the updates it feeds
+    const bool below = panel && J < 3;   // rows below block J to update
     if (warp == 0) {
-      // (a) factor the 16x16 diagonal block in registers: lane i < 16 row i
-      const int il = lane & 15;
-      if (factor) {
-      double a[16];
-#pragma unroll
-      for (int c = 0; c < 16; c++) a[c] = sL[(j0 + c) * LD + j0 + il];
-      // The pivot column goes to the other lanes through shared memory (one
-      // store per lane, then broadcast loads): fifteen double shuffles per
-      // pivot are throughput-bound and cost 2.5x more on this part.
-      // The next pivot, a(jj+1, jj+1) - l(jj+1, jj)^2, is formed by lane
-      // jj+1 from its own values right after its multiplier, so the chain
-      // from pivot to pivot is shuffle -> rsqrt -> multiply -> FMA and the
-      // broadcast and the other updates run beside it.
-      double* colb = sT;  // free until the inverse assembly: 2 x 16 doubles
-      double dn = a[0];
-      int first_bad = -1;  // first non-positive pivot, reported once after the loop
-#pragma unroll
-      for (int jj = 0; jj < 16; jj++) {
-        const double d = __shfl_sync(0xffffffffu, dn, jj);
-        const bool bad = !(d > 0.0);
-        first_bad = (bad && first_bad < 0) ? jj : first_bad;
-        const double x = bad ? 1.0 : d;
-        const double rs = rsqrt(x);
-        const double l = (il == jj) ? x * rs : a[jj] * rs;
-        a[jj] = (il >= jj) ? l : a[jj];
-        if (jj + 1 < 16) dn = fma(-l, l, a[jj + 1]);
-        if (lane == jj) rdiag[j0 + jj] = rs;
-        if (lane < 16) colb[16 * (jj & 1) + il] = l;
+      if (panel) {
+        potrf_panel_rows(sL, sM, jp, j0);
+        if (below) named_bar_arrive(1, NTHREADS);
+        potrf_syrk_tile(sL, jp, j0, j0);
+        potrf_syrk_tile(sL, jp, j0, j0 + 8);
         __syncwarp();
+      }
+      if (!factor) {
+        // invert-only: reciprocals of the diagonal (a zero pivot is singular)
+        const int il = lane & 15;
+        const double d = sL[(j0 + il) * LD + j0 + il];
+        if (lane < 16) {
+          if (d == 0.0 && j0 + il < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + il + 1);
+          rdiag[j0 + il] = 1.0 / (d == 0.0 ? 1.0 : d);
+        }
+        __syncwarp();
+      }
+      {
+        // (a) factor the 16x16 diagonal block in registers: lane i < 16 row i
+        const int il = lane & 15;
+        if (factor) {
+        double a[16];
 #pragma unroll
-        for (int kk = jj + 1; kk < 16; kk++) {
-          const double lkj = colb[16 * (jj & 1) + kk];
-          if (il >= kk) a[kk] = fma(-l, lkj, a[kk]);
+        for (int c = 0; c < 16; c++) a[c] = sL[(j0 + c) * LD + j0 + il];
+        // The pivot column goes to the other lanes through shared memory (one
+        // store per lane, then broadcast loads): fifteen double shuffles per
+        // pivot are throughput-bound and cost 2.5x more on this part.
+        // The next pivot, a(jj+1, jj+1) - l(jj+1, jj)^2, is formed by lane
+        // jj+1 from its own values right after its multiplier, so the chain
+        // from pivot to pivot is shuffle -> rsqrt -> multiply -> FMA and the
+        // broadcast and the other updates run beside it.
+        double dn = a[0];
+        int first_bad = -1;  // first non-positive pivot, reported once after the loop
+#pragma unroll
+        for (int jj = 0; jj < 16; jj++) {
+          const double d = __shfl_sync(0xffffffffu, dn, jj);
+          const bool bad = !(d > 0.0);
+          first_bad = (bad && first_bad < 0) ? jj : first_bad;
+          const double x = bad ? 1.0 : d;
+          const double rs = rsqrt(x);
+          const double l = (il == jj) ? x * rs : a[jj] * rs;
+          a[jj] = (il >= jj) ? l : a[jj];
+          if (jj + 1 < 16) dn = fma(-l, l, a[jj + 1]);
+          if (lane == jj) rdiag[j0 + jj] = rs;
+          if (lane < 16) colb[16 * (jj & 1) + il] = l;
+          __syncwarp();
+#pragma unroll
+          for (int kk = jj + 1; kk < 16; kk++) {
+            const double lkj = colb[16 * (jj & 1) + kk];
+            if (il >= kk) a[kk] = fma(-l, lkj, a[kk]);
+          }
+        }
+        if (lane == 0 && first_bad >= 0 && j0 + first_bad < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + first_bad + 1);
+        if (lane < 16) {
+#pragma unroll
+          for (int c = 0; c < 16; c++)
+            if (c <= il) sL[(j0 + c) * LD + j0 + il] = a[c];
+        }
+        }
+        __syncwarp();
+        POTRF_STAMP(1);
+        // inverse of the block: lane c < 16 holds column c,
+        // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c),
+        // right-looking: as soon as M(l, c) is known it is added into the
+        // partial sums of all later rows, so the dependent chain per row is
+        // one multiply and one FMA (FP64 latency, not the row's dot product)
+        double m[16], sacc[16];
+#pragma unroll
+        for (int r = 0; r < 16; r++) sacc[r] = 0.0;
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+          const double rd = rdiag[j0 + l];
+          m[l] = (l == il) ? rd : ((l > il) ? -rd * sacc[l] : 0.0);
+#pragma unroll
+          for (int r = l + 1; r < 16; r++) sacc[r] = fma(sL[(j0 + l) * LD + j0 + r], m[l], sacc[r]);
+        }
+        if (lane < 16) {
+#pragma unroll
+          for (int r = 0; r < 16; r++)
+            if (r >= il) sM[(j0 + il) * LD + j0 + r] = m[r];
+        }
+        POTRF_STAMP(2);
+      }
+    } else {
+      if (below) {
+        const int rb = j0 + 16 * warp;  // warps 1, 2: the panel rows below block J
+        if (rb < TILE) potrf_panel_rows(sL, sM, jp, rb);
+        named_bar_sync(1, NTHREADS);
+        // rows >= j1, columns >= j0, lower part, from the panel of block J-1
+        const int nti = (TILE - j1) / 16, ntj = (TILE - j0) / 8;
+        for (int tt = warp - 1; tt < nti * ntj; tt += NTHREADS / 32 - 1) {
+          const int r0 = j1 + 16 * (tt / ntj), c0 = j0 + 8 * (tt % ntj);
+          if (c0 <= r0 + 15) potrf_syrk_tile(sL, jp, r0, c0);
         }
       }
-      if (lane == 0 && first_bad >= 0 && j0 + first_bad < b) atomicCAS(&ra.ctl[2], 0, info_base + j0 + first_bad + 1);
-      if (lane < 16) {
-#pragma unroll
-        for (int c = 0; c < 16; c++)
-          if (c <= il) sL[(j0 + c) * LD + j0 + il] = a[c];
-      }
-      }
-      __syncwarp();
-      POTRF_STAMP(1);
-      // inverse of the block: lane c < 16 holds column c,
-      // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c),
-      // right-looking: as soon as M(l, c) is known it is added into the
-      // partial sums of all later rows, so the dependent chain per row is
-      // one multiply and one FMA (FP64 latency, not the row's dot product)
-      double m[16], sacc[16];
-#pragma unroll
-      for (int r = 0; r < 16; r++) sacc[r] = 0.0;
-#pragma unroll
-      for (int l = 0; l < 16; l++) {
-        const double rd = rdiag[j0 + l];
-        m[l] = (l == il) ? rd : ((l > il) ? -rd * sacc[l] : 0.0);
-#pragma unroll
-        for (int r = l + 1; r < 16; r++) sacc[r] = fma(sL[(j0 + l) * LD + j0 + r], m[l], sacc[r]);
-      }
-      if (lane < 16) {
-#pragma unroll
-        for (int r = 0; r < 16; r++)
-          if (r >= il) sM[(j0 + il) * LD + j0 + r] = m[r];
-      }
-      POTRF_STAMP(2);
+      if (want_inv && J >= 2) potrf_inv_row(sL, sM, sT + 128 * warp, J - 1, warp - 1, NTHREADS / 32 - 1);
     }
     __syncthreads();
     POTRF_STAMP(3);
-    const int prow = TILE - j1;  // rows below the block: 48, 32, 16, 0
-    if (factor && prow > 0) {
-      // (b) panel: X(r, n) = sum_k A(r, k) Minv(n, k), 16x8 tiles; at most
-      // six tiles, so warp w owns tiles w and w + 4
-      const int ntiles = (prow / 16) * 2;
-      double acc0[4] = {0.0, 0.0, 0.0, 0.0}, acc1[4] = {0.0, 0.0, 0.0, 0.0};
-      const int t0 = warp, t1 = warp + NTHREADS / 32;
-      if (t0 < ntiles)
-        warp_mma_16x8(acc0, sL + j0 * LD + j1 + 16 * (t0 >> 1), LD, sM + j0 * LD + j0 + 8 * (t0 & 1), LD, 1, 16,
-                      false);
-      if (t1 < ntiles)
-        warp_mma_16x8(acc1, sL + j0 * LD + j1 + 16 * (t1 >> 1), LD, sM + j0 * LD + j0 + 8 * (t1 & 1), LD, 1, 16,
-                      false);
-      __syncthreads();
-      if (t0 < ntiles) {
-        const int r0 = j1 + 16 * (t0 >> 1) + g, c0 = j0 + 8 * (t0 & 1) + 2 * q;
-        sL[c0 * LD + r0] = acc0[0];
-        sL[(c0 + 1) * LD + r0] = acc0[1];
-        sL[c0 * LD + r0 + 8] = acc0[2];
-        sL[(c0 + 1) * LD + r0 + 8] = acc0[3];
-      }
-      if (t1 < ntiles) {
-        const int r0 = j1 + 16 * (t1 >> 1) + g, c0 = j0 + 8 * (t1 & 1) + 2 * q;
-        sL[c0 * LD + r0] = acc1[0];
-        sL[(c0 + 1) * LD + r0] = acc1[1];
-        sL[c0 * LD + r0 + 8] = acc1[2];
-        sL[(c0 + 1) * LD + r0 + 8] = acc1[3];
-      }
-      __syncthreads();
-      // (c) trailing: C(r, c) -= sum_k L(r, k) L(c, k) on the lower triangle
-      const int nti = prow / 16, ntj = prow / 8;
-      for (int tt = warp; tt < nti * ntj; tt += NTHREADS / 32) {
-        const int ti = tt / ntj, tj = tt % ntj;
-        if (8 * tj > 16 * ti + 15) continue;  // tile entirely above the diagonal
-        const int r0 = j1 + 16 * ti + g, c0 = j1 + 8 * tj + 2 * q;
-        double ac[4] = {sL[c0 * LD + r0], sL[(c0 + 1) * LD + r0], sL[c0 * LD + r0 + 8], sL[(c0 + 1) * LD + r0 + 8]};
-        warp_mma_16x8(ac, sL + j0 * LD + j1 + 16 * ti, LD, sL + j0 * LD + j1 + 8 * tj, LD, 1, 16, true);
-        if (r0 >= c0) sL[c0 * LD + r0] = ac[0];
-        if (r0 >= c0 + 1) sL[(c0 + 1) * LD + r0] = ac[1];
-        if (r0 + 8 >= c0) sL[c0 * LD + r0 + 8] = ac[2];
-        if (r0 + 8 >= c0 + 1) sL[(c0 + 1) * LD + r0 + 8] = ac[3];
-      }
-      __syncthreads();
-    }
-    POTRF_STAMP(4);
   }
+  POTRF_STAMP(4);
   if (factor) {
 #pragma unroll 8
     for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
@@ -1114,34 +1251,9 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   }
   POTRF_STAMP(5);
   if (!want_inv) return;
-  // full inverse, block row by block row (M's diagonal blocks are in place)
-#pragma unroll 1
-  for (int I = 1; I < 4; I++) {
-    const int i0 = 16 * I;
-    const int ntj = i0 / 8;
-    // T(r, c) = sum_{l < i0} L(i0 + r, l) M(l, c), c < i0
-    for (int tj = warp; tj < ntj; tj += NTHREADS / 32) {
-      double ac[4] = {0.0, 0.0, 0.0, 0.0};
-      warp_mma_16x8(ac, sL + i0, LD, sM + (8 * tj) * LD, 1, LD, i0, false);
-      const int c0 = 8 * tj + 2 * q;
-      sT[g + 16 * c0] = ac[0];
-      sT[g + 16 * (c0 + 1)] = ac[1];
-      sT[g + 8 + 16 * c0] = ac[2];
-      sT[g + 8 + 16 * (c0 + 1)] = ac[3];
-    }
-    __syncthreads();
-    // M(i0 + r, c) = -sum_k Minv_II(r, k) T(k, c)
-    for (int tj = warp; tj < ntj; tj += NTHREADS / 32) {
-      double ac[4] = {0.0, 0.0, 0.0, 0.0};
-      warp_mma_16x8(ac, sM + i0 * LD + i0, LD, sT + 16 * (8 * tj), 1, 16, 16, true);
-      const int c0 = 8 * tj + 2 * q, r0 = i0 + g;
-      sM[c0 * LD + r0] = ac[0];
-      sM[(c0 + 1) * LD + r0] = ac[1];
-      sM[c0 * LD + r0 + 8] = ac[2];
-      sM[(c0 + 1) * LD + r0 + 8] = ac[3];
-    }
-    __syncthreads();
-  }
+  // the last block row of the inverse (rows 1 and 2 were assembled above)
+  potrf_inv_row(sL, sM, sT + 128 * warp, 3, warp, NTHREADS / 32);
+  __syncthreads();
   POTRF_STAMP(6);
 #pragma unroll 8
   for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
