@@ -42,7 +42,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     }
   }
   // split-K scratch, handed out as the long-K tiles are built
-  const int KSPLIT = 384;
+  const int KSPLIT = pinv_ksplit();
   auto scratch = [&ws](int K, int kc) {
     const int p = split_count(K, kc);
     if (p == 1) return (int64_t)0;

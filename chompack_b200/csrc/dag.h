@@ -525,6 +525,16 @@ struct DagBuilder {
   }
 };
 
+// Largest K of one partial product of projected_inverse's long-K tiles
+// (CHB_PINV_KSPLIT, rounded down to a multiple of TILE, at least 2 TILE;
+// default 768: at 40^3 the sweep is bound by the CTAs' total work, and
+// 384 / 768 / 1536 gave 6.01 / 5.76 / 6.09 ms).
+inline int pinv_ksplit() {
+  const char* e = std::getenv("CHB_PINV_KSPLIT");
+  const int v = e ? (std::atoi(e) / TILE) * TILE : 768;
+  return v < 2 * TILE ? 2 * TILE : v;
+}
+
 // Largest front order (nj) that a sweep runs as one shared-memory task
 // (cholesky, projected_inverse): TILE, or CHB_SMALL_FRONT_NJ when set
 // (0 turns the small-front tasks off).
