@@ -30,7 +30,8 @@ int build_cholesky(const chb_plan& P, Program& prog) {
 
   // workspace: update matrices first (shared layout), then per-front scratch
   int64_t ws = P.upd_total;
-  std::vector<int64_t> scrS(N, -1), scrM(N, -1);
+  const int kc = chol_ksplit();
+  std::vector<int64_t> scrS(N, -1), scrM(N, -1), scrK(N, -1);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int NBc = ceil_div(f.nn, T);
@@ -42,6 +43,12 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     if (NBc > 1 || f.na > 0) {
       scrM[k] = ws;
       ws += (int64_t)f.nn * f.nn;
+    }
+    if (f.na > 0 && kc > 0 && split_count(f.nn, kc) > 1) {
+      // partial products of the split Schur-complement tiles
+      const int64_t NBb = ceil_div(f.na, T);
+      scrK[k] = ws;
+      ws += NBb * (NBb + 1) / 2 * split_count(f.nn, kc) * (int64_t)T * T;
     }
   }
   prog.ws_doubles = ws;
@@ -273,16 +280,29 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       }
     }
     if (na == 0) continue;
-    // Schur complement U_k -= S_k S_k^T (cholesky.c:64-69)
+    // Schur complement U_k -= S_k S_k^T (cholesky.c:64-69); with a split
+    // K the partial products are summed in a fixed order into U_k
+    int64_t part = 0;
     for (int j = 0; j < NBb; j++) {
       for (int i = j; i < NBb; i++) {
         Operand sa = opnd(B_WS, S + i * T, na);
         Operand sb = opnd(B_WS, S + j * T, na);
         Operand cc = opnd(B_WS, upd + (int64_t)(j * T) * na + i * T, na);
         Task t = gemm(bh(i), bh(j), nn, -1.0, sa, sb, 1.0, cc, i == j, 0);
-        int id = B.add(t, {lv, NBc, 0, (int)k, j, i}, uc_group[k]);
-        B.wait_task(id, trsmb[i]);
-        B.wait_task(id, trsmb[j]);
+        if (scrK[k] >= 0) {
+          const int p = split_count(nn, kc);
+          SplitTask st = add_split_gemm(B, t, kc, scrK[k] + part * p * T * T, {lv, NBc, 0, (int)k, j, i},
+                                        uc_group[k]);
+          part++;
+          for (int id : st.parts) {
+            B.wait_task(id, trsmb[i]);
+            B.wait_task(id, trsmb[j]);
+          }
+        } else {
+          int id = B.add(t, {lv, NBc, 0, (int)k, j, i}, uc_group[k]);
+          B.wait_task(id, trsmb[i]);
+          B.wait_task(id, trsmb[j]);
+        }
       }
     }
     // blk21 = S_k * M  (= L21 L11^{-1}, cholesky.c:72)

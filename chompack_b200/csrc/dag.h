@@ -535,6 +535,15 @@ inline int pinv_ksplit() {
   return v < 2 * TILE ? 2 * TILE : v;
 }
 
+// Largest K of one partial product of cholesky's Schur-complement tiles
+// U_k -= S_k S_k^T (CHB_CHOL_KSPLIT, rounded down to a multiple of TILE;
+// 0, the default, leaves them whole).
+inline int chol_ksplit() {
+  const char* e = std::getenv("CHB_CHOL_KSPLIT");
+  const int v = e ? (std::atoi(e) / TILE) * TILE : 0;
+  return v <= 0 ? 0 : (v < 2 * TILE ? 2 * TILE : v);
+}
+
 // Largest front order (nj) that a sweep runs as one shared-memory task
 // (cholesky, projected_inverse): TILE, or CHB_SMALL_FRONT_NJ when set
 // (0 turns the small-front tasks off).

@@ -94,3 +94,31 @@ def test_wide_front_projected_inverse(kind, args, merge, order, seed):
     bases = {0: y, 1: np.full(prog.ws_doubles, np.nan)}
     assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
     assert_blocks_close(s, y, ref)
+
+
+@pytest.mark.parametrize("kind,args,merge", [("grid3d", (12,), (128, 128)), ("grid2d", (60,), (256, 256))])
+@pytest.mark.parametrize("order,seed", [("random", 5), ("dynamic", 6)])
+def test_split_schur_cholesky(kind, args, merge, order, seed):
+    """cholesky with the Schur-complement tiles U_k -= S_k S_k^T split along
+    K (CHB_CHOL_KSPLIT=128): partial products in scratch, summed in a fixed
+    order by T_SUM tasks into U_k."""
+    old = os.environ.get("CHB_CHOL_KSPLIT")
+    os.environ["CHB_CHOL_KSPLIT"] = "128"
+    try:
+        A, s = problem(kind, *args, merge=merge, seed=3)
+        pl = Plan(s, device=-1)
+        prog = taskvm.Program(pl.handle, N.OP_CHOLESKY, nsn=s.Nsn)
+        sch = taskvm.Schedule(pl.handle, N.OP_CHOLESKY)
+    finally:
+        if old is None:
+            os.environ.pop("CHB_CHOL_KSPLIT", None)
+        else:
+            os.environ["CHB_CHOL_KSPLIT"] = old
+    assert int(np.sum(prog.tasks["op"] == taskvm.T_SUM)) > 0
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    ref = x0.copy()
+    assert oracle.cholesky(s, ref) == 0
+    x = x0.copy()
+    bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, x, ref)
