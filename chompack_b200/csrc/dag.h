@@ -527,11 +527,11 @@ struct DagBuilder {
 
 // Largest K of one partial product of projected_inverse's long-K tiles
 // (CHB_PINV_KSPLIT, rounded down to a multiple of TILE, at least 2 TILE;
-// default 768: at 40^3 the sweep is bound by the CTAs' total work, and
-// 384 / 768 / 1536 gave 6.01 / 5.76 / 6.09 ms).
+// default 512: at 40^3 the sweep is bound by the CTAs' total work, and
+// 384 / 512 / 768 / 1024 / 1536 gave 6.01 / 5.64 / 5.74 / 5.72 / 6.09 ms).
 inline int pinv_ksplit() {
   const char* e = std::getenv("CHB_PINV_KSPLIT");
-  const int v = e ? (std::atoi(e) / TILE) * TILE : 768;
+  const int v = e ? (std::atoi(e) / TILE) * TILE : 512;
   return v < 2 * TILE ? 2 * TILE : v;
 }
 
