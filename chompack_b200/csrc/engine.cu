@@ -827,18 +827,34 @@ constexpr int POTRF_LD = TILE + 1;
 constexpr int POTRF_SMEM_DOUBLES = 2 * TILE * POTRF_LD + TILE + 32 + 16 * TILE;
 
 // Phase timing for development builds (-DCHB_PROFILE_POTRF); compiled out
-// otherwise.
+// otherwise.  Cycles per phase summed over tasks (thread 0's view):
+// diagonal task 0 tile load, 1 panel rows and diagonal-block update,
+// 2 16x16 factor, 3 16x16 inverse, 4 end-of-step barrier, 5 L store,
+// 6 last inverse block row, 7 M store, 8 first-part publish; look-ahead
+// 16 mid waits, 17 tile load, 18 L' product, 19 L' store, 20 early signal,
+// 21 L'L'^T product, 22 D update.  Task counts at 12 and 24.
 #ifdef CHB_PROFILE_POTRF
-__device__ unsigned long long g_potrf_phase[8];
+__device__ unsigned long long g_potrf_phase[32];
 #define POTRF_STAMP(i)                                                    \
   do {                                                                    \
     long long now_ = clock64();                                           \
     if (threadIdx.x == 0) atomicAdd(&g_potrf_phase[i], now_ - stamp_);    \
     stamp_ = now_;                                                        \
   } while (0)
+#define POTRF_COUNT(i)                                        \
+  do {                                                        \
+    if (threadIdx.x == 0) atomicAdd(&g_potrf_phase[i], 1ull); \
+  } while (0)
+#define POTRF_CLOCK_START long long stamp_ = clock64()
 #else
 #define POTRF_STAMP(i) \
   do {                 \
+  } while (0)
+#define POTRF_COUNT(i) \
+  do {                 \
+  } while (0)
+#define POTRF_CLOCK_START \
+  do {                    \
   } while (0)
 #endif
 
@@ -1002,6 +1018,8 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
   double* __restrict__ P = X + b;
   double* __restrict__ D = X + (int64_t)b * lda + b;
   const int tid = threadIdx.x;
+  POTRF_CLOCK_START;
+  POTRF_COUNT(24);
   __syncthreads();
   if (tid == 0) {
     int abort = 0;
@@ -1025,6 +1043,7 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
   }
   __syncthreads();
   if (s_la_abort) return;
+  POTRF_STAMP(16);
   // A(c+1, c) into sL (rows >= m2 zero)
   {
     double v[TILE * TILE / NTHREADS];
@@ -1041,6 +1060,7 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
     }
   }
   __syncthreads();
+  POTRF_STAMP(17);
   const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
   {
     double acc[TILE / 8][4];
@@ -1048,6 +1068,7 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
     for (int j = 0; j < TILE / 8; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
     mma_rows_lower_b(sL, sM, acc);  // b = TILE: only the last block column of a front has b < TILE
     __syncthreads();
+    POTRF_STAMP(18);
     // L' into sL and in place
 #pragma unroll
     for (int j = 0; j < TILE / 8; j++)
@@ -1060,6 +1081,7 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
       }
   }
   __syncthreads();
+  POTRF_STAMP(19);
   if (t.aux[3] > 0) {
     if (ra.dynamic) {
       const int c = t.aux[3] - 1;
@@ -1069,11 +1091,13 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
       red_release_add(ra.counters + (t.aux[3] - 1), 1);
     }
   }
+  POTRF_STAMP(20);
   // D -= L' L'^T on and below the diagonal
   double acc[5][4];
 #pragma unroll
   for (int i = 0; i < 5; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.0;
   mma_lower_tiles(sL, b, acc);
+  POTRF_STAMP(21);
   double old[5][4];
 #pragma unroll
   for (int i = 0; i < 5; i++) {
@@ -1095,6 +1119,7 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
       if (r < m2 && r >= c) D[(int64_t)c * lda + r] = old[i][h] - acc[i][h];
     }
   }
+  POTRF_STAMP(22);
 }
 
 __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti) {
@@ -1114,9 +1139,8 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   const int ldm = t.c.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, q = lane & 3;
-#ifdef CHB_PROFILE_POTRF
-  long long stamp_ = clock64();
-#endif
+  POTRF_CLOCK_START;
+  POTRF_COUNT(12);
   {
     double v[TILE * TILE / NTHREADS];
 #pragma unroll
@@ -1147,6 +1171,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
         potrf_syrk_tile(sL, jp, j0, j0 + 8);
         __syncwarp();
       }
+      POTRF_STAMP(1);
       if (!factor) {
         // invert-only: reciprocals of the diagonal (a zero pivot is singular)
         const int il = lane & 15;
@@ -1200,7 +1225,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
         }
         }
         __syncwarp();
-        POTRF_STAMP(1);
+        POTRF_STAMP(2);
         // inverse of the block: lane c < 16 holds column c,
         // M(r, c) = -rd(r) sum_{l<r} L(r, l) M(l, c) for r > c, M(c, c) = rd(c),
         // right-looking: as soon as M(l, c) is known it is added into the
@@ -1221,7 +1246,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
           for (int r = 0; r < 16; r++)
             if (r >= il) sM[(j0 + il) * LD + j0 + r] = m[r];
         }
-        POTRF_STAMP(2);
+        POTRF_STAMP(3);
       }
     } else {
       if (below) {
@@ -1238,9 +1263,8 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
       if (want_inv && J >= 2) potrf_inv_row(sL, sM, sT + 128 * warp, J - 1, warp - 1, NTHREADS / 32 - 1);
     }
     __syncthreads();
-    POTRF_STAMP(3);
+    POTRF_STAMP(4);
   }
-  POTRF_STAMP(4);
   if (factor) {
 #pragma unroll 8
     for (int s2 = 0; s2 < TILE * TILE / NTHREADS; s2++) {
@@ -1271,6 +1295,7 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
       __threadfence();
       red_release_add(ra.counters + ti, 1);
     }
+    POTRF_STAMP(8);
     potrf_lookahead(ra, t, smem);
   }
 }
@@ -2104,6 +2129,19 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
 static_assert(2 * TILE * LDS <= ENGINE_SMEM_BASE_DOUBLES, "GEMM staging exceeds the engine's shared memory");
 static_assert(GEMM_STAGES * STAGE_DOUBLES <= ENGINE_SMEM_BASE_DOUBLES, "GEMM ring exceeds the engine's shared memory");
 static_assert(POTRF_SMEM_DOUBLES <= ENGINE_SMEM_BASE_DOUBLES, "POTRF exceeds the engine's shared memory");
+
+#ifdef CHB_PROFILE_POTRF
+// Development builds only: copies out (and optionally clears) the diagonal
+// task's phase counters.
+extern "C" int chb_dev_potrf_phase(unsigned long long* out, int clear) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_potrf_phase, sizeof(g_potrf_phase));
+  if (e == cudaSuccess && clear) {
+    static const unsigned long long zero[32] = {};
+    e = cudaMemcpyToSymbol(g_potrf_phase, zero, sizeof(zero));
+  }
+  return (int)e;
+}
+#endif
 
 size_t engine_smem_bytes() { return (size_t)ENGINE_SMEM_DOUBLES * sizeof(double); }
 
