@@ -1138,7 +1138,6 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   double* __restrict__ Mout = want_inv ? ra.bases[t.c.base] + t.c.off : nullptr;
   const int ldm = t.c.ld;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, q = lane & 3;
   POTRF_CLOCK_START;
   POTRF_COUNT(12);
   {

@@ -122,3 +122,34 @@ def test_split_schur_cholesky(kind, args, merge, order, seed):
     bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
     assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
     assert_blocks_close(s, x, ref)
+
+
+@pytest.mark.parametrize("ksplit", ["128", "1024"])
+@pytest.mark.parametrize("order,seed", [("random", 7), ("dynamic", 8)])
+def test_projected_inverse_split_sizes(ksplit, order, seed):
+    """projected_inverse with other split-K chunk sizes (CHB_PINV_KSPLIT):
+    the number of partial products changes, the result stays the
+    reference's within the FP64 tolerance."""
+    old = os.environ.get("CHB_PINV_KSPLIT")
+    os.environ["CHB_PINV_KSPLIT"] = ksplit
+    try:
+        A, s = problem("grid3d", 12, merge=(128, 128), seed=3)
+        pl = Plan(s, device=-1)
+        prog = taskvm.Program(pl.handle, N.OP_PROJECTED_INVERSE, nsn=s.Nsn)
+        sch = taskvm.Schedule(pl.handle, N.OP_PROJECTED_INVERSE)
+    finally:
+        if old is None:
+            os.environ.pop("CHB_PINV_KSPLIT", None)
+        else:
+            os.environ["CHB_PINV_KSPLIT"] = old
+    nsum = int(np.sum(prog.tasks["op"] == taskvm.T_SUM))
+    assert (nsum > 0) if ksplit == "128" else True
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    L = x0.copy()
+    assert oracle.cholesky(s, L) == 0
+    ref = L.copy()
+    assert oracle.projected_inverse(s, ref) == 0
+    y = L.copy()
+    bases = {0: y, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, y, ref)
