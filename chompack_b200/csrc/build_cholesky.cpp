@@ -172,12 +172,16 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       for (int r = 0; r < NBc; r++) trsm_prev[r] = trsm_top[r];
       if (fuse) {
         const int r = c + 1;
-        B.split_task(pot, 9.0);
+        // modelled second part and early-signal offset of the fused task:
+        // list-order parameters, not durations (the look-ahead takes
+        // ~13 us; at 40^3, (9, +5) / (6, +3) / (3, +1.5) / (1, +0.5) gave
+        // cholesky 6.61 / 6.56 / 6.52 / 6.54 ms)
+        B.split_task(pot, 3.0);
         if (c > 0) {
           B.wait_mid(pot, last_top[(size_t)r * NBc + c]);
           B.wait_mid(pot, last_top[(size_t)r * NBc + r]);
         }
-        trsm_top[r].id = B.early_signal(pot, B.cost[pot] + 5.0);
+        trsm_top[r].id = B.early_signal(pot, B.cost[pot] + 1.5);
         trsm_top[r].group = true;
         last_top[(size_t)r * NBc + r] = pot;
       }
