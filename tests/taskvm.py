@@ -14,17 +14,9 @@ import ctypes
 import numpy as np
 
 from chompack_b200 import _native as N
+from chompack_b200 import trace
 
-OPERAND = np.dtype([("off", "<i8"), ("ld", "<i4"), ("base", "u1"), ("mode", "u1"), ("prec", "<i2"),
-                    ("diag", "<i4"), ("pad2", "<i4")])
-TASK = np.dtype({
-    "names": ["op", "cmode", "nwait", "wait_off", "group", "m", "n", "k", "cdiag", "aux", "alpha", "beta",
-              "a", "b", "c", "off2"],
-    "formats": ["u1", "u1", "<u2", "<i4", "<i4", "<i4", "<i4", "<i4", "<i4", ("<i4", 4), "<f8", "<f8",
-                OPERAND, OPERAND, OPERAND, "<i8"],
-    "offsets": [0, 1, 2, 4, 8, 12, 16, 20, 24, 28, 48, 56, 64, 88, 112, 136],
-    "itemsize": 144,
-})
+TASK = trace.TASK  # the engine's 144-byte task record
 FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4"), ("chbeg", "<i4"),
                   ("chend", "<i4"), ("parent", "<i4"), ("level", "<i4"), ("blk", "<i8"), ("upd", "<i8"),
                   ("col0", "<i8"), ("vpos", "<i8")])
