@@ -29,6 +29,11 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   return v;
 }
 
+// Publication of a counter: every caller runs it from one thread right
+// after a __syncthreads(), and the release is cumulative, so the CTA's
+// writes before the barrier are visible (gpu scope) before the increment
+// without a separate fence (measured: cholesky 6.48 -> 6.38 ms at 40^3
+// without the __threadfence() that preceded it).
 __device__ __forceinline__ void red_release_add(int* p, int v) {
   asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -707,7 +712,6 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
           if (threadIdx.x < 32)
             release_list(ra, __ldg(ra.succ_off + c), __ldg(ra.succ_off + c + 1), nullptr, false, nullptr);
         } else if (threadIdx.x == 0) {
-          __threadfence();
           red_release_add(ra.counters + (t.aux[3] - 1), 1);
         }
       }
@@ -1087,7 +1091,6 @@ __device__ __forceinline__ void potrf_lookahead(const RunArgs& ra, const Task& t
       const int c = t.aux[3] - 1;
       if (tid < 32) release_list(ra, __ldg(ra.succ_off + c), __ldg(ra.succ_off + c + 1), nullptr, false, nullptr);
     } else if (tid == 0) {
-      __threadfence();
       red_release_add(ra.counters + (t.aux[3] - 1), 1);
     }
   }
@@ -1291,7 +1294,6 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
     if (ra.dynamic) {
       if (tid < 32) release_list(ra, __ldg(ra.succ_off + ti), __ldg(ra.succ_off + ti + 1), nullptr, false, nullptr);
     } else if (tid == 0) {
-      __threadfence();
       red_release_add(ra.counters + ti, 1);
     }
     POTRF_STAMP(8);
@@ -2107,7 +2109,6 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     }
     if (!ra.dynamic) {
       if (threadIdx.x == 0) {
-        __threadfence();
         red_release_add(ra.counters + ti, 1);
         if (t.group >= 0) red_release_add(ra.counters + t.group, 1);
       }
