@@ -153,3 +153,44 @@ def test_projected_inverse_split_sizes(ksplit, order, seed):
     bases = {0: y, 1: np.full(prog.ws_doubles, np.nan)}
     assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
     assert_blocks_close(s, y, ref)
+
+
+@pytest.mark.parametrize("nj", ["0", "32"])
+@pytest.mark.parametrize("order,seed", [("random", 9), ("dynamic", 10)])
+def test_small_front_threshold(nj, order, seed):
+    """CHB_SMALL_FRONT_NJ: with 0 every front is a tile graph, with 32 the
+    fronts of order <= 32 are single shared-memory tasks and the others tile
+    graphs; both sweeps reproduce the reference in either case."""
+    old = os.environ.get("CHB_SMALL_FRONT_NJ")
+    os.environ["CHB_SMALL_FRONT_NJ"] = nj
+    try:
+        A, s = problem("grid2d", 40, merge=(16, 16), seed=5)
+        pl = Plan(s, device=-1)
+        progs = {op: (taskvm.Program(pl.handle, op, nsn=s.Nsn), taskvm.Schedule(pl.handle, op))
+                 for op in (N.OP_CHOLESKY, N.OP_PROJECTED_INVERSE)}
+    finally:
+        if old is None:
+            os.environ.pop("CHB_SMALL_FRONT_NJ", None)
+        else:
+            os.environ["CHB_SMALL_FRONT_NJ"] = old
+    fronts = np.diff(np.asarray(s.sncolptr))
+    want = int(np.sum(fronts <= int(nj)))
+    assert int(np.sum(progs[N.OP_CHOLESKY][0].tasks["op"] == taskvm.T_FRONT)) == want
+    assert int(np.sum(progs[N.OP_PROJECTED_INVERSE][0].tasks["op"] == taskvm.T_PFRONT)) == want
+    if nj == "32":
+        assert 0 < want < len(fronts)
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    L = x0.copy()
+    assert oracle.cholesky(s, L) == 0
+    Y = L.copy()
+    assert oracle.projected_inverse(s, Y) == 0
+    x = x0.copy()
+    prog, sch = progs[N.OP_CHOLESKY]
+    assert taskvm.VM(prog, {0: x, 1: np.full(prog.ws_doubles, np.nan)}, s.relidx, s.chidx).run(
+        order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, x, L)
+    y = L.copy()
+    prog, sch = progs[N.OP_PROJECTED_INVERSE]
+    assert taskvm.VM(prog, {0: y, 1: np.full(prog.ws_doubles, np.nan)}, s.relidx, s.chidx).run(
+        order, seed=seed + 1, schedule=sch) == 0
+    assert_blocks_close(s, y, Y)
