@@ -9,7 +9,7 @@ supernodal clique tree, with the API of CHOMPACK.
 
 The symbolic analysis runs on the host (native C++); the numeric sweeps
 (`cholesky`, `llt`, `projected_inverse`, `completion`, `hessian`, `trsm`,
-`dot`) run as CUDA kernels on the GPU through the C ABI in
+`trmm`, `dot`) run as CUDA kernels on the GPU through the C ABI in
 include/chompack_b200.h.  There is no CPU fallback for the sweeps.
 """
 from .sparse import spmatrix, tril, triu, symmetrize, perm, eye
@@ -20,9 +20,9 @@ from . import amd
 __all__ = ["spmatrix", "tril", "triu", "symmetrize", "perm", "eye", "symbolic", "merge_size_fill", "peo",
            "cspmatrix", "amd"]
 
-from .cbase import cholesky, llt, projected_inverse, completion, hessian, trsm, dot  # noqa: E402,F401
+from .cbase import cholesky, llt, projected_inverse, completion, hessian, trsm, trmm, dot  # noqa: E402,F401
 from . import autograd  # noqa: E402,F401
 from .batch import batch  # noqa: E402,F401
 from . import mixed  # noqa: E402,F401
 
-__all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot", "autograd", "batch"]
+__all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot", "autograd", "batch"]

@@ -74,6 +74,7 @@ completion = _sig("chb_completion", ctypes.c_int, [PPLAN, vp, ctypes.c_int, vp, 
 hessian = _sig("chb_hessian", ctypes.c_int, [PPLAN, vp, vp, ctypes.POINTER(vp), i64, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, vp, ctypes.c_size_t, vp])
 trsm = _sig("chb_trsm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
+trmm = _sig("chb_trmm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
 dot = _sig("chb_dot", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 plan_merge = _sig("chb_plan_merge", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
                                                     ctypes.POINTER(PPLAN)])
@@ -98,5 +99,5 @@ projected_inverse_io = _sig("chb_projected_inverse_io", ctypes.c_int, [PPLAN, vp
 llt_io = _sig("chb_llt_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 program_io = _sig("chb_program_io", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64, vp, vp, vp, vp])
 
-OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT = range(7)
+OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT, OP_TRMM = range(8)
 HESSIAN_MAX_U = 59   # U matrices per chb_hessian call (base slots 5..63)

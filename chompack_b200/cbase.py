@@ -20,7 +20,7 @@ import torch
 
 from . import _native as N
 
-__all__ = ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "dot"]
+__all__ = ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot"]
 
 
 def _on_host(X):
@@ -239,6 +239,59 @@ def trsm(L, B, alpha=1.0, trans='N', nrhs=None, offsetB=0, ldB=None):
         host.reshape(-1, order="F")[:] = out if host.ndim == 1 else out
         if host.ndim > 1:
             host[:, :] = out.reshape(host.shape, order="F")
+
+
+def trmm(L, B, alpha=1.0, trans='N', nrhs=None, offsetB=0, ldB=None):
+    """Multiplication with a cspmatrix factor (pybase/trmm.py:4-116):
+    B := alpha L B (trans 'N') or alpha L^T B (trans 'T'), in place.
+
+    Arguments and the layout of B are those of trsm: a CUDA float64 tensor
+    (element (i, j) at storage offset i + j*ld) or a Fortran-ordered numpy
+    array (copied to the GPU and back), rows in the original order."""
+    if L.is_factor is not True:
+        raise ValueError("L must be a cspmatrix factor")
+    if trans not in ('N', 'T'):
+        raise ValueError("trans must be 'N' or 'T'")
+    v = _values(L, "L")
+    dev = v.device
+    Bt, host, cols, ld0 = _rhs_on_device(B, dev)
+    if nrhs is None:
+        nrhs = cols
+    if ldB is None:
+        ldB = ld0
+    plan = L.symb.plan(dev.index)
+    ptr = Bt.data_ptr() + 8 * int(offsetB)
+    _run_and_status(plan, N.OP_TRMM,
+                    lambda ws, nb, s: N.trmm(plan.handle, trans.encode(), int(nrhs), float(alpha), v.data_ptr(), ptr,
+                                             int(ldB), ws, nb, s), k=int(nrhs), flags=1 if trans == 'T' else 0)
+    if host is not None:
+        out = Bt.cpu().numpy()
+        if host.ndim == 1:
+            host[:] = out
+        else:
+            host[:, :] = out.reshape(host.shape, order="F")
+
+
+def _rhs_on_device(B, dev):
+    """(tensor on dev, host array or None, columns, leading dimension) of a
+    right-hand-side block given as a column-major CUDA float64 tensor or a
+    Fortran-ordered float64 numpy array."""
+    if isinstance(B, torch.Tensor):
+        if B.device != dev or B.dtype != torch.float64:
+            raise ValueError("B must be a float64 tensor on the device of L")
+        if B.dim() == 1:
+            return B, None, 1, B.shape[0]
+        if B.stride(0) != 1:
+            raise ValueError("B must be column-major (stride(0) == 1)")
+        return B, None, B.shape[1], B.stride(1)
+    import numpy as np
+    host = np.asarray(B)
+    if host.dtype != np.float64:
+        raise ValueError("B must be float64")
+    if host.ndim > 1 and not host.flags["F_CONTIGUOUS"]:
+        raise ValueError("B must be column-major (Fortran order)")
+    cols = 1 if host.ndim == 1 else host.shape[1]
+    return torch.from_numpy(host.reshape(-1, order="F")).to(dev), host, cols, host.shape[0]
 
 
 def dot(X, Y):

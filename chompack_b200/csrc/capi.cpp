@@ -128,6 +128,15 @@ extern "C" int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, 
                 alpha);
 }
 
+extern "C" int chb_trmm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
+                        int64_t ldB, void* work, size_t work_bytes, void* stream) {
+  if (trans != 'N' && trans != 'T') return set_error(-1, "trans must be 'N' or 'T'");
+  if (nrhs < 0 || (plan && ldB < plan->n)) return set_error(-1, "invalid nrhs or ldB");
+  double* bases[B_RHS + 1] = {const_cast<double*>(blkval), nullptr, nullptr, nullptr, B};
+  return run_op(plan, CHB_OP_TRMM, nrhs, trans == 'T' ? 1 : 0, bases, B_RHS + 1, work, work_bytes, stream, ldB,
+                alpha);
+}
+
 extern "C" int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
                        size_t work_bytes, void* stream) {
   clear_error();

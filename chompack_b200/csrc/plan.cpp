@@ -140,6 +140,7 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     case CHB_OP_LLT: rc = build_llt(*plan, *prog); break;
     case CHB_OP_COMPLETION: rc = build_completion(*plan, *prog, k != 0); break;
     case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, flags != 0); break;
+    case CHB_OP_TRMM: rc = build_trmm(*plan, *prog, k, flags != 0); break;
     case CHB_OP_HESSIAN: rc = build_hessian(*plan, *prog, (int)k, flags); break;
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
@@ -151,9 +152,10 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
   // Default schedule per sweep, by measurement on a 3-D grid of 64,000
   // unknowns: the chains of small dependent tasks of cholesky, llt and trsm
-  // run faster in static list order (a CTA already waits on the next task);
+  // run faster in static list order (a CTA already waits on the next task;
+  // trmm has the solve's structure and takes its schedule);
   // the other sweeps gain from running whichever task is ready.
-  prog->static_default = op == CHB_OP_CHOLESKY || op == CHB_OP_LLT || op == CHB_OP_TRSM;
+  prog->static_default = op == CHB_OP_CHOLESKY || op == CHB_OP_LLT || op == CHB_OP_TRSM || op == CHB_OP_TRMM;
   Program* p = prog.get();
   plan->progs[key] = std::move(prog);
   return p;

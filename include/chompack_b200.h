@@ -84,10 +84,12 @@ enum chb_op {
   CHB_OP_COMPLETION = 3,
   CHB_OP_HESSIAN = 4,
   CHB_OP_TRSM = 5,
-  CHB_OP_DOT = 6
+  CHB_OP_DOT = 6,
+  CHB_OP_TRMM = 7
 };
 
-/* Device workspace (bytes) an operation needs; `k` is nrhs for CHB_OP_TRSM,
+/* Device workspace (bytes) an operation needs; `k` is nrhs for CHB_OP_TRSM
+ * and CHB_OP_TRMM,
  * the number of U matrices for CHB_OP_HESSIAN and factored_updates for
  * CHB_OP_COMPLETION (ignored otherwise); `flags` is the hessian adj/inv
  * selector (adj | inv << 1 | factored_updates << 2), else 0.  This replaces
@@ -198,6 +200,13 @@ int chb_hessian(chb_plan* plan, const double* lblkval, const double* yblkval, do
  * (trans 'N') or alpha*L^{-T}B (trans 'T'); B is n x nrhs column-major with
  * leading dimension ldB, rows in the original (unpermuted) order. */
 int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
+             int64_t ldB, void* work, size_t work_bytes, void* stream);
+
+/* trmm — pybase/trmm.py:4-116 (Python only in the reference).  B :=
+ * alpha*L*B (trans 'N') or alpha*L^T*B (trans 'T') with the factor that
+ * chb_cholesky leaves in blkval; B as for chb_trsm.  Workspace
+ * chb_workspace_size(plan, CHB_OP_TRMM, nrhs, trans == 'T', ...). */
+int chb_trmm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
              int64_t ldB, void* work, size_t work_bytes, void* stream);
 
 /* dot — dot.c:3-23 (wrapper cbase.c:106-174).  Writes <X,Y> to result (one
