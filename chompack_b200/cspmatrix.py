@@ -157,9 +157,12 @@ class cspmatrix(object):
         lo = I >= J
         I, J, V = I[lo], J[lo], V[lo]
         idx = self._entry_index(I, J)
-        host = self.blkval.detach().to("cpu").numpy().copy()
-        host[idx] += alpha * V
-        self.blkval.copy_(torch.from_numpy(host))
+        # one entry per position (spmatrix sums duplicates; of (i, j) and
+        # (j, i) only one is in the permuted lower triangle), added in place
+        # where the values live: no copy of blkval through the host
+        dev = self.blkval.device
+        self.blkval.index_add_(0, torch.from_numpy(np.ascontiguousarray(idx, dtype=np.int64)).to(dev),
+                               torch.from_numpy(np.ascontiguousarray(alpha * V, dtype=np.float64)).to(dev))
 
     def add_projection(self, A, alpha=1.0, beta=1.0, reordered=False):
         """X := alpha*proj(A) + beta*X for a dense symmetric A
