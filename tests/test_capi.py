@@ -46,3 +46,23 @@ def test_host_only_plan_programs_and_workspace():
         info = pl.program_info(op)
         assert info["tasks"] > 0 and info["ws_bytes"] >= 256 + 8 * info["upd_doubles"]
     assert pl.workspace_bytes(N.OP_DOT) >= 8 * s.Nsn
+
+
+def test_trsm_and_trmm_reject_bad_arguments_before_touching_the_device():
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    from chompack_b200.plan import Plan
+    A = grids.grid2d(8, seed=0)
+    s = cp.symbolic(A, p=cp.amd.order(A))
+    pl = Plan(s, device=-1)
+    for fn in (N.trsm, N.trmm):
+        assert fn(pl.handle, b"X", 2, 1.0, None, None, s.n, None, 0, None) < 0
+        assert b"trans" in N.last_error()
+        assert fn(pl.handle, b"N", 2, 1.0, None, None, s.n - 1, None, 0, None) < 0
+        assert b"ldB" in N.last_error()
+    # the trmm programs exist for both transposes and need the right-hand
+    # sides' workspace: Bp and the update blocks, plus u'_k for 'N'
+    n_ws = pl.program_info(N.OP_TRMM, k=3, flags=0)["ws_doubles"]
+    t_ws = pl.program_info(N.OP_TRMM, k=3, flags=1)["ws_doubles"]
+    na = np.diff(np.asarray(s.relptr)).sum()
+    assert t_ws == 3 * (s.n + na) and n_ws == 3 * (s.n + 2 * na)
