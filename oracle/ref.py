@@ -53,6 +53,12 @@ def lib():
         _lib.trsm.restype = None
         _lib.dot.argtypes = [pi, pi, pi, pi, pd, pd]
         _lib.dot.restype = dbl
+        ci = P(ctypes.c_int)
+        _lib.dpftrf.argtypes = [ci, ci, pd, pd, ci, pd, ci, pd, ci]
+        _lib.dpftrf.restype = ctypes.c_int
+        for f in (_lib.dpfsv, _lib.dpfmv):
+            f.argtypes = [ci, ci, ctypes.c_char_p, pd, ci, pd, ci, pd, ci, pd]
+            f.restype = None
     return _lib
 
 
@@ -184,3 +190,48 @@ def set_threads(n):
             ob.scipy_openblas_set_num_threads(int(n))
             return True
     return False
+
+
+# Product-form factor of I + V diag(a) V^T (pfcholesky.c:52-136, called by
+# pfcholesky.py:113-211 as pfchol / pftrsm / pftrmm).  V, L, B are n x k
+# Fortran-ordered float64 arrays; V is overwritten as dpftrf does.
+
+def _ci(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _dF(a):
+    assert a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def pfchol(a, V):
+    """Returns (L, B, info) of dpftrf on V (modified in place)."""
+    assert V.flags["F_CONTIGUOUS"] and V.dtype == np.float64
+    n, k = V.shape
+    L = np.zeros((n, k), order="F")
+    B = np.zeros((n, k), order="F")
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    info = lib().dpftrf(_ci(n), _ci(k), _d(a), _dF(V), _ci(n), _dF(L), _ci(n), _dF(B), _ci(n))
+    return L, B, info
+
+
+def _pf_columns(fn, V, L, B, U, trans):
+    assert U.flags["F_CONTIGUOUS"] and U.dtype == np.float64
+    n, k = V.shape
+    U2 = U.reshape(n, -1, order="F")
+    for j in range(U2.shape[1]):
+        col = np.ascontiguousarray(U2[:, j])
+        fn(_ci(n), _ci(k), trans.encode(), _dF(V), _ci(n), _dF(L), _ci(n), _dF(B), _ci(n), _d(col))
+        U2[:, j] = col
+    return U
+
+
+def pftrsm(V, L, B, U, trans='N'):
+    """U := (L_1 ... L_k)^{-1} U ('N') or (L_k^T ... L_1^T)^{-1} U ('T')."""
+    return _pf_columns(lib().dpfsv, V, L, B, U, trans)
+
+
+def pftrmm(V, L, B, U, trans='N'):
+    """U := L_1 ... L_k U ('N') or L_k^T ... L_1^T U ('T')."""
+    return _pf_columns(lib().dpfmv, V, L, B, U, trans)
