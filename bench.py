@@ -14,31 +14,39 @@ explicit flush is done between steps.
 Metric: algorithmic GFLOP/s of the two sweeps (flop formulas summed over
 supernodes from the symbolic arrays).  `--impl reference` times the
 reference's own C kernels (compiled from its sources against OpenBLAS,
-oracle/_ref) on the host cores, same workload.  With N > 1 (torchrun) every
-rank factors its own replica of the matrix (the path has no cross-GPU
-exchange for independent matrices): value = total flops / max rank time.
+oracle/_ref) on the host cores, same workload; that process loads no library
+of this package (its inputs come from oracle/workload.py and the committed
+symbolic fixture).  With N > 1 every rank factors its own replica of the
+matrix (the path has no cross-GPU exchange for independent matrices):
+value = total flops / max rank time; `--gpus N` without a launcher starts
+the N ranks itself.  The batch section shards its 256 matrices over the
+ranks.  Every result is compared with the reference's output on the same
+inputs (`parity`, outside the timed region).
 """
 import argparse
 import json
 import os
+import socket
 import subprocess
 import sys
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-OUT_DIR = os.environ.get("CHB_OUT_DIR", "gpurun_out")  # the folder whose files are kept after a run
+OUT_DIR = os.environ.get("CHB_OUT_DIR")  # where the clock samples are written as CSV (unset: not written)
 sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
 METRIC = "chordal Cholesky+adjoint ms & GFLOP/s, mixed vs FP64 on B200 at stated error"
 WORKLOAD = "FP64 drop-in: 3-D 7-point grid 40^3 (n=64000), AMD, merge_size_fill(32,32); cholesky + projected_inverse"
+RTOL = 1e-12
+HBM_FALLBACK_GBS = 6650.0
 
 
 def sweep_flops(symb):
     """Algorithmic flops per supernode (the reference's BLAS sequence)."""
-    nn = np.diff(symb.snptr).astype(np.float64)
-    na = np.diff(symb.relptr).astype(np.float64)
+    nn = np.diff(np.asarray(symb.snptr)).astype(np.float64)
+    na = np.diff(np.asarray(symb.relptr)).astype(np.float64)
     nj = nn + na
     chol = nn ** 3 / 3 + 2 * nn ** 2 * na + nn * na ** 2
     pinv = nn ** 3 / 3 + nn ** 3 + 2 * na ** 2 * nn + 2 * nn ** 2 * na
@@ -51,6 +59,22 @@ def sweep_flops(symb):
             "potrf_updates": float((na ** 3 / 3).sum())}
 
 
+def sweep_bytes(symb):
+    """Algorithmic HBM bytes of one sweep: the block values read and written
+    once, and each update triangle written and read once."""
+    na = np.diff(np.asarray(symb.relptr)).astype(np.float64)
+    return int(16 * int(symb.blkptr[-1]) + np.sum(16 * na * (na + 1) / 2))
+
+
+def bench_config(symb):
+    """The workload description both arms print (identical dicts)."""
+    fl = sweep_flops(symb)
+    return {"workload": WORKLOAD, "n": int(symb.n), "nsn": int(symb.Nsn), "sweeps": ["cholesky", "projected_inverse"],
+            "flops_per_step": fl["cholesky"] + fl["projected_inverse"],
+            "l2": "inputs 246 MB > 126 MB L2; no flush",
+            "parallelism": "replicas: one matrix per rank, no data-path collective"}
+
+
 def build_problem(side=40, merge=(32, 32), seed=0):
     import chompack_b200 as cp
     from chompack_b200 import grids
@@ -59,10 +83,24 @@ def build_problem(side=40, merge=(32, 32), seed=0):
     return A, s
 
 
+def hbm_peak_gbs():
+    """Measured copy bandwidth of this pool's B200s when the driver wrote it,
+    else the fallback figure."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in d:
+                v = d[k]
+                return float(v["value"] if isinstance(v, dict) else v), "measured (MEASURED_PEAKS.json)"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return HBM_FALLBACK_GBS, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+
+
 class ClockSampler(object):
     """SM clock and clock-event-reason sampling during the timed region, by
-    NVML polling from a thread (every 2 ms; read-only queries).  The samples
-    are also written as CSV beside the run's other outputs (OUT_DIR)."""
+    NVML polling from a thread (every 2 ms; read-only queries).  With
+    CHB_OUT_DIR set the samples are also written there as CSV."""
 
     # NVML clocks-event-reason bits
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
@@ -72,7 +110,7 @@ class ClockSampler(object):
         self.dev = dev
         self.thread = None
         self.samples = []
-        self.path = os.path.join(ROOT, OUT_DIR, "clocks_bench_%d.csv" % os.getpid())
+        self.path = os.path.join(OUT_DIR, "clocks_bench_%d.csv" % os.getpid()) if OUT_DIR else None
 
     def _handle(self):
         import pynvml
@@ -120,14 +158,15 @@ class ClockSampler(object):
         self.thread.join(timeout=5)
         if not self.samples:
             return None
-        try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            with open(self.path, "w") as f:
-                f.write("time,sm_mhz,reasons_mask,power_w\n")
-                for t, sm, rs, pw in self.samples:
-                    f.write("%.4f,%.0f,0x%x,%.1f\n" % (t, sm, rs, pw))
-        except OSError:
-            pass
+        if self.path:
+            try:
+                os.makedirs(os.path.dirname(self.path), exist_ok=True)
+                with open(self.path, "w") as f:
+                    f.write("time,sm_mhz,reasons_mask,power_w\n")
+                    for t, sm, rs, pw in self.samples:
+                        f.write("%.4f,%.0f,0x%x,%.1f\n" % (t, sm, rs, pw))
+            except OSError:
+                pass
         reasons = set()
         for _, _, rs, _ in self.samples:
             for bit, nm in self.REASONS.items():
@@ -170,22 +209,25 @@ def fp64_peak_tflops(dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
+# ------------------------------------------------------------ reference arm
+
 def run_reference(args, rank, world):
-    """The reference's own C kernels on the host cores."""
+    """The reference's own C kernels on the host cores (rank 0 only).  The
+    inputs come from oracle/workload.py: no library of this package is
+    loaded by this process."""
     if rank != 0:
         return 0
-    from oracle import ref
-    import chompack_b200 as cp
+    from oracle import ref, workload
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference kernels not built (oracle/_ref)"}))
         return 0
     cores = os.cpu_count() or 1
     ref.set_threads(cores)
-    A, s = build_problem()
-    fl = sweep_flops(s)
-    step_flops = fl["cholesky"] + fl["projected_inverse"]
-    X = cp.cspmatrix(s, device="cpu") + A
-    x0 = X.blkval.numpy().copy()
+    s = workload.load_symbolic("grid3d_40_m32")
+    n, I, J, V = workload.grid3d_lower(40, seed=0)
+    x0 = workload.assemble(s, n, I, J, V)
+    cfg = bench_config(s)
+    step_flops = cfg["flops_per_step"]
 
     def step():
         x = x0.copy()
@@ -204,24 +246,37 @@ def run_reference(args, rank, world):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(val, 3), "unit": "GFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD + " [reference C kernels + OpenBLAS on host]", "n": s.n, "nsn": s.Nsn},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": round(val, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
-                         "sample": "full workload per step (cholesky + projected_inverse), %d steps" % args.steps},
+                         "sample": "full workload per step (cholesky + projected_inverse), %d steps; reference C "
+                                   "kernels + OpenBLAS threads on the host" % args.steps},
         "e2e": {"value": round(val, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
 
 
-def cpu_baseline(s, A, budget_s=15.0):
+# --------------------------------------------------- reference outputs, CPU
+
+def reference_outputs(s, x0):
+    """Reference factor and projected inverse of the workload (all cores)."""
     from oracle import ref
-    import chompack_b200 as cp
+    ref.set_threads(os.cpu_count() or 1)
+    L = x0.copy()
+    assert ref.cholesky(s, L) == 0
+    Y = L.copy()
+    assert ref.projected_inverse(s, Y) == 0
+    return L, Y
+
+
+def cpu_baseline(s, x0, budget_s=15.0):
+    """The reference's kernels on the host: cholesky + projected_inverse with
+    all cores (median of up to 5 runs within the budget) and with 1 thread
+    (one run), and the other drop-in sweeps once each with all cores."""
+    from oracle import ref
     cores = os.cpu_count() or 1
     ref.set_threads(cores)
     fl = sweep_flops(s)
     step_flops = fl["cholesky"] + fl["projected_inverse"]
-    X = cp.cspmatrix(s, device="cpu") + A
-    x0 = X.blkval.numpy().copy()
     times = []
     t_start = time.perf_counter()
     while len(times) < 5 and (time.perf_counter() - t_start) < budget_s:
@@ -232,7 +287,17 @@ def cpu_baseline(s, A, budget_s=15.0):
         times.append(time.perf_counter() - t0)
     med = float(np.median(times))
     out = {"value": round(step_flops / med / 1e9, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
-           "sample": "%d full runs of cholesky+projected_inverse (median %.1f ms)" % (len(times), med * 1e3)}
+           "sample": "%d full runs of cholesky+projected_inverse (median %.1f ms), OpenBLAS on %d threads"
+                     % (len(times), med * 1e3, cores)}
+    ref.set_threads(1)
+    x = x0.copy()
+    t0 = time.perf_counter()
+    ref.cholesky(s, x)
+    ref.projected_inverse(s, x)
+    t1 = time.perf_counter() - t0
+    out["one_thread"] = {"value": round(step_flops / t1 / 1e9, 3), "unit": "GFLOP/s", "cores": 1,
+                         "ms": round(t1 * 1e3, 1), "sample": "1 full run of cholesky+projected_inverse"}
+    ref.set_threads(cores)
     # the other drop-in sweeps once each, for the same comparison
     L = x0.copy()
     ref.cholesky(s, L)
@@ -258,57 +323,17 @@ def cpu_baseline(s, A, budget_s=15.0):
     return out
 
 
-def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
-    """Mixed-precision form (GEMM tiles on TF32 tensor cores, FP64 diagonal
-    tiles): log det forward + backward (cholesky + projected_inverse) on the
-    3-D 7-point grid side^3 with merge_size_fill(merge), timed in FP64,
-    TF32 and 3xTF32, with the errors of log det, its gradient and the factor
-    against the FP64 path, and an nrhs solve refined with FP64 residuals to
-    a normwise relative residual of 1e-12."""
-    import torch
-    import chompack_b200 as cp
-    from chompack_b200 import mixed
-    A, s = build_problem(side=side, merge=merge)
-    fl = sweep_flops(s)
-    flops = fl["cholesky"] + fl["projected_inverse"]
-    X0 = cp.cspmatrix(s, device=dev) + A
-    out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d); log det forward + backward "
-                       "(cholesky + projected_inverse)" % (side, s.n, merge[0], merge[1]),
-           "flops": flops}
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for prec in ("fp64", "tf32", "tf32x3"):
-        X = cp.cspmatrix(s, blkval=X0.blkval.clone())
-        times = []
-        for it in range(reps + 2):
-            X.blkval.copy_(X0.blkval)
-            X.is_factor = False
-            torch.cuda.synchronize(dev)
-            ev0.record()
-            cp.cholesky(X, precision=prec)
-            cp.projected_inverse(X, precision=prec)
-            ev1.record()
-            torch.cuda.synchronize(dev)
-            if it >= 2:
-                times.append(ev0.elapsed_time(ev1))
-        ms = float(np.median(times))
-        entry = {"ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1)}
-        if prec != "fp64":
-            ld, Y, rep = mixed.logdet_and_gradient(X0, precision=prec)
-            entry.update({k: rep[k] for k in ("logdet_rel_error", "gradient_rel_error", "factor_rel_error")})
-            L = cp.cspmatrix(s, blkval=X0.blkval.clone())
-            cp.cholesky(L, precision=prec)
-            B = torch.from_numpy(np.asfortranarray(np.random.default_rng(11).standard_normal((s.n, nrhs)))).to(dev)
-            torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
-            x, srep = mixed.solve(X0, L, B, tol=1e-12, maxiter=40)
-            torch.cuda.synchronize(dev)
-            entry["solve"] = {"nrhs": nrhs, "iterations": srep["iterations"],
-                              "residual": srep["residuals"][-1], "ms": round((time.perf_counter() - t0) * 1e3, 2)}
-        out[prec] = entry
-    out["speedup_tf32"] = round(out["fp64"]["ms"] / out["tf32"]["ms"], 3)
-    out["speedup_tf32x3"] = round(out["fp64"]["ms"] / out["tf32x3"]["ms"], 3)
-    return out
+def _logdet_of_factor(s, L):
+    ld = 0.0
+    for k in range(int(s.Nsn)):
+        nn = int(s.snptr[k + 1] - s.snptr[k])
+        nj = int(s.sncolptr[k + 1] - s.sncolptr[k])
+        blk = L[int(s.blkptr[k]):int(s.blkptr[k + 1])].reshape((nj, nn), order="F")
+        ld += 2.0 * float(np.sum(np.log(np.diag(blk[:nn]))))
+    return ld
 
+
+# ----------------------------------------------------------- side sections
 
 def _event_ms(dev, fn, reps):
     """Median CUDA-event time of fn() over reps runs after two warm-ups."""
@@ -326,24 +351,104 @@ def _event_ms(dev, fn, reps):
     return float(np.median(times))
 
 
-def batch_section(dev, count=256, value_sets=64, reps=5):
+def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
+    """Mixed-precision form (GEMM tiles on TF32 tensor cores, FP64 diagonal
+    tiles): log det forward + backward (cholesky + projected_inverse) on the
+    3-D 7-point grid side^3 with merge_size_fill(merge), timed in FP64,
+    TF32 and 3xTF32.  Errors of log det, its gradient (the projected inverse)
+    and the factor are stated against the reference's FP64 kernels run on
+    the same inputs; the FP64 GPU path's parity there is reported too.  An
+    nrhs solve is refined with FP64 residuals to a normwise relative
+    residual of 1e-12 (timed after a warm-up solve)."""
+    import torch
+    import chompack_b200 as cp
+    from chompack_b200 import mixed
+    from oracle import workload
+    A, s = build_problem(side=side, merge=merge)
+    fl = sweep_flops(s)
+    flops = fl["cholesky"] + fl["projected_inverse"]
+    X0 = cp.cspmatrix(s, device=dev) + A
+    x0 = X0.blkval.cpu().numpy()
+    Lr, Yr = reference_outputs(s, x0)
+    ld_ref = _logdet_of_factor(s, Lr)
+    out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d); log det forward + backward "
+                       "(cholesky + projected_inverse)" % (side, s.n, merge[0], merge[1]),
+           "flops": flops, "errors_against": "reference C kernels (oracle/_ref), FP64, same inputs"}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for prec in ("fp64", "tf32", "tf32x3"):
+        X = cp.cspmatrix(s, blkval=X0.blkval.clone())
+        times = []
+        for it in range(reps + 2):
+            X.blkval.copy_(X0.blkval)
+            X.is_factor = False
+            torch.cuda.synchronize(dev)
+            ev0.record()
+            cp.cholesky(X, precision=prec)
+            cp.projected_inverse(X, precision=prec)
+            ev1.record()
+            torch.cuda.synchronize(dev)
+            if it >= 2:
+                times.append(ev0.elapsed_time(ev1))
+        ms = float(np.median(times))
+        entry = {"ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1)}
+        ld, Ym, _ = mixed.logdet_and_gradient(X0, precision=prec, reference=False)
+        Lm = cp.cspmatrix(s, blkval=X0.blkval.clone())
+        cp.cholesky(Lm, precision=prec)
+        Lh = Lm.blkval.cpu().numpy()
+        Yh = Ym.blkval.cpu().numpy()
+        entry["logdet_rel_error"] = abs(ld - ld_ref) / abs(ld_ref)
+        entry["gradient_rel_error"] = float(np.abs(Yh - Yr).max() / np.abs(Yr).max())
+        entry["factor_rel_error"] = float(np.abs(Lh - Lr).max() / np.abs(Lr).max())
+        if prec == "fp64":
+            entry["parity_scaled_error"] = max(workload.block_errors(s, Lh, Lr), workload.block_errors(s, Yh, Yr))
+        else:
+            B = torch.from_numpy(np.asfortranarray(np.random.default_rng(11).standard_normal((s.n, nrhs)))).to(dev)
+            mixed.solve(X0, Lm, B, tol=1e-12, maxiter=40)     # warm-up: builds the solve programs
+            torch.cuda.synchronize(dev)
+            ev0.record()
+            x, srep = mixed.solve(X0, Lm, B, tol=1e-12, maxiter=40)
+            ev1.record()
+            torch.cuda.synchronize(dev)
+            sms = ev0.elapsed_time(ev1)
+            entry["solve"] = {"nrhs": nrhs, "iterations": srep["iterations"], "residual": srep["residuals"][-1],
+                              "ms": round(sms, 3), "ms_per_iteration": round(sms / srep["iterations"], 3)}
+        out[prec] = entry
+    out["speedup_tf32"] = round(out["fp64"]["ms"] / out["tf32"]["ms"], 3)
+    out["speedup_tf32x3"] = round(out["fp64"]["ms"] / out["tf32x3"]["ms"], 3)
+    return out
+
+
+def batch_section(dev, rank, world, count=256, value_sets=64, reps=5):
     """Batched FP64 factorisation: `count` independent 2-D 5-point grids
     (side uniform in 20..120, each node with 2 extra random neighbours
     within grid distance 5, AMD ordering), and `value_sets` value sets on
     one 64x64 grid pattern.  Each batch is one merged plan: cholesky and
-    projected_inverse of all its matrices take one launch each."""
+    projected_inverse of all its matrices take one launch each.  With
+    world > 1 the uneven grids are sharded over the ranks by estimated
+    flops (chompack_b200.shard): every rank sweeps its share with its own
+    merged plan, the time is the max over ranks and the per-matrix log dets
+    are gathered.  Rank 0 also times the reference's kernels on the same
+    matrices and checks parity on a sample."""
+    import torch
     import chompack_b200 as cp
-    from chompack_b200 import grids
+    from chompack_b200 import grids, shard
     out = {}
-    rng = np.random.default_rng(2024)
-    sides = rng.integers(20, 121, size=count)
+    specs = grids.uneven_batch_specs(count)
     As, symbs = [], []
-    for i, sd in enumerate(sides):
-        A = grids.grid2d_extra(int(sd), seed=1000 + i)
+    for sd, seed in specs:
+        A = grids.grid2d_extra(sd, seed=seed)
         As.append(A)
         symbs.append(cp.symbolic(A, p=cp.amd.order(A)))
-    for name, Bs, Xs in (("uneven_grids", symbs, As), ("value_sets_64x64", None, None)):
-        if Bs is None:
+    costs = [sweep_flops(sb)["cholesky"] for sb in symbs]
+    mine = shard.my_share(costs, rank, world) if world > 1 else list(range(count))
+    peak, peak_src = hbm_peak_gbs()
+    for name in ("uneven_grids", "value_sets_64x64"):
+        if name == "uneven_grids":
+            Bs = [symbs[i] for i in mine]
+            Xs = [As[i] for i in mine]
+        else:
+            if world > 1 and rank != 0:
+                continue
             A0 = grids.grid2d(64, seed=7)
             s0 = cp.symbolic(A0, p=cp.amd.order(A0))
             Bs = [s0] * value_sets
@@ -358,62 +463,128 @@ def batch_section(dev, count=256, value_sets=64, reps=5):
             B.projected_inverse(x)
         ms = _event_ms(dev, step, reps)
         flops = sum(sweep_flops(sb)["cholesky"] + sweep_flops(sb)["projected_inverse"] for sb in Bs)
-        out[name] = {"matrices": len(Bs), "n_total": int(sum(sb.n for sb in Bs)), "values": int(B.size),
-                     "launches_per_step": 2, "ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1),
-                     "matrices_per_s": round(len(Bs) / ms * 1e3, 1), "step": "cholesky + projected_inverse (copy of "
-                     "the values included)"}
+        alg = sum(2 * sweep_bytes(sb) for sb in Bs)
+        entry = {"matrices": len(Bs), "n_total": int(sum(sb.n for sb in Bs)), "values": int(B.size),
+                 "launches_per_step": 2, "ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1),
+                 "matrices_per_s": round(len(Bs) / ms * 1e3, 1),
+                 "algorithmic_bytes": alg, "achieved_gbs": round(alg / ms / 1e6, 1),
+                 "hbm_frac": round(alg / ms / 1e6 / peak, 4), "hbm_peak_gbs": peak, "hbm_peak_source": peak_src,
+                 "step": "cholesky + projected_inverse (copy of the values included)"}
+        if name == "uneven_grids" and world > 1:
+            x.copy_(x0)
+            B.cholesky(x)
+            lds = B.logdet(x).cpu().numpy()
+            all_ld = shard.gather_results(mine, lds, count)
+            t_max = shard.max_over_ranks(ms, device=dev)
+            import torch.distributed as dist
+            per_rank = [None] * world
+            dist.all_gather_object(per_rank, {"rank": rank, "matrices": len(Bs), "ms": round(ms, 3),
+                                              "gflops": round(flops / ms / 1e6, 1)})
+            entry = {"matrices": count, "ranks": per_rank, "ms": round(t_max, 3),
+                     "matrices_per_s": round(count / t_max * 1e3, 1), "logdets_gathered": sum(
+                         v is not None for v in all_ld), "sharding": "chompack_b200.shard.partition by cholesky flops"}
+        if rank == 0 and name == "uneven_grids":
+            entry.update(_batch_reference(Bs, x0, x, B, dev))
+        out[name] = entry
     return out
 
 
+def _batch_reference(Bs, x0, x, B, dev, sample_every=16):
+    """Reference kernels on the host for the same batch (all matrices, all
+    cores), and parity of cholesky + projected_inverse on every 16th."""
+    from oracle import ref, workload
+    ref.set_threads(os.cpu_count() or 1)
+    xh = x0.cpu().numpy()
+    x.copy_(x0)
+    B.cholesky(x)
+    Lg = x.cpu().numpy().copy()
+    B.projected_inverse(x)
+    Yg = x.cpu().numpy()
+    t0 = time.perf_counter()
+    outs = []
+    for m, s in enumerate(Bs):
+        r = xh[B.offsets[m]:B.offsets[m + 1]].copy()
+        ref.cholesky(s, r)
+        L = r.copy() if m % sample_every == 0 else None
+        ref.projected_inverse(s, r)
+        outs.append((L, r))
+    dt = time.perf_counter() - t0
+    worst = 0.0
+    for m in range(0, len(Bs), sample_every):
+        seg = slice(B.offsets[m], B.offsets[m + 1])
+        worst = max(worst, workload.block_errors(Bs[m], Lg[seg], outs[m][0]),
+                    workload.block_errors(Bs[m], Yg[seg], outs[m][1]))
+    return {"reference_ms": round(dt * 1e3, 1), "reference_cores": os.cpu_count() or 1,
+            "parity": {"max_scaled_error": worst, "rtol": RTOL, "matrices_checked": len(range(0, len(Bs),
+                                                                                            sample_every))}}
+
+
 def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
-    """Differentiation: log det and its gradient (the projected inverse) for
-    `value_sets` value sets on the 3-D 7-point grid side^3 in one batch
-    (forward + backward = two launches), a central finite-difference check
-    of the gradient and of the second derivative (hessian) along a random
-    symmetric direction on the pattern, for the first value set."""
+    """Differentiation: log det of `value_sets` value sets on the 3-D 7-point
+    grid side^3 through the autograd Function (chompack_b200.autograd) with a
+    leading batch dimension, forward + backward by torch.autograd.grad: one
+    cholesky launch, one projected_inverse launch and three small reduction
+    and weight kernels for all value sets.  Checks on value set 0: the
+    gradient against the reference's projected inverse (<g,U> = <Y_ref,U>),
+    the central finite difference with h = 1e-6, and the Hessian-vector
+    product -<U, H(U)> (double backward, one merged hessian launch per pass)
+    against the reference hessian."""
     import torch
     import chompack_b200 as cp
     from chompack_b200 import grids, autograd
+    from oracle import ref
     A0 = grids.grid3d(side, seed=0)
     s = cp.symbolic(A0, p=cp.amd.order(A0), merge_function=cp.merge_size_fill(32, 32))
-    B = cp.batch([s] * value_sets, device=dev.index)
-    x0 = B.assemble([grids.grid3d(side, seed=v) for v in range(value_sets)])
-    x = x0.clone()
-    res = {}
+    xs = []
+    for v in range(value_sets):
+        xs.append((cp.cspmatrix(s, device=dev) + grids.grid3d(side, seed=v)).blkval)
+    x0 = torch.stack(xs)
 
     def fwd_bwd():
-        x.copy_(x0)
-        B.cholesky(x)
-        res["ld"] = B.logdet(x)
-        B.projected_inverse(x)
+        x = x0.detach().requires_grad_(True)
+        ld = autograd.logdet_values(x, s)
+        (g,) = torch.autograd.grad(ld.sum(), x)
+        return ld, g
     ms = _event_ms(dev, fwd_bwd, reps)
     fl = sweep_flops(s)
     flops = value_sets * (fl["cholesky"] + fl["projected_inverse"])
-    # checks on value set 0
-    X = cp.cspmatrix(s, blkval=x0[:int(s.blkptr[-1])].clone())
-    rng = np.random.default_rng(5)
-    U = cp.cspmatrix(s, blkval=torch.from_numpy(rng.standard_normal(int(s.blkptr[-1]))).to(dev))
+    # checks on value set 0 against the reference
+    xh = x0[0].cpu().numpy().copy()
+    Lr, Yr = reference_outputs(s, xh)
+    U = np.random.default_rng(6).standard_normal(xh.size)
+    ld, g = fwd_bwd()
+    gU = float((g[0] * torch.from_numpy(U).to(dev)).sum())
+    want = ref.dot(s, Yr.copy(), U.copy())
+    u = torch.from_numpy(U).to(dev)
+    fd = (float(autograd.logdet_values(x0[0] + h * u, s)) - float(autograd.logdet_values(x0[0] - h * u, s))) / (2 * h)
+    x = x0[:1].detach().requires_grad_(True)
+    (g1,) = torch.autograd.grad(autograd.logdet_values(x, s).sum(), x, create_graph=True)
+    (hv,) = torch.autograd.grad((g1 * u[None, :]).sum(), x)
+    second = float((hv[0] * u).sum())
+    Hu = U.copy()
+    ref.hessian(s, Lr, Yr, [Hu], adj=None, factored_updates=True)
+    second_ref = -ref.dot(s, U.copy(), Hu)
+    return {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(32,32), %d value sets through "
+                        "chompack_b200.autograd.logdet_values (torch.autograd.grad)" % (side, s.n, value_sets),
+            "fwd_bwd_ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1),
+            "launches": {"sweeps": 2, "kernels": 5,
+                         "note": "cholesky and projected_inverse engine launches for all value sets, log-det "
+                                 "reduction (2 kernels) and the gradient weights (1 kernel)"},
+            "gradient_rel_error_vs_reference": abs(gU - want) / abs(want),
+            "gradient_fd_rel_error": abs(gU - fd) / abs(fd), "fd_step": h,
+            "hvp_rel_error_vs_reference": abs(second - second_ref) / abs(second_ref)}
 
-    def ld_at(t):
-        return float(autograd.logdet_values(X.blkval + t * U.blkval, s))
-    Y = autograd.logdet_gradient(X)
-    g = cp.dot(Y, U)
-    fd = (ld_at(h) - ld_at(-h)) / (2 * h)
-    L = cp.cspmatrix(s, blkval=X.blkval.clone())
-    cp.cholesky(L)
-    HU = autograd.logdet_hvp(L, Y, U)
-    second = cp.dot(U, HU)
 
-    def g_at(t):
-        Xt = cp.cspmatrix(s, blkval=X.blkval + t * U.blkval)
-        return cp.dot(autograd.logdet_gradient(Xt), U)
-    fd2 = (g_at(1e-4) - g_at(-1e-4)) / 2e-4
-    return {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(32,32), %d value sets in one batch"
-                        % (side, s.n, value_sets),
-            "fwd_bwd_ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1), "launches": 2,
-            "gradient_fd_rel_error": abs(g - fd) / max(abs(fd), 1e-300),
-            "hvp_fd_rel_error": abs(second - fd2) / max(abs(fd2), 1e-300),
-            "fd_steps": [h, 1e-4]}
+# ------------------------------------------------------------------- main
+
+def _spawn(args):
+    """Start args.gpus ranks of this script under torch.distributed.run."""
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -430,9 +601,13 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        return _spawn(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit("bench.py: --gpus %d but WORLD_SIZE=%d" % (args.gpus, world))
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -450,7 +625,8 @@ def main():
     A, s = build_problem()
     fl = sweep_flops(s)
     ops = ["cholesky", "projected_inverse"]
-    step_flops = sum(fl[o] for o in ops)
+    cfg = bench_config(s)
+    step_flops = cfg["flops_per_step"]
     X0 = cp.cspmatrix(s, device=dev) + A
     Xw = X0.blkval.clone()
     plan = s.plan(local)
@@ -498,6 +674,9 @@ def main():
     clocks = sampler.stop()
     if world > 1:
         dist.barrier()
+    info = N.info(plan.handle, ws, sp)
+    if info != 0:
+        raise RuntimeError("sweep status %d (%s)" % (info, N.last_error().decode()))
     elapsed = t0.elapsed_time(t1) / 1e3
     kern = {op: float(np.mean([a.elapsed_time(b) for a, b in ev_k[op]])) / 1e3 for op in ops}
     # the job ends with the slowest rank (chompack_b200.shard, NCCL here)
@@ -505,6 +684,7 @@ def main():
     elapsed = shard.max_over_ranks(elapsed, device=dev)
     kern = {o: shard.max_over_ranks(kern[o], device=dev) for o in ops}
     value = step_flops * args.steps * world / elapsed / 1e9
+    Y_step = Xw.cpu().numpy()          # output of the last timed step (steps are bit-identical)
 
     # the other drop-in sweeps of the workload, timed alone after the step
     # loop (not part of the step): completion of the projected inverse the
@@ -514,6 +694,7 @@ def main():
     Yw = Xw.clone()
     Lw = X0.blkval.clone()
     launch["cholesky"](plan.handle, Lw.data_ptr(), ws, nbytes, sp)
+    L_gpu = Lw.cpu().numpy()
     Cw = torch.empty_like(Yw)
     reps = max(3, min(args.steps, 10))
     for name, op, k, src, call in () if not sweeps_other else (
@@ -559,7 +740,9 @@ def main():
         Bt = Bd.t().contiguous()   # column-major n x nrhs
         ms = timed(lambda: N.trsm(plan.handle, tr.encode(), nrhs, 1.0, Lw.data_ptr(), Bt.data_ptr(), s.n, wt, nbt, sp),
                    reps)
-        other["trsm_%s_nrhs%d" % (tr, nrhs)] = {"ms": round(ms, 4), "gflops": round(fl["trsm_rhs"] * nrhs / ms / 1e6, 3)}
+        fb = 8.0 * int(s.blkptr[-1]) + 16.0 * s.n * nrhs     # factor read once, B read and written
+        other["trsm_%s_nrhs%d" % (tr, nrhs)] = {"ms": round(ms, 4), "gflops": round(fl["trsm_rhs"] * nrhs / ms / 1e6, 3),
+                                                "achieved_gbs": round(fb / ms / 1e6, 1)}
     import ctypes
     Ud = Yw * torch.randn(Yw.shape, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(6))
     Uw = torch.empty_like(Ud)
@@ -567,6 +750,7 @@ def main():
     for fu in ((1, 0) if sweeps_other else ()):
         for a in (0, 1):
             plan.workspace(N.OP_HESSIAN, 1, a | fu << 2)
+
         def full_hessian():
             Uw.copy_(Ud)
             for a in (0, 1):   # adj = inv = False first, then adj toggled (the reference's adj=None)
@@ -583,6 +767,7 @@ def main():
     # runs, projected_inverse streams Y back out (its input, L, is already
     # on the device).  Host bytes per step: the values in, L and Y out.
     e2e = None
+    Y_e2e = None
     if not args.no_e2e:
         host_in = X0.blkval.cpu()
         bufs = [host_in.clone().pin_memory() for _ in range(2 + args.steps)]
@@ -596,23 +781,43 @@ def main():
             del X   # its device copy goes back to torch's cache for the next step
         torch.cuda.synchronize(dev)
         w = (time.perf_counter() - w0) / args.steps
-        nbytes = host_in.numel() * 8
-        e2e = {"value": round(step_flops / w / 1e9, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": 2 * nbytes, "ms_per_step": round(w * 1e3, 3),
+        w = shard.max_over_ranks(w, device=dev)
+        nb_in = host_in.numel() * 8
+        e2e = {"value": round(step_flops * world / w / 1e9, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": nb_in,
+               "d2h_bytes_per_step": 2 * nb_in, "ms_per_step": round(w * 1e3, 3),
                "path": "cbase.cholesky + cbase.projected_inverse on host-resident values (streamed chunks)"}
+        Y_e2e = bufs[-1].numpy()
+
+    # sharded batch section: every rank takes part (collectives inside)
+    batch_out = None
+    if not args.no_batch and not args.no_other:
+        try:
+            batch_out = batch_section(dev, rank, world)
+        except Exception as exc:  # reported beside the headline, never required
+            batch_out = {"unavailable": str(exc)}
 
     if rank == 0:
+        x0h = X0.blkval.cpu().numpy()
+        parity = None
+        try:
+            from oracle import workload
+            Lr, Yr = reference_outputs(s, x0h)
+            parity = {"rtol": RTOL, "against": "reference C kernels (oracle/_ref) on the same inputs",
+                      "cholesky": workload.block_errors(s, L_gpu, Lr),
+                      "projected_inverse": workload.block_errors(s, Y_step, Yr)}
+            if Y_e2e is not None:
+                parity["e2e_projected_inverse"] = workload.block_errors(s, Y_e2e, Yr)
+            parity["max_scaled_error"] = max(v for k, v in parity.items() if isinstance(v, float) and k != "rtol")
+            parity["pass"] = parity["max_scaled_error"] <= RTOL
+        except Exception as exc:  # the checker is reported, never required
+            parity = {"unavailable": str(exc)}
         peak = fp64_peak_tflops(dev)
-        na = np.diff(np.asarray(s.relptr)).astype(np.float64)
-        alg_bytes = int(16 * int(s.blkptr[-1]) + np.sum(16 * na * (na + 1) / 2))
+        alg_bytes = sweep_bytes(s)
         achieved = fl["cholesky"] / kern["cholesky"] / 1e12
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(elapsed / args.steps * 1e3, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": s.n, "nsn": s.Nsn, "sweeps": ops,
-                       "flops_per_step": step_flops, "l2": "inputs 246 MB > 126 MB L2; no flush",
-                       "parallelism": "replicas x%d" % world},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "gpu_launches": args.steps * len(ops),
             "roofline": {"bound": "tensor", "achieved": round(achieved, 3), "peak": round(peak, 3),
                          "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
@@ -623,6 +828,7 @@ def main():
                          "kernel": "chb::engine_kernel (cholesky)",
                          "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; MEASURED_PEAKS.json "
                                         "lists bf16 and HBM only)"},
+            "parity": parity,
             "kernel_ms": {o: round(kern[o] * 1e3, 4) for o in ops},
             "other_sweeps": other,
         }
@@ -630,20 +836,21 @@ def main():
             out["clocks"] = clocks
         if e2e:
             out["e2e"] = e2e
+        if batch_out is not None:
+            out["batch"] = batch_out
         if not args.no_mixed and not args.no_other:
             try:
                 out["mixed_precision"] = mixed_precision_section(dev)
             except Exception as exc:  # reported beside the headline, never required
                 out["mixed_precision"] = {"unavailable": str(exc)}
         if not args.no_batch and not args.no_other:
-            for key, fn in (("batch", batch_section), ("autograd", autograd_section)):
-                try:
-                    out[key] = fn(dev)
-                except Exception as exc:  # reported beside the headline, never required
-                    out[key] = {"unavailable": str(exc)}
+            try:
+                out["autograd"] = autograd_section(dev)
+            except Exception as exc:  # reported beside the headline, never required
+                out["autograd"] = {"unavailable": str(exc)}
         if not args.no_cpu:
             try:
-                out["cpu_baseline"] = cpu_baseline(s, A)
+                out["cpu_baseline"] = cpu_baseline(s, x0h)
             except Exception as exc:  # the baseline is reported, never required
                 out["cpu_baseline"] = {"unavailable": str(exc)}
         print(json.dumps(out))

@@ -21,7 +21,13 @@ application.  All three run as the package's CUDA sweeps; torch only holds
 the tensors and the autograd graph.
 
 A leading batch dimension of value sets on one pattern (values of shape
-(B, blkptr[Nsn])) is supported; each value set is swept on its own.
+(B, blkptr[Nsn])) runs every sweep over all B value sets in ONE launch: a
+merged plan over B copies of the clique tree (chompack_b200.batch), cached
+on the symbolic object, with per-set log dets from a segmented reduction.
+
+What the backward keeps is the factor L (the size of X per value set), not
+the fronts or update matrices of the forward sweep: the projected inverse
+needs only L, so no front has to be checkpointed or recomputed.
 """
 import torch
 
@@ -99,15 +105,65 @@ class _Logdet(torch.autograd.Function):
         return g * _LogdetGrad.apply(x, Lv, ctx.symb), None
 
 
+def _value_sets(symb, count, device):
+    """Merged plan over `count` copies of symb's clique tree (cached)."""
+    from .batch import batch
+    cache = symb.__dict__.setdefault("_value_set_batches", {})
+    key = (int(count), int(device.index))
+    if key not in cache:
+        cache[key] = batch([symb] * int(count), device=device.index)
+    return cache[key]
+
+
+class _LogdetGradBatch(torch.autograd.Function):
+    """x (B, nv) -> w .* P(X_b^{-1}) for every value set, given the factors."""
+
+    @staticmethod
+    def forward(ctx, x, L, symb):
+        Bt = _value_sets(symb, x.shape[0], x.device)
+        Y = L.reshape(-1).clone()
+        Bt.projected_inverse(Y)
+        ctx.save_for_backward(L, Y)
+        ctx.symb = symb
+        return Bt.sym_weight(Y).reshape(x.shape)
+
+    @staticmethod
+    def backward(ctx, c):
+        L, Y = ctx.saved_tensors
+        Bt = _value_sets(ctx.symb, L.shape[0], L.device)
+        U = c.detach().to(torch.float64).reshape(-1).contiguous().clone()
+        Bt.hessian(L.reshape(-1), Y, U, adj=None)
+        return Bt.sym_weight(U, -1.0).reshape(L.shape), None, None
+
+
+class _LogdetBatch(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, symb):
+        Bt = _value_sets(symb, x.shape[0], x.device)
+        L = x.detach().reshape(-1).clone()
+        Bt.cholesky(L)
+        L = L.reshape(x.shape)
+        ctx.save_for_backward(x, L)
+        ctx.symb = symb
+        return Bt.logdet(L.reshape(-1))
+
+    @staticmethod
+    def backward(ctx, g):
+        x, L = ctx.saved_tensors
+        return g[:, None] * _LogdetGradBatch.apply(x, L, ctx.symb), None
+
+
 def logdet_values(x, symb):
     """log det of the chordal SPD matrix with block values x (1-D, or
-    (B, n_values) for B value sets on `symb`'s pattern), differentiable
-    (first and second order)."""
+    (B, n_values) for B value sets on `symb`'s pattern, swept together),
+    differentiable (first and second order)."""
     if not isinstance(x, torch.Tensor) or x.device.type != "cuda" or x.dtype != torch.float64:
         raise ValueError("values must be a float64 CUDA tensor")
     if x.dim() == 1:
         return _Logdet.apply(x, symb)
-    return torch.stack([_Logdet.apply(x[b], symb) for b in range(x.shape[0])])
+    if x.dim() != 2 or x.shape[1] != int(symb.blkptr[-1]):
+        raise ValueError("batched values must have shape (B, %d)" % int(symb.blkptr[-1]))
+    return _LogdetBatch.apply(x.contiguous(), symb)
 
 
 def logdet(X):

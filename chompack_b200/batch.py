@@ -114,6 +114,39 @@ class batch(object):
         if self._run(N.OP_COMPLETION, lambda w, nb, s: N.completion(h, values.data_ptr(), fu, w, nb, s), k=fu):
             raise ArithmeticError("completion failed")
 
+    def hessian(self, factor_values, pinv_values, u_values, adj=None, inv=False, factored_updates=True):
+        """Hessian factors of every matrix's log-det barrier applied in place
+        to one direction per matrix (u_values, the batch layout): the modes
+        of cbase.hessian, adj=None the full H_X(U) (two passes), one launch
+        per pass for the whole batch."""
+        for v in (factor_values, pinv_values, u_values):
+            self._check_values(v)
+        import ctypes
+        inv_i = 1 if inv is True else 0
+        adj_i = inv_i if adj is None else (1 if adj is True else 0)
+        fu = 1 if factored_updates is True else 0
+        h = self.plan.handle
+        arr = (ctypes.c_void_p * 1)(u_values.data_ptr())
+        info = 0
+        for a in ([adj_i, 1 ^ adj_i] if adj is None else [adj_i]):
+            info |= self._run(N.OP_HESSIAN,
+                              lambda w, nb, s: N.hessian(h, factor_values.data_ptr(), pinv_values.data_ptr(), arr, 1,
+                                                         a, inv_i, fu, w, nb, s),
+                              k=1, flags=a | inv_i << 1 | fu << 2)
+        if info:
+            raise ArithmeticError("hessian failed")
+
+    def sym_weight(self, values, alpha=1.0):
+        """alpha * w .* values with the weights of `dot` (2 below the
+        diagonal, 1 on it, 0 in the strict upper part of a diagonal block),
+        for every matrix: a new tensor."""
+        self._check_values(values)
+        out = torch.empty_like(values)
+        rc = N.sym_weight(self.plan.handle, values.data_ptr(), out.data_ptr(), float(alpha), _stream(self.device))
+        if rc < 0:
+            raise RuntimeError("sym_weight failed: %s" % N.last_error().decode())
+        return out
+
     # ------------------------------------------------------------ reductions
     def logdet(self, factor_values):
         """log det of every matrix from its factor: a (count,) tensor."""

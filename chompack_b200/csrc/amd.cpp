@@ -12,6 +12,18 @@
 // max(16, 10*sqrt(n)), and a final postorder of the assembly tree that places
 // the child with the largest front last).  The quotient graph lives in one
 // integer workspace with in-place garbage collection.
+//
+// Credit and licence.  Reproducing cvxopt's permutation exactly means taking
+// the same steps in the same order as SuiteSparse AMD's implementation, so
+// the structure of this file follows that implementation (the elimination
+// loop of AMD_2 in amd_2.c and the tree postorder of amd_post_tree.c), and
+// several of its helper names (EMPTY, FLIP, clear_flag, post_tree) are
+// SuiteSparse's.  SuiteSparse AMD is Copyright (c) 1996-2023 Timothy A.
+// Davis, Patrick R. Amestoy and Iain S. Duff, and is distributed under the
+// BSD-3-Clause licence; this file is a derivative work under those terms.
+// Redistribution must retain that copyright notice and the licence's
+// conditions and disclaimer; the names of the copyright holders may not be
+// used to endorse products derived from this software without permission.
 #include <cstdint>
 #include <cmath>
 #include <vector>

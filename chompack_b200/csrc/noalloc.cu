@@ -1,14 +1,16 @@
 // Allocation-free variant of the Cholesky sweep.
 //
 // Some callers cannot call cudaMalloc at the point where they need a
-// factorisation: code running while a CUDA graph is being captured, code
-// inside a framework that owns all device memory through its own pool, or
-// a host process that must not grow its device footprint after start-up.
-// chb_cholesky_noalloc serves them: everything the sweep needs on the device
-// besides the caller's values (control words, task counters, the uploaded
-// symbolic data, the task program and the workspace) lives in one file-scope
-// __device__ array of CHB_NOALLOC_SCRATCH_BYTES, which every GPU that loads
-// this library holds until the process exits.
+// factorisation: a framework whose device memory all comes from its own pool
+// and that forbids allocations behind its back, or a host process that must
+// not grow its device footprint after start-up (a fixed memory budget agreed
+// with the other jobs on the GPU).  chb_cholesky_noalloc serves them:
+// everything the sweep needs on the device besides the caller's values
+// (control words, task counters, the uploaded symbolic data, the task program
+// and the workspace) lives in one file-scope __device__ array of
+// CHB_NOALLOC_SCRATCH_BYTES, which every GPU that loads this library holds
+// until the process exits.  The call is synchronous: it waits for the sweep
+// and reads its status back, as chb_cholesky followed by chb_info does.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -27,13 +29,16 @@ namespace {
 constexpr int MAX_DEVICES = 64;
 unsigned char* g_scratch_addr[MAX_DEVICES];  // device address of the array, per device
 int g_scratch_grid[MAX_DEVICES];
+// Held for the whole of every call: host threads of one process that call
+// concurrently take turns instead of interleaving their staging copies into
+// the shared array.  Other processes, and other streams of this process that
+// launch work which overlaps a call, are not covered.
 std::mutex g_scratch_mu;
 
-// Once per device, with that device current: look up the array's device
-// address (the host-side symbol is only a stand-in) and prepare the kernel's
-// launch shape.  Nothing here allocates.
+// Once per device, with that device current and g_scratch_mu held: look up
+// the array's device address (the host-side symbol is only a stand-in) and
+// prepare the kernel's launch shape.  Nothing here allocates.
 int setup_device(int dev) {
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
   if (g_scratch_addr[dev]) return 0;
   void* p = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -63,6 +68,7 @@ extern "C" int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream
   if (dev < 0 || dev >= MAX_DEVICES) return set_error(-3, "device %d out of range", dev);
   if (plan->device >= 0 && plan->device != dev)
     return set_error(-3, "plan is bound to device %d but device %d is current", plan->device, dev);
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
   int rc = setup_device(dev);
   if (rc) return rc;
   Program* prog = build_host_program(plan, CHB_OP_CHOLESKY, 0, 0);

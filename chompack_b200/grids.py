@@ -11,7 +11,7 @@ import numpy as np
 
 from .sparse import spmatrix
 
-__all__ = ["grid2d", "grid3d", "grid2d_extra", "random_lower", "spd_from_lower_pattern"]
+__all__ = ["grid2d", "grid3d", "grid2d_extra", "random_lower", "spd_from_lower_pattern", "uneven_batch_specs"]
 
 
 def spd_from_lower_pattern(n, I, J, seed):
@@ -98,3 +98,11 @@ def random_lower(n, density, seed=0, diag=None):
         V[d] = diag
         A = spmatrix(V, A._I, A._J, A.size)
     return A
+
+
+def uneven_batch_specs(count=256, seed=2024, lo=20, hi=120):
+    """(side, seed) of each matrix of the batched workload: `count` 2-D grids
+    with sides drawn uniformly from lo..hi (numpy default_rng(seed)); matrix i
+    is grid2d_extra(side_i, seed=1000 + i)."""
+    sides = np.random.default_rng(seed).integers(lo, hi + 1, size=count)
+    return [(int(sd), 1000 + i) for i, sd in enumerate(sides)]

@@ -264,18 +264,21 @@ int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
 int chb_plan_set_schedule(chb_plan* plan, int mode);
 
 /* Allocation-free Cholesky.  No counterpart in the reference: an addition for
- * callers that cannot call cudaMalloc when they factor (code running under
- * CUDA graph capture, frameworks whose device memory all comes from their own
- * pool, processes that must not grow their device footprint after start-up).
- * Same result as chb_cholesky, but all device scratch comes from one static
- * __device__ array of CHB_NOALLOC_SCRATCH_BYTES (32 MiB) that every GPU which
- * loads this library holds until the process exits; problems that need more
- * are rejected with error -40 and a message giving the size.  The plan may be
- * host-only (device < 0).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current: make that
- * first call before any stream capture.  The call is synchronous and returns
- * the status like chb_info.  Every call shares the one array, so calls that
- * overlap on the GPU (other streams, other host threads) race: serialise them. */
+ * callers that cannot call cudaMalloc when they factor (frameworks whose
+ * device memory all comes from their own pool and that forbid allocations
+ * behind their back, processes that must not grow their device footprint
+ * after start-up).  Same result as chb_cholesky, but all device scratch comes
+ * from one static __device__ array of CHB_NOALLOC_SCRATCH_BYTES (32 MiB) that
+ * every GPU which loads this library holds until the process exits; problems
+ * that need more are rejected with error -40 and a message giving the size.
+ * The plan may be host-only (device < 0).  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current.  The call is synchronous: it waits for the sweep on `stream` and
+ * returns its status like chb_info.  It always runs the static list order
+ * (chb_plan_set_schedule does not apply) and writes no trace (chb_set_trace
+ * does not apply).  Every call shares the one array: calls from host threads
+ * of one process take turns on an internal lock, but work of another stream
+ * or process that overlaps a call on the GPU races with it: serialise it. */
 #define CHB_NOALLOC_SCRATCH_BYTES (32u << 20)
 int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream);
 

@@ -173,7 +173,17 @@ def main():
         lines.append("scalars %d %d %d %d" % (sr.n, sr.Nsn, sr.nnz, sr.clique_number))
         with open(os.path.join(HERE, "grid3d_40_m32.sha256"), "w") as f:
             f.write("\n".join(lines) + "\n")
-        print("grid3d_40_m32 digests written")
+        # the arrays themselves, compact (int32 fits every entry), for the
+        # benchmark's reference leg: it runs the reference kernels on them
+        # without loading the product library (oracle/workload.py)
+        mem = sr.memory
+        np.savez_compressed(
+            os.path.join(HERE, "grid3d_40_m32_symbolic.npz"),
+            scalars=np.array([sr.n, sr.Nsn, sr.nnz, sr.clique_number], dtype=np.int64),
+            memory=np.array([mem["stack_depth"], mem["stack_mem"], mem["frontal_mem"], mem["stack_solve"]],
+                            dtype=np.int64),
+            **{a: np.array(list(getattr(sr, a)), dtype=np.int32) for a in SYMB_ARRAYS})
+        print("grid3d_40_m32 digests and arrays written")
 
 
 if __name__ == "__main__":
