@@ -86,6 +86,7 @@ sym_weight = _sig("chb_sym_weight", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_doubl
 info = _sig("chb_info", ctypes.c_int, [PPLAN, vp, vp])
 set_trace = _sig("chb_set_trace", ctypes.c_int, [PPLAN, vp, i64])
 plan_set_schedule = _sig("chb_plan_set_schedule", ctypes.c_int, [PPLAN, ctypes.c_int])
+plan_set_spin_limit = _sig("chb_plan_set_spin_limit", ctypes.c_int, [PPLAN, i64])
 io_flags = _sig("chb_io_flags", ctypes.c_int, [ctypes.c_int, ctypes.c_int])
 io_overlap_available = _sig("chb_io_overlap_available", ctypes.c_int, [])
 precision_flags = _sig("chb_precision_flags", ctypes.c_int, [ctypes.c_int])
@@ -99,5 +100,22 @@ projected_inverse_io = _sig("chb_projected_inverse_io", ctypes.c_int, [PPLAN, vp
 llt_io = _sig("chb_llt_io", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 program_io = _sig("chb_program_io", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64, vp, vp, vp, vp])
 
-OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT, OP_TRMM = range(8)
+OP_CHOLESKY, OP_LLT, OP_PROJECTED_INVERSE, OP_COMPLETION, OP_HESSIAN, OP_TRSM, OP_DOT, OP_TRMM, OP_CONVENTIONAL = range(9)
 HESSIAN_MAX_U = 59   # U matrices per chb_hessian call (base slots 5..63)
+
+# ---- product-form Cholesky factor (chb_pftrf / chb_pfsv / chb_pfmv)
+pf_workspace_size = _sig("chb_pf_workspace_size", ctypes.c_int, [i64, i64, ctypes.POINTER(ctypes.c_size_t)])
+pftrf = _sig("chb_pftrf", ctypes.c_int, [i64, i64, vp, vp, i64, vp, i64, vp, i64, vp, ctypes.c_size_t, vp])
+pfsv = _sig("chb_pfsv", ctypes.c_int, [i64, i64, ctypes.c_char, vp, i64, vp, i64, vp, i64, vp, i64, i64, vp,
+                                       ctypes.c_size_t, vp])
+pfmv = _sig("chb_pfmv", ctypes.c_int, [i64, i64, ctypes.c_char, vp, i64, vp, i64, vp, i64, vp, i64, i64, vp,
+                                       ctypes.c_size_t, vp])
+pf_info = _sig("chb_pf_info", ctypes.c_int, [vp, vp])
+
+# ---- block exports and element-wise updates (csrc/export.cu, build_conventional.cpp)
+factor_conventional = _sig("chb_factor_conventional", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
+lower_ccs = _sig("chb_lower_ccs", ctypes.c_int, [PPLAN, vp, vp, vp, vp, vp, vp, vp])
+syr2 = _sig("chb_syr2", ctypes.c_int, [PPLAN, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, vp])
+add_projection = _sig("chb_add_projection", ctypes.c_int, [PPLAN, vp, vp, vp, vp, i64, ctypes.c_double,
+                                                           ctypes.c_double, ctypes.c_int, vp])
+diag = _sig("chb_diag", ctypes.c_int, [PPLAN, vp, vp, vp])

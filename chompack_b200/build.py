@@ -52,16 +52,24 @@ def build(force=False, verbose=False):
             and os.path.getmtime(OUT) >= max(os.path.getmtime(f) for f in srcs + hdr + [__file__])):
         return OUT
     os.makedirs(BUILD, exist_ok=True)
+    newest_hdr = max([os.path.getmtime(f) for f in hdr + [__file__]])
+
+    def stale(src, obj):
+        # an object is rebuilt when its source, any header or this script is newer
+        return force or verbose or not os.path.exists(obj) or \
+            os.path.getmtime(obj) < max(os.path.getmtime(src), newest_hdr)
     objs = []
     for f in cpp:
         o = os.path.join(BUILD, os.path.basename(f) + ".o")
-        _run(["g++"] + CXXFLAGS + ["-c", f, "-o", o])
+        if stale(f, o):
+            _run(["g++"] + CXXFLAGS + ["-c", f, "-o", o])
         objs.append(o)
     for f in cu:
         o = os.path.join(BUILD, os.path.basename(f) + ".o")
-        out = _run([NVCC] + NVFLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", f, "-o", o])
-        if verbose:
-            sys.stdout.write(out)
+        if stale(f, o):
+            out = _run([NVCC] + NVFLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", f, "-o", o])
+            if verbose:
+                sys.stdout.write(out)
         objs.append(o)
     tmp = OUT + ".tmp"
     _run([NVCC, "-shared"] + ARCH + ["-o", tmp] + objs + ["-lcudart"])

@@ -20,7 +20,8 @@ import torch
 
 from . import _native as N
 
-__all__ = ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot"]
+__all__ = ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot", "pfchol",
+           "pftrsm", "pftrmm"]
 
 
 def _on_host(X):
@@ -380,3 +381,111 @@ def hessian(L, Y, U, adj=False, inv=False, factored_updates=True):
         _write_back(u)
     if info:
         raise ArithmeticError("hessian failed")
+
+
+# ------------------------------------------------------- product-form factor
+# cbase.pfchol / pftrsm / pftrmm (cbase.c:859-942) over the GPU kernels of
+# csrc/pf.cu.  V, L, B and U are n x k (n x nrhs) column-major float64: CUDA
+# tensors with stride(0) == 1 (transformed in place on the device) or
+# Fortran-ordered numpy arrays (copied to the current device and back).
+
+def _dense_on_device(M, name, dev=None):
+    """(tensor, host array or None, rows, cols, ld) of a column-major block."""
+    import numpy as np
+    if isinstance(M, torch.Tensor):
+        if M.device.type != "cuda" or M.dtype != torch.float64:
+            raise ValueError("%s must be a float64 CUDA tensor" % name)
+        if dev is not None and M.device != dev:
+            raise ValueError("%s must be on %s" % (name, dev))
+        if M.dim() == 1:
+            return M, None, M.shape[0], 1, max(1, M.shape[0])
+        if M.dim() != 2 or (M.shape[0] > 1 and M.stride(0) != 1):
+            raise ValueError("%s must be column-major (stride(0) == 1)" % name)
+        return M, None, M.shape[0], M.shape[1], max(1, M.stride(1) if M.shape[1] > 1 else M.shape[0])
+    host = np.asarray(M)
+    if host.dtype != np.float64:
+        raise ValueError("%s must be float64" % name)
+    if host.ndim > 2 or (host.ndim == 2 and not host.flags["F_CONTIGUOUS"]):
+        raise ValueError("%s must be column-major (Fortran order)" % name)
+    d = dev if dev is not None else torch.device("cuda", torch.cuda.current_device())
+    rows = host.shape[0]
+    cols = 1 if host.ndim == 1 else host.shape[1]
+    return torch.from_numpy(host.reshape(-1, order="F")).to(d), host, rows, cols, max(1, rows)
+
+
+def _copy_back(t, host):
+    if host is not None:
+        out = t.cpu().numpy()
+        if host.ndim == 1:
+            host[:] = out
+        else:
+            host[:, :] = out.reshape(host.shape, order="F")
+
+
+def _pf_workspace(n, ncols, dev):
+    sz = ctypes.c_size_t()
+    with torch.cuda.device(dev):
+        _check(N.pf_workspace_size(int(n), int(ncols), ctypes.byref(sz)), "pf_workspace_size")
+    buf = torch.empty(sz.value + 256, dtype=torch.uint8, device=dev)
+    return buf, (buf.data_ptr() + 255) // 256 * 256, sz.value
+
+
+def _pf_status(ws, dev):
+    info = N.pf_info(ws, _stream(dev))
+    if info < -1:
+        raise RuntimeError("product-form sweep failed: %s" % N.last_error().decode())
+    return info
+
+
+def pfchol(alpha, V, L, B):
+    """Product-form Cholesky factorisation of I + V diag(alpha) V^T
+    (cbase.c:862-880 / dpftrf): V (n x k) is overwritten, L and B receive
+    the factors.  ArithmeticError when the matrix is not positive definite."""
+    Vt, Vh, n, k, ldv = _dense_on_device(V, "V")
+    dev = Vt.device
+    Lt, Lh, nl, kl, ldl = _dense_on_device(L, "L", dev)
+    Bt, Bh, nb, kb, ldb = _dense_on_device(B, "B", dev)
+    if (nl, kl) != (n, k) or (nb, kb) != (n, k):
+        raise ValueError("V, L and B must have the same size")
+    a = torch.as_tensor(alpha, dtype=torch.float64).reshape(-1).to(dev).contiguous()
+    if a.numel() < k:
+        raise ValueError("alpha must have at least k entries")
+    buf, ws, nbytes = _pf_workspace(n, k, dev)
+    with torch.cuda.device(dev):
+        _check(N.pftrf(n, k, a.data_ptr(), Vt.data_ptr(), ldv, Lt.data_ptr(), ldl, Bt.data_ptr(), ldb, ws, nbytes,
+                       _stream(dev)), "pftrf")
+        info = _pf_status(ws, dev)
+    for t, h in ((Vt, Vh), (Lt, Lh), (Bt, Bh)):
+        _copy_back(t, h)
+    if info:
+        raise ArithmeticError("factorization failed")
+
+
+def _pf_apply(fn, what, V, L, B, U, trans):
+    if trans not in ('N', 'T'):
+        raise ValueError("trans must be 'N' or 'T'")
+    Vt, _, n, k, ldv = _dense_on_device(V, "V")
+    dev = Vt.device
+    Lt, _, _, _, ldl = _dense_on_device(L, "L", dev)
+    Bt, _, _, _, ldb = _dense_on_device(B, "B", dev)
+    Ut, Uh, nu, nrhs, ldu = _dense_on_device(U, "U", dev)
+    if nu != n:
+        raise ValueError("U must have n rows")
+    buf, ws, nbytes = _pf_workspace(n, nrhs, dev)
+    with torch.cuda.device(dev):
+        _check(fn(n, k, trans.encode(), Vt.data_ptr(), ldv, Lt.data_ptr(), ldl, Bt.data_ptr(), ldb, Ut.data_ptr(),
+                  ldu, nrhs, ws, nbytes, _stream(dev)), what)
+        _pf_status(ws, dev)
+    _copy_back(Ut, Uh)
+
+
+def pftrsm(V, L, B, U, trans='N'):
+    """U := (L_1...L_k)^{-1} U ('N') or (L_k^T...L_1^T)^{-1} U ('T'), in place
+    (cbase.c:885-911 / dpfsv)."""
+    _pf_apply(N.pfsv, "pfsv", V, L, B, U, trans)
+
+
+def pftrmm(V, L, B, U, trans='N'):
+    """U := L_1...L_k U ('N') or L_k^T...L_1^T U ('T'), in place
+    (cbase.c:916-942 / dpfmv)."""
+    _pf_apply(N.pfmv, "pfmv", V, L, B, U, trans)

@@ -16,6 +16,16 @@ from .sparse import as_spmatrix, spmatrix, symmetrize, tril
 __all__ = ["cspmatrix"]
 
 
+def _symbolic_arrays(symb, dev):
+    """sncolptr / snrowidx of a symbolic factorisation on a device (cached)."""
+    cache = symb.__dict__.setdefault("_sym_dev", {})
+    key = str(dev)
+    if key not in cache:
+        cache[key] = (torch.as_tensor(np.asarray(symb.sncolptr), dtype=torch.int64).to(dev),
+                      torch.as_tensor(np.asarray(symb.snrowidx), dtype=torch.int64).to(dev))
+    return cache[key]
+
+
 def _default_device():
     return torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else torch.device("cpu")
 
@@ -166,64 +176,81 @@ class cspmatrix(object):
 
     def add_projection(self, A, alpha=1.0, beta=1.0, reordered=False):
         """X := alpha*proj(A) + beta*X for a dense symmetric A
-        (symbolic.py:1176-1210)."""
+        (symbolic.py:1176-1210), on the values' device (chb_add_projection):
+        every entry of every block is updated; with reordered=False the
+        symmetric matrix of A's lower triangle is read through p."""
         assert self.is_factor is False, "cannot project matrix onto a cspmatrix factor"
+        from . import _native as N
+        from . import cbase
         s = self.symb
-        A = np.asarray(A.cpu().numpy() if isinstance(A, torch.Tensor) else A, dtype=np.float64)
-        if not reordered:
-            At = np.tril(A)
-            At = At + At.T
-            At[np.diag_indices_from(At)] *= 0.5
-            A = At[np.ix_(s.p, s.p)]
-        host = self.blkval.detach().to("cpu").numpy().copy()
-        for k in range(s.Nsn):
-            rows = s.snrowidx[s.sncolptr[k]:s.sncolptr[k + 1]]
-            cols = s.snode[s.snptr[k]:s.snptr[k + 1]]
-            blk = A[np.ix_(rows, cols)].reshape(-1, order="F")
-            host[s.blkptr[k]:s.blkptr[k + 1]] = beta * host[s.blkptr[k]:s.blkptr[k + 1]] + alpha * blk
-        self.blkval.copy_(torch.from_numpy(host))
+        v = cbase._values(self)
+        dev = v.device
+        At = A if isinstance(A, torch.Tensor) else torch.from_numpy(np.asarray(A, dtype=np.float64))
+        At = At.to(device=dev, dtype=torch.float64)
+        if At.dim() != 2 or tuple(At.shape) != (s.n, s.n):
+            raise ValueError("A must be a dense %d x %d matrix" % (s.n, s.n))
+        Acm = At.t().contiguous()                      # column-major storage of A
+        colptr, rowidx = _symbolic_arrays(s, dev)
+        plan = s.plan(dev.index)
+        rc = N.add_projection(plan.handle, v.data_ptr(), colptr.data_ptr(), rowidx.data_ptr(), Acm.data_ptr(), s.n,
+                              float(alpha), float(beta), 0 if reordered else 1, torch.cuda.current_stream(dev).cuda_stream)
+        if rc < 0:
+            raise RuntimeError("add_projection failed: %s" % N.last_error().decode())
+        cbase._write_back(self)
 
-    def _lower_entries(self, blk):
-        """(I, J, V) of the reordered lower triangle stored in blk (host)."""
+    def _ccs(self, values):
+        """(colptr, row indices, values) of the lower trapezoid of the blocks
+        in compressed-column order (reordered numbering), gathered on the
+        device (chb_lower_ccs); the symbolic parts are cached on symb."""
+        from . import _native as N
         s = self.symb
-        Is, Js, Vs = [], [], []
-        nn = np.diff(s.snptr)
-        for k in range(s.Nsn):
-            nj = int(s.sncolptr[k + 1] - s.sncolptr[k])
-            rows = s.snrowidx[s.sncolptr[k]:s.sncolptr[k + 1]]
-            b = blk[s.blkptr[k]:s.blkptr[k + 1]].reshape((nj, int(nn[k])), order="F")
-            for i in range(int(nn[k])):
-                Is.append(rows[i:])
-                Js.append(np.full(nj - i, s.snptr[k] + i, dtype=np.int64))
-                Vs.append(b[i:, i])
-        if not Is:
-            z = np.zeros(0, dtype=np.int64)
-            return z, z, np.zeros(0)
-        return np.concatenate(Is), np.concatenate(Js), np.concatenate(Vs)
+        dev = values.device
+        cache = s.__dict__.setdefault("_ccs_cache", {})
+        key = str(dev)
+        nn = np.diff(np.asarray(s.snptr))
+        nj = np.diff(np.asarray(s.sncolptr))
+        if key not in cache:
+            # column j = snptr[k] + i holds nj_k - i entries
+            cc = np.repeat(nj, nn) - (np.arange(s.n) - np.repeat(np.asarray(s.snptr)[:-1], nn))
+            cp = np.concatenate([[0], np.cumsum(cc)]).astype(np.int64)
+            cache[key] = [torch.from_numpy(cp).to(dev), cp, None]
+        cp_d, cp, rows = cache[key]
+        sncolptr, snrowidx = _symbolic_arrays(s, dev)
+        vals = torch.empty(int(cp[-1]), dtype=torch.float64, device=dev)
+        ri = torch.empty(int(cp[-1]), dtype=torch.int64, device=dev) if rows is None else None
+        plan = s.plan(dev.index)
+        rc = N.lower_ccs(plan.handle, values.data_ptr(), sncolptr.data_ptr(), snrowidx.data_ptr(), cp_d.data_ptr(),
+                         vals.data_ptr(), None if ri is None else ri.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+        if rc < 0:
+            raise RuntimeError("lower_ccs failed: %s" % N.last_error().decode())
+        if rows is None:
+            rows = ri.cpu().numpy()
+            cache[key][2] = rows
+        return cp, rows, vals.cpu().numpy()
 
     def spmatrix(self, reordered=True, symmetric=False):
         """Convert to a sparse matrix (symbolic.py:1032-1111).  For a factor
-        the off-diagonal blocks are multiplied back by L_kk to give the
-        conventional lower-triangular factor; only the default options are
-        allowed then."""
+        the off-diagonal blocks are multiplied back by L_kk on the device
+        (chb_factor_conventional) to give the conventional lower-triangular
+        factor; only the default options are allowed then.  The lower
+        trapezoid is gathered on the device (chb_lower_ccs) and only the
+        nonzeros cross to the host."""
+        from . import _native as N
+        from . import cbase
         s = self.symb
-        blk = self.blkval.detach().to("cpu").numpy().copy()
         if self.is_factor:
             if symmetric:
                 raise ValueError("'symmetric = True' not implemented for Cholesky factors")
             if not reordered:
                 raise ValueError("'reordered = False' not implemented for Cholesky factors")
-            for k in range(s.Nsn):
-                nn = int(s.snptr[k + 1] - s.snptr[k])
-                na = int(s.relptr[k + 1] - s.relptr[k])
-                if na == 0:
-                    continue
-                nj = nn + na
-                b = blk[s.blkptr[k]:s.blkptr[k + 1]].reshape((nj, nn), order="F").copy()
-                Lkk = np.tril(b[:nn, :nn])
-                b[nn:, :] = b[nn:, :] @ Lkk
-                blk[s.blkptr[k]:s.blkptr[k + 1]] = b.reshape(-1, order="F")
-        I, J, V = self._lower_entries(blk)
+        v = cbase._values(self, "L" if self.is_factor else "X")
+        if self.is_factor:
+            v = v.clone()
+            plan = s.plan(v.device.index)
+            cbase._run_and_status(plan, N.OP_CONVENTIONAL,
+                                  lambda ws, nb, st: N.factor_conventional(plan.handle, v.data_ptr(), ws, nb, st))
+        cp, I, V = self._ccs(v)
+        J = np.repeat(np.arange(s.n, dtype=np.int64), np.diff(cp))
         tmp = spmatrix(V, I, J, (s.n, s.n))
         if reordered:
             return symmetrize(tmp) if symmetric else tmp
@@ -233,13 +260,16 @@ class cspmatrix(object):
         return out if symmetric else tril(out)
 
     def diag(self, reordered=True):
-        """Diagonal entries (symbolic.py:1113-1128), as a numpy array."""
+        """Diagonal entries (symbolic.py:1113-1128), gathered on the device
+        (chb_diag), as a numpy array."""
+        from . import _native as N
+        from . import cbase
         s = self.symb
-        blk = self.blkval.detach().to("cpu").numpy()
-        D = np.zeros(s.n)
-        for k in range(s.Nsn):
-            nn = int(s.snptr[k + 1] - s.snptr[k])
-            w = int(s.sncolptr[k + 1] - s.sncolptr[k])
-            for i in range(nn):
-                D[s.snode[s.snptr[k] + i]] = blk[s.blkptr[k] + i * w + i]
+        v = cbase._values(self, "L" if self.is_factor else "X")
+        dev = v.device
+        d = torch.empty(s.n, dtype=torch.float64, device=dev)
+        rc = N.diag(s.plan(dev.index).handle, v.data_ptr(), d.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+        if rc < 0:
+            raise RuntimeError("diag failed: %s" % N.last_error().decode())
+        D = d.cpu().numpy()
         return D if reordered else D[s.ip]

@@ -89,6 +89,12 @@ extern "C" int chb_cholesky(chb_plan* plan, double* blkval, void* work, size_t w
   return run_op(plan, CHB_OP_CHOLESKY, 0, 0, bases, 1, work, work_bytes, stream);
 }
 
+extern "C" int chb_factor_conventional(chb_plan* plan, double* blkval, void* work, size_t work_bytes,
+                                       void* stream) {
+  double* bases[1] = {blkval};
+  return run_op(plan, CHB_OP_CONVENTIONAL, 0, 0, bases, 1, work, work_bytes, stream);
+}
+
 extern "C" int chb_projected_inverse(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream) {
   double* bases[1] = {blkval};
   return run_op(plan, CHB_OP_PROJECTED_INVERSE, 0, 0, bases, 1, work, work_bytes, stream);

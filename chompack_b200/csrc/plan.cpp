@@ -142,6 +142,7 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, flags != 0); break;
     case CHB_OP_TRMM: rc = build_trmm(*plan, *prog, k, flags != 0); break;
     case CHB_OP_HESSIAN: rc = build_hessian(*plan, *prog, (int)k, flags); break;
+    case CHB_OP_CONVENTIONAL: rc = build_conventional(*plan, *prog); break;
     default: rc = set_error(-2, "operation %d is not available", op); break;
   }
   if (rc != 0) return nullptr;
@@ -155,7 +156,8 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   // run faster in static list order (a CTA already waits on the next task;
   // trmm has the solve's structure and takes its schedule);
   // the other sweeps gain from running whichever task is ready.
-  prog->static_default = op == CHB_OP_CHOLESKY || op == CHB_OP_LLT || op == CHB_OP_TRSM || op == CHB_OP_TRMM;
+  prog->static_default = op == CHB_OP_CHOLESKY || op == CHB_OP_LLT || op == CHB_OP_TRSM || op == CHB_OP_TRMM ||
+                         op == CHB_OP_CONVENTIONAL;
   Program* p = prog.get();
   plan->progs[key] = std::move(prog);
   return p;
@@ -231,7 +233,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.fronts = plan->d_fronts;
   ra.relidx = plan->d_relidx;
   ra.chidx = plan->d_chidx;
-  ra.spin_limit = 40000000LL;  // about 10 s of polling at the longest back-off
+  ra.spin_limit = plan->spin_limit >= 0 ? plan->spin_limit : kDefaultSpinLimit;
   ra.trace = (plan->trace && plan->trace_cap >= (int64_t)prog->tasks.size()) ? plan->trace : nullptr;
   ra.perm = plan->d_perm;
   ra.ldb = run_ldb;
@@ -600,6 +602,13 @@ extern "C" int chb_plan_set_schedule(chb_plan* plan, int mode) {
   if (!plan) return set_error(-1, "null plan");
   if (mode < -1 || mode > 1) return set_error(-2, "schedule mode must be -1, 0 or 1");
   plan->schedule = mode;
+  return 0;
+}
+
+extern "C" int chb_plan_set_spin_limit(chb_plan* plan, int64_t polls) {
+  clear_error();
+  if (!plan) return set_error(-1, "null plan");
+  plan->spin_limit = polls < 0 ? -1 : polls;
   return 0;
 }
 

@@ -98,6 +98,7 @@ struct chb_plan {
   int64_t* d_seg = nullptr;
   int grid = 0;                 // persistent grid size
   int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
+  int64_t spin_limit = -1;      // polls before a wait gives up; -1: the default (kDefaultSpinLimit)
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;
@@ -127,6 +128,9 @@ struct HostIo {
 
 // Program flags selecting the streamed variants (bits above the sweeps' own
 // flags).
+// Polls of a task's wait (with a back-off of up to ~1 us) before it gives
+// up and the sweep ends with status -30: about 10 s.
+constexpr int64_t kDefaultSpinLimit = 40000000LL;
 constexpr int PF_IO_IN = 1 << 16;
 constexpr int PF_IO_OUT = 1 << 17;
 // Program flags selecting the mixed-precision variants of cholesky and
@@ -161,6 +165,7 @@ cudaError_t dot_launch(const double* x, const double* y, const FrontDesc* fronts
 int build_cholesky(const chb_plan& P, Program& prog);
 int build_projected_inverse(const chb_plan& P, Program& prog);
 int build_llt(const chb_plan& P, Program& prog);
+int build_conventional(const chb_plan& P, Program& prog);
 int build_completion(const chb_plan& P, Program& prog, bool factored);
 int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans);
 int build_trmm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans);

@@ -35,12 +35,8 @@ def _device_index(symb):
 
 def _sym_arrays(symb, dev):
     """sncolptr / snrowidx of the symbolic on the device (cached)."""
-    cache = symb.__dict__.setdefault("_sym_dev", {})
-    key = str(dev)
-    if key not in cache:
-        cache[key] = (torch.as_tensor(symb.sncolptr, dtype=torch.int64).to(dev),
-                      torch.as_tensor(symb.snrowidx, dtype=torch.int64).to(dev))
-    return cache[key]
+    from .cspmatrix import _symbolic_arrays
+    return _symbolic_arrays(symb, dev)
 
 
 def _as_columns(B, dev):

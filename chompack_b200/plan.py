@@ -103,6 +103,12 @@ class Plan(object):
         code = {None: -1, "dynamic": 0, "static": 1}[mode]
         N.check(N.plan_set_schedule(self.handle, code), "plan_set_schedule")
 
+    def set_spin_limit(self, polls=None):
+        """Bound of every wait inside this plan's sweeps, in polls (None:
+        the default, about 10 s); a wait that runs out ends the sweep with
+        status -30 (RuntimeError from the sweeps)."""
+        N.check(N.plan_set_spin_limit(self.handle, -1 if polls is None else int(polls)), "plan_set_spin_limit")
+
     def program_info(self, op, k=0, flags=0):
         info = (ctypes.c_int64 * 8)()
         N.check(N.program_info(self.handle, op, int(k), int(flags), info), "program_info")

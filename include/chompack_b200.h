@@ -85,7 +85,8 @@ enum chb_op {
   CHB_OP_HESSIAN = 4,
   CHB_OP_TRSM = 5,
   CHB_OP_DOT = 6,
-  CHB_OP_TRMM = 7
+  CHB_OP_TRMM = 7,
+  CHB_OP_CONVENTIONAL = 8
 };
 
 /* Device workspace (bytes) an operation needs; `k` is nrhs for CHB_OP_TRSM
@@ -209,6 +210,71 @@ int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const doubl
 int chb_trmm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
              int64_t ldB, void* work, size_t work_bytes, void* stream);
 
+/* Conventional factor — the block products of cspmatrix.spmatrix() on a
+ * factor (symbolic.py:1052-1068): every off-diagonal block W = L_{Ak,Nk}
+ * L_kk^{-1} that chb_cholesky leaves (cholesky.c:72) becomes W L_kk, in
+ * place.  Workspace chb_workspace_size(plan, CHB_OP_CONVENTIONAL, 0, 0, ...). */
+int chb_factor_conventional(chb_plan* plan, double* blkval, void* work, size_t work_bytes, void* stream);
+
+/* Element-wise block operations (Python loops over supernodes in the
+ * reference).  sncolptr / snrowidx are the symbolic's arrays (int64) in
+ * device memory; all vectors and matrices are device memory.
+ * chb_lower_ccs — the lower trapezoid of every block in compressed-column
+ *   order (cspmatrix.spmatrix(), symbolic.py:1071-1098): colptr (n+1, column
+ *   j of supernode k has nj - (j - snptr[k]) entries) gives where each column
+ *   goes; values and, unless NULL, row indices (reordered numbering) are
+ *   written.
+ * chb_syr2 — X := alpha P(u v^T + v u^T) + beta X on the lower trapezoid of
+ *   every block (base.py:28-67); u, v are n-vectors in the original
+ *   numbering (gathered through p) unless `reordered`.
+ * chb_add_projection — X := alpha P(A) + beta X for a dense column-major A
+ *   (lda >= n) on every entry of every block (symbolic.py:1176-1210):
+ *   symmetric_original != 0 reads the symmetric matrix of A's lower triangle
+ *   through p (the reference's reordered=False), else A[r, c] in the
+ *   reordered numbering.
+ * chb_diag — the n diagonal entries in the reordered numbering
+ *   (symbolic.py:1113-1128). */
+int chb_lower_ccs(chb_plan* plan, const double* blkval, const int64_t* sncolptr, const int64_t* snrowidx,
+                  const int64_t* colptr, double* values, int64_t* rowidx, void* stream);
+int chb_syr2(chb_plan* plan, double* blkval, const int64_t* sncolptr, const int64_t* snrowidx, const double* u,
+             const double* v, double alpha, double beta, int reordered, void* stream);
+int chb_add_projection(chb_plan* plan, double* blkval, const int64_t* sncolptr, const int64_t* snrowidx,
+                       const double* A, int64_t lda, double alpha, double beta, int symmetric_original,
+                       void* stream);
+int chb_diag(chb_plan* plan, const double* blkval, double* d, void* stream);
+
+/* Product-form Cholesky factor of I + V diag(a) V^T = L_1...L_k L_k^T...L_1^T
+ * (V n x k), each L_i held as column i of V, L and B (pfcholesky.c:52-136;
+ * the reference's pfcholesky class composes them with the chordal factor,
+ * pfcholesky.py:113-211).  All arrays are column-major device memory with
+ * the given leading dimensions (>= max(1, n)).  Each call is one launch on
+ * `stream` into a caller-provided workspace of chb_pf_workspace_size(n,
+ * ncols) bytes (256-byte aligned; ncols = k for chb_pftrf, nrhs for the
+ * others), and its status comes back from chb_pf_info(work, stream).
+ *
+ * chb_pftrf — dpftrf (pfcholesky.c:52-88, wrapper cbase.pfchol cbase.c:862-880):
+ *   a (k device doubles), V overwritten as dpftrf does, L and B written.
+ *   chb_pf_info returns -1 when 1 - alpha v^2 <= 0 for some row (the
+ *   reference's return value; cbase raises ArithmeticError); the contents of
+ *   V, L and B are then unspecified.
+ * chb_pfsv — dpfsv (:90-112) on each of the nrhs columns of U (cbase.pftrsm
+ *   cbase.c:885-911): U := (L_1...L_k)^{-1} U ('N') or (L_k^T...L_1^T)^{-1} U ('T').
+ * chb_pfmv — dpfmv (:114-136) on each column of U (cbase.pftrmm
+ *   cbase.c:916-942): U := L_1...L_k U ('N') or L_k^T...L_1^T U ('T'). */
+int chb_pf_workspace_size(int64_t n, int64_t ncols, size_t* bytes);
+int chb_pftrf(int64_t n, int64_t k, const double* a, double* V, int64_t ldv, double* L, int64_t ldl, double* B,
+              int64_t ldb, void* work, size_t work_bytes, void* stream);
+int chb_pfsv(int64_t n, int64_t k, char trans, const double* V, int64_t ldv, const double* L, int64_t ldl,
+             const double* B, int64_t ldb, double* U, int64_t ldu, int64_t nrhs, void* work, size_t work_bytes,
+             void* stream);
+int chb_pfmv(int64_t n, int64_t k, char trans, const double* V, int64_t ldv, const double* L, int64_t ldl,
+             const double* B, int64_t ldb, double* U, int64_t ldu, int64_t nrhs, void* work, size_t work_bytes,
+             void* stream);
+/* Synchronise `stream` and return the status of the last product-form call
+ * that used `work`: 0, -1 (dpftrf: not positive definite), or -30 when a
+ * grid-wide wait of the kernel ran out. */
+int chb_pf_info(void* work, void* stream);
+
 /* dot — dot.c:3-23 (wrapper cbase.c:106-174).  Writes <X,Y> to result (one
  * device double). */
 int chb_dot(chb_plan* plan, const double* x, const double* y, double* result, void* work,
@@ -262,6 +328,13 @@ int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
  * static for cholesky, llt and trsm and dynamic for the others).  Both give
  * bit-identical results. */
 int chb_plan_set_schedule(chb_plan* plan, int mode);
+
+/* Bound of every wait inside the plan's sweeps: a task's wait on its
+ * dependencies, on an incoming chunk or for ready work gives up after
+ * `polls` polls (with a back-off of up to ~1 us each); the sweep then ends
+ * early and chb_info returns -30.  polls < 0 restores the default (about
+ * 10 s of polling).  Small values are for tests of that failure path. */
+int chb_plan_set_spin_limit(chb_plan* plan, int64_t polls);
 
 /* Allocation-free Cholesky.  No counterpart in the reference: an addition for
  * callers that cannot call cudaMalloc when they factor (frameworks whose

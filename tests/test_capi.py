@@ -66,3 +66,16 @@ def test_trsm_and_trmm_reject_bad_arguments_before_touching_the_device():
     t_ws = pl.program_info(N.OP_TRMM, k=3, flags=1)["ws_doubles"]
     na = np.diff(np.asarray(s.relptr)).sum()
     assert t_ws == 3 * (s.n + na) and n_ws == 3 * (s.n + 2 * na)
+
+
+def test_product_form_entry_points_reject_bad_arguments_before_touching_the_device():
+    """chb_pfsv / chb_pfmv / chb_pftrf validate trans and the leading
+    dimensions on the host (no CUDA call), like cbase.pftrsm's ValueError."""
+    from chompack_b200 import _native as N
+    for fn in (N.pfsv, N.pfmv):
+        assert fn(10, 2, b"X", None, 10, None, 10, None, 10, None, 10, 1, None, 0, None) < 0
+        assert "trans" in N.last_error().decode()
+        assert fn(10, 2, b"N", 16, 9, 16, 10, 16, 10, 16, 10, 1, None, 0, None) < 0   # never dereferenced
+        assert "leading" in N.last_error().decode()
+    assert N.pftrf(10, 2, None, None, 10, None, 10, None, 10, None, 0, None) < 0
+    assert N.pftrf(-1, 2, None, None, 10, None, 10, None, 10, None, 0, None) < 0

@@ -95,19 +95,3 @@ def test_trmm_then_trsm_is_the_identity():
         bases = {0: L.copy(), 1: np.full(prog.ws_doubles, np.nan), 4: Xf}
         taskvm.VM(prog, bases, s.relidx, s.chidx, perm=s.p, ldb=s.n, alpha=0.5).run("random", seed=7)
         assert np.max(np.abs(Xf.reshape(B0.shape, order="F") - B0)) <= 1e-11 * np.max(np.abs(B0))
-
-
-@pytest.mark.parametrize("name", NAMES)
-def test_factor_export_is_the_dense_factor(name):
-    """cspmatrix.spmatrix() of a factor (symbolic.py:1032-1111: off-diagonal
-    blocks multiplied back by L_kk) equals the oracle's dense factor, the
-    matrix trmm(L, I)[p, p] gives in the reference's own test."""
-    import torch
-    d, A, s = G.load(name)
-    L = d["ref_cholesky"]
-    X = cp.cspmatrix(s, blkval=torch.from_numpy(L.copy()), factor=True)
-    S = X.spmatrix(reordered=True)
-    D = np.zeros((s.n, s.n))
-    D[np.asarray(S._I), np.asarray(S._J)] = np.asarray(S._V)
-    Ld = OT.dense_factor(s, L)
-    assert np.max(np.abs(D - Ld)) <= 1e-13 * np.max(np.abs(Ld))
