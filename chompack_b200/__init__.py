@@ -26,6 +26,7 @@ from .batch import batch  # noqa: E402,F401
 from . import mixed  # noqa: E402,F401
 from .pfcholesky import pfcholesky  # noqa: E402,F401
 from .base import syr2  # noqa: E402,F401
+from .completions import psdcompletion, mrcompletion  # noqa: E402,F401
 
 __all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot", "autograd", "batch",
-            "pfcholesky", "syr2"]
+            "pfcholesky", "syr2", "psdcompletion", "mrcompletion"]

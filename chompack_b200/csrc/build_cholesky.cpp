@@ -53,9 +53,21 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   }
   prog.ws_doubles = ws;
 
-  std::vector<int> uc_group(N, -1);
+  // small subtrees: one warp per range, four ranges per task; the parent of
+  // a range's root waits on the whole task (utask)
+  const Bundles bd = make_bundles(P);
+  std::vector<int> uc_group(N, -1), utask(N, -1);
   for (int64_t k = 0; k < N; k++)
-    if (P.fronts[k].na > 0) uc_group[k] = B.new_group();
+    if (P.fronts[k].na > 0 && bd.of[k] < 0) uc_group[k] = B.new_group();
+  for (size_t b = 0; b < bd.tasks.size(); b++) {
+    const int r0 = bd.roots[b].front();
+    int id = B.add(bundle_task(P, bd, (int)b, T_SUBTREE), {P.fronts[r0].level, -1, 0, r0, 0, 0}, -1, bd.cost[b]);
+    for (int r : bd.roots[b]) utask[r] = id;
+  }
+  auto wait_child = [&](int id, int c) {
+    if (utask[c] >= 0) B.wait_task(id, utask[c]);
+    else B.wait_group(id, uc_group[c]);
+  };
 
   // a dependency on a task's end, or on an early-signal group
   struct Dep {
@@ -85,6 +97,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     auto bw = [&](int c) { return std::min(T, nn - c * T); };  // column block width
     auto bh = [&](int i) { return std::min(T, na - i * T); };  // bottom tile height
 
+    if (bd.of[k] >= 0) continue;  // inside a small-subtree bundle
     // A front that fits one tile is one task: extend-add, partial Cholesky
     // and Schur complement in shared memory (cholesky.c:33-72 for one node).
     if (nj <= small_nj) {
@@ -96,7 +109,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       t.c = opnd(B_WS, upd, std::max(na, 1));
       const double est = 3.0 + 0.02 * nn * (double)nj + 0.002 * (double)nj * nj;
       int id = B.add(t, {lv, -1, 0, (int)k, 0, 0}, uc_group[k], est);
-      for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
+      for (int l = f.chbeg; l < f.chend; l++) wait_child(id, P.chidx[l]);
       continue;
     }
 
@@ -129,7 +142,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         // modelled cost (list order): w / 1000 gave cholesky 6.51 ms at 40^3
         // against 6.55 ms for w / 2000
         int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group, 3.0 + w / 1000.0);
-        for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, uc_group[P.chidx[l]]);
+        for (int l = f.chbeg; l < f.chend; l++) wait_child(id, P.chidx[l]);
         j0 = j1;
       }
     }

@@ -62,9 +62,38 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     else B.wait_group(id, vready[k]);
   };
 
+  // small subtrees: one warp per range, four ranges per task, each task
+  // added once the parents of all its roots are (their V_k), parents first
+  const Bundles bd = make_bundles(P);
+  std::vector<std::pair<int64_t, int>> pending;  // (smallest parent of a root, bundle)
+  for (size_t b = 0; b < bd.tasks.size(); b++) {
+    int64_t m = N;
+    for (int r : bd.roots[b]) {
+      const int p = P.fronts[r].parent;
+      if (p != r && p >= 0 && p < N) m = std::min<int64_t>(m, p);
+    }
+    pending.push_back({m, (int)b});
+  }
+  std::sort(pending.begin(), pending.end(), [](const std::pair<int64_t, int>& x, const std::pair<int64_t, int>& y) {
+    return x.first > y.first || (x.first == y.first && x.second < y.second);
+  });
+  size_t next_bundle = 0;
+  auto emit_bundles = [&](int64_t k) {  // every bundle whose roots' parents are all above k
+    for (; next_bundle < pending.size() && pending[next_bundle].first > k; next_bundle++) {
+      const int b = pending[next_bundle].second;
+      const int r0 = bd.roots[b].back();
+      Task t = bundle_task(P, bd, b, T_PSUBTREE);
+      int id = B.add(t, {P.nlevels - P.fronts[r0].level, 0, 0, r0, 0, 0}, -1, 1.5 * bd.cost[b]);
+      for (int r : bd.roots[b])
+        if (P.fronts[r].na > 0) wait_v(id, r);
+    }
+  };
+
   const int maxlv = P.nlevels;
   std::vector<int> inv, last_mrow;
   for (int64_t k = N - 1; k >= 0; k--) {
+    emit_bundles(k);
+    if (bd.of[k] >= 0) continue;  // inside a small-subtree bundle
     const FrontDesc& f = P.fronts[k];
     const int nn = f.nn, na = f.na, nj = f.nj;
     const int lv = maxlv - f.level;  // roots first
@@ -258,6 +287,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     }
   }
   prog.ws_doubles = ws;
+  emit_bundles(-1);
   return B.finish(prog, P.grid > 0 ? P.grid : 296);
 }
 

@@ -12,6 +12,7 @@
 #include <numeric>
 #include <queue>
 #include <string>
+#include <array>
 #include <vector>
 
 #include "engine.h"
@@ -119,6 +120,12 @@ struct DagBuilder {
       if (j >= 0 && j + 1 < (int)io.in_off.size() && std::find(out.begin(), out.end(), j) == out.end())
         out.push_back(j);
     };
+    if (t.op == T_SUBTREE || t.op == T_PSUBTREE) {  // every chunk of [a.off, b.off)
+      const auto& v = io.in_off;
+      int j = (int)(std::upper_bound(v.begin(), v.end(), t.a.off) - v.begin()) - 1;
+      for (j = std::max(j, 0); j + 1 < (int)v.size() && v[j] < t.b.off; j++) out.push_back(j);
+      return;
+    }
     for (const Operand* o : {&t.a, &t.b, &t.c})
       if (o->base == B_X && o->ld > 0) add_off(o->off);
     if (t.op == T_MROW && t.aux[0] == B_X) add_off((int64_t)(uint32_t)t.aux[2] | ((int64_t)t.aux[3] << 32));
@@ -142,6 +149,10 @@ struct DagBuilder {
     };
     switch (t.op) {
       case T_NOP: case T_SIGNAL: case T_ARRIVAL: case T_EXTRACT: break;  // an extract writes the workspace
+      case T_SUBTREE:  // the blocks of its ranges, within [a.off, b.off)
+      case T_PSUBTREE:
+        add_range(t.a.off, t.b.off);
+        break;
       case T_FRONT:  // the front's whole nj x nn block (its update matrices are workspace)
       case T_PFRONT:
         if (t.a.base == B_X && t.a.ld > 0) add_range(t.a.off, t.a.off + (int64_t)t.m * t.n);
@@ -661,6 +672,105 @@ inline SplitTask add_split_gemm(DagBuilder& B, const Task& t, int kc, int64_t sc
   st.out = B.add(s, key, group, 2.0 + 0.4 * p);
   for (int id : st.parts) B.wait_task(st.out, id);
   return st;
+}
+
+// Small-subtree bundles (T_SUBTREE / T_PSUBTREE).  A subtree qualifies when
+// every front in it has nj <= SUB_NJ (and the small-front tasks are on);
+// the maximal ones are cut into warp ranges (adjacent subtrees in postorder
+// merged up to a modelled cost), four ranges per task.  CHB_NO_SUBTREES
+// turns bundling off (every small front is then its own T_FRONT / T_PFRONT).
+struct Bundles {
+  // per task: up to four inclusive ranges [lo, hi] (lo < 0: no range)
+  std::vector<std::array<int, 8>> tasks;
+  std::vector<int> of;      // supernode -> bundle index, or -1
+  std::vector<double> cost; // modelled duration of each bundle (us): its longest range
+  std::vector<std::vector<int>> roots;  // per bundle: the supernodes whose parent lies outside it
+};
+
+inline double bundle_front_us(const FrontDesc& f) {
+  // measured order of magnitude of one warp's front: a fixed part for the
+  // loads, pivots and stores, plus the O(nj^2 nn) arithmetic
+  return 0.4 + 0.002 * (double)f.nj * f.nj + 0.0004 * (double)f.nj * f.nj * f.nn;
+}
+
+inline Bundles make_bundles(const chb_plan& P) {
+  Bundles out;
+  const int64_t N = P.nsn;
+  out.of.assign(N, -1);
+  if (std::getenv("CHB_NO_SUBTREES") != nullptr || small_front_nj() < SUB_NJ || N == 0) return out;
+  std::vector<char> all(N, 1);
+  std::vector<int> size(N, 1);
+  for (int64_t k = 0; k < N; k++) {
+    const FrontDesc& f = P.fronts[k];
+    if (f.nj > SUB_NJ) all[k] = 0;
+    const int p = f.parent;
+    if (p != k && p >= 0 && p < N) {
+      all[p] = all[p] && all[k];
+      size[p] += size[k];
+    }
+  }
+  // warp ranges: maximal qualifying subtrees in postorder, adjacent ones merged
+  const double cap_us = 24.0;
+  std::vector<std::array<int, 2>> ranges;
+  std::vector<double> rcost;
+  for (int64_t k = 0; k < N; k++) {
+    const int p = P.fronts[k].parent;
+    const bool root = all[k] && (p == k || p < 0 || p >= N || !all[p]);
+    if (!root) continue;
+    const int lo = (int)(k - size[k] + 1);
+    double c = 0.0;
+    for (int64_t q = lo; q <= k; q++) c += bundle_front_us(P.fronts[q]);
+    if (!ranges.empty() && ranges.back()[1] + 1 == lo && rcost.back() + c <= cap_us) {
+      ranges.back()[1] = (int)k;
+      rcost.back() += c;
+    } else {
+      ranges.push_back({lo, (int)k});
+      rcost.push_back(c);
+    }
+  }
+  for (size_t r0 = 0; r0 < ranges.size(); r0 += 4) {
+    std::array<int, 8> t;
+    t.fill(-1);
+    double c = 0.0;
+    const int b = (int)out.tasks.size();
+    out.roots.emplace_back();
+    for (size_t w = 0; w < 4 && r0 + w < ranges.size(); w++) {
+      t[2 * w] = ranges[r0 + w][0];
+      t[2 * w + 1] = ranges[r0 + w][1];
+      c = std::max(c, rcost[r0 + w]);
+      for (int q = ranges[r0 + w][0]; q <= ranges[r0 + w][1]; q++) {
+        out.of[q] = b;
+        const int p = P.fronts[q].parent;
+        if (p == q || p < 0 || p >= N || p > ranges[r0 + w][1]) out.roots[b].push_back(q);
+      }
+    }
+    out.tasks.push_back(t);
+    out.cost.push_back(c);
+  }
+  return out;
+}
+
+// The task of bundle b: op T_SUBTREE or T_PSUBTREE; operands a / b carry the
+// [first, end) offsets of the values the bundle touches (for the streamed
+// programs' chunk bookkeeping; the device code does not read them).
+inline Task bundle_task(const chb_plan& P, const Bundles& bd, int b, uint8_t op) {
+  Task t = make_task(op);
+  const std::array<int, 8>& r = bd.tasks[b];
+  for (int w = 0; w < 4; w++) t.aux[w] = r[2 * w];
+  t.m = r[1];
+  t.n = r[3];
+  t.k = r[5];
+  t.cdiag = r[7];
+  int64_t lo = INT64_MAX, hi = 0;
+  for (int w = 0; w < 4; w++)
+    if (r[2 * w] >= 0) {
+      lo = std::min<int64_t>(lo, P.fronts[r[2 * w]].blk);
+      const FrontDesc& l = P.fronts[r[2 * w + 1]];
+      hi = std::max<int64_t>(hi, l.blk + (int64_t)l.nj * l.nn);
+    }
+  t.a = opnd(B_X, lo, 1);
+  t.b = opnd(B_X, hi, 1);
+  return t;
 }
 
 }  // namespace chb

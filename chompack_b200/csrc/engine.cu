@@ -1988,6 +1988,178 @@ __device__ void run_vec(const RunArgs& ra, const Task& t) {
 }
 
 // ---------------------------------------------------------------- kernel
+// ------------------------------------------------------------ bundles
+// Small-subtree bundles.  A T_SUBTREE / T_PSUBTREE task carries up to four
+// ranges of supernodes, one per warp: warp w owns [aux[w], bundle_last(t, w)]
+// (aux[w] < 0: idle).  Each range is a union of complete subtrees,
+// contiguous in postorder, whose fronts all have nj <= SUB_NJ, so a range
+// needs nothing from outside but, for projected_inverse, its roots' V_k.
+// The warp processes its fronts alone (cholesky in postorder, projected
+// inverse parents first), one row of the front per lane, in its own
+// shared-memory matrices (row-major, stride SUB_LD).  The update matrices
+// inside a range pass through the workspace at their usual offsets and are
+// written and read by the same warp (ordered by __syncwarp); the parents of
+// a range's roots wait on the whole task.  Arithmetic and summation orders
+// are those of the one-front tasks (T_FRONT / T_PFRONT).
+__device__ __forceinline__ int bundle_last(const Task& t, int w) {
+  return w == 0 ? t.m : w == 1 ? t.n : w == 2 ? t.k : t.cdiag;
+}
+
+// cholesky.c:33-72 for one front of at most SUB_NJ rows, by one warp.
+__device__ void chol_front_warp(const RunArgs& ra, int k, double* F, int lane) {
+  const FrontDesc f = ra.fronts[k];
+  const int nn = f.nn, na = f.na, nj = f.nj;
+  double* __restrict__ X = ra.bases[B_X] + f.blk;
+  double* __restrict__ W = ra.bases[B_WS];
+  double* row = F + lane * SUB_LD;
+  if (lane < nj)
+    for (int c = 0; c < nj; c++) row[c] = (c < nn && lane >= c) ? __ldcg(X + (int64_t)c * nj + lane) : 0.0;
+  __syncwarp();
+  // extend-add, children last to first (the reference's stack order)
+  for (int l = f.chend - 1; l >= f.chbeg; l--) {
+    const FrontDesc ch = ra.fronts[ra.chidx[l]];
+    const int Nc = ch.na;
+    const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
+    const double* __restrict__ Uc = W + ch.upd;
+    if (lane < Nc) {
+      double* dst = F + __ldg(rr + lane) * SUB_LD;
+      for (int q = 0; q <= lane; q++) dst[__ldg(rr + q)] += __ldcg(Uc + (int64_t)q * Nc + lane);
+    }
+    __syncwarp();
+  }
+  // partial Cholesky of the nn pivot columns; the trailing block becomes U_k
+  int first_bad = -1;
+  for (int j = 0; j < nn; j++) {
+    const double d = F[j * SUB_LD + j];
+    const bool bad = !(d > 0.0);
+    if (bad && first_bad < 0) first_bad = j;
+    const double lj = sqrt(bad ? 1.0 : d), rl = 1.0 / lj;
+    double a = 0.0;
+    if (lane > j && lane < nj) {
+      a = row[j] * rl;
+      row[j] = a;
+    }
+    __syncwarp();
+    if (lane == j) row[j] = lj;
+    if (lane > j && lane < nj)
+      for (int c = j + 1; c <= lane; c++) row[c] -= a * F[c * SUB_LD + j];
+    __syncwarp();
+  }
+  if (lane == 0 && first_bad >= 0) atomicCAS(&ra.ctl[2], 0, first_bad + 1);
+  // separator rows: L21 L11^{-1}, the reference's off-diagonal layout (:72)
+  if (lane >= nn && lane < nj)
+    for (int j = nn - 1; j >= 0; j--) {
+      double v = row[j];
+      for (int l2 = j + 1; l2 < nn; l2++) v -= row[l2] * F[l2 * SUB_LD + j];
+      row[j] = v / F[j * SUB_LD + j];
+    }
+  __syncwarp();
+  for (int c = 0; c < nn; c++)
+    if (lane >= c && lane < nj) X[(int64_t)c * nj + lane] = row[c];
+  double* __restrict__ U = W + f.upd;
+  for (int q = 0; q < na; q++)
+    if (lane >= nn + q && lane < nj) U[(int64_t)q * na + (lane - nn)] = row[nn + q];
+  __syncwarp();
+}
+
+// projected_inverse.c:33-73 for one front of at most SUB_NJ rows, by one
+// warp: G holds L11, then M = L11^{-1}, then S21; F holds [W, V_k], then
+// [Y11; S21 | V_k].
+__device__ void pinv_front_warp(const RunArgs& ra, int k, double* G, double* F, int lane) {
+  const FrontDesc f = ra.fronts[k];
+  const int nn = f.nn, na = f.na, nj = f.nj;
+  double* __restrict__ X = ra.bases[B_X] + f.blk;
+  double* __restrict__ W = ra.bases[B_WS];
+  const double* __restrict__ V = W + f.upd;
+  if (lane < nj)
+    for (int c = 0; c < nn; c++) {
+      const double v = __ldcg(X + (int64_t)c * nj + lane);
+      if (lane < nn) G[lane * SUB_LD + c] = (lane >= c) ? v : 0.0;
+      else F[lane * SUB_LD + c] = v;
+    }
+  if (lane < na)
+    for (int q = 0; q <= lane; q++) F[(nn + lane) * SUB_LD + nn + q] = __ldcg(V + (int64_t)q * na + lane);
+  __syncwarp();
+  // M = L11^{-1} in place, columns last to first
+  int first_bad = -1;
+  for (int j = nn - 1; j >= 0; j--) {
+    const double d = G[j * SUB_LD + j];
+    if (d == 0.0 && first_bad < 0) first_bad = j;
+    const double ajj = 1.0 / (d == 0.0 ? 1.0 : d);
+    double ti = 0.0;
+    if (lane > j && lane < nn)
+      for (int l = j + 1; l <= lane; l++) ti = fma(G[lane * SUB_LD + l], G[l * SUB_LD + j], ti);
+    __syncwarp();
+    if (lane > j && lane < nn) G[lane * SUB_LD + j] = -ajj * ti;
+    if (lane == j) G[j * SUB_LD + j] = ajj;
+    __syncwarp();
+  }
+  if (lane == 0 && first_bad >= 0) atomicCAS(&ra.ctl[2], 0, first_bad + 1);
+  // Y11 = M^T M (lower part), rows < nn of F
+  if (lane < nn)
+    for (int j = 0; j <= lane; j++) {
+      double v = 0.0;
+      for (int l = lane; l < nn; l++) v = fma(G[l * SUB_LD + lane], G[l * SUB_LD + j], v);
+      F[lane * SUB_LD + j] = v;
+    }
+  __syncwarp();
+  if (na > 0) {
+    // S21 = -V_k W (V_k read as symmetric from its lower part) into G
+    if (lane < na)
+      for (int j = 0; j < nn; j++) {
+        double v = 0.0;
+        for (int l = 0; l < na; l++) {
+          const double vil = (lane >= l) ? F[(nn + lane) * SUB_LD + nn + l] : F[(nn + l) * SUB_LD + nn + lane];
+          v = fma(vil, F[(nn + l) * SUB_LD + j], v);
+        }
+        G[lane * SUB_LD + j] = -v;
+      }
+    __syncwarp();
+    // Y11 -= S21^T W
+    if (lane < nn)
+      for (int j = 0; j <= lane; j++) {
+        double v = 0.0;
+        for (int l = 0; l < na; l++) v = fma(G[l * SUB_LD + lane], F[(nn + l) * SUB_LD + j], v);
+        F[lane * SUB_LD + j] -= v;
+      }
+    __syncwarp();
+    if (lane < na)
+      for (int j = 0; j < nn; j++) F[(nn + lane) * SUB_LD + j] = G[lane * SUB_LD + j];
+    __syncwarp();
+  }
+  // the children's updates F(r_c, r_c), lower parts
+  for (int l = f.chbeg; l < f.chend; l++) {
+    const FrontDesc ch = ra.fronts[ra.chidx[l]];
+    const int Nc = ch.na;
+    const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
+    double* __restrict__ Uc = W + ch.upd;
+    if (lane < Nc) {
+      const double* src = F + __ldg(rr + lane) * SUB_LD;
+      for (int q = 0; q <= lane; q++) Uc[(int64_t)q * Nc + lane] = src[__ldg(rr + q)];
+    }
+  }
+  for (int c = 0; c < nn; c++)
+    if (lane < nj) X[(int64_t)c * nj + lane] = (lane < nn && lane < c) ? 0.0 : F[lane * SUB_LD + c];
+  __syncwarp();
+}
+
+__device__ void run_subtrees(const RunArgs& ra, const Task& t, double* smem) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lo = t.aux[warp];
+  if (lo < 0) return;
+  const int hi = bundle_last(t, warp);
+  if (t.op == T_SUBTREE) {
+    double* F = smem + warp * SUB_NJ * SUB_LD;
+    for (int k = lo; k <= hi; k++) chol_front_warp(ra, k, F, lane);
+  } else {
+    double* G = smem + warp * 2 * SUB_NJ * SUB_LD;
+    for (int k = hi; k >= lo; k--) pinv_front_warp(ra, k, G, G + SUB_NJ * SUB_LD, lane);
+  }
+}
+
+static_assert(NTHREADS == 128, "a bundle has one range per warp of a 4-warp CTA");
+static_assert(8 * SUB_NJ * SUB_LD <= ENGINE_SMEM_BASE_DOUBLES, "bundle fronts exceed the engine's shared memory");
+
 __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   extern __shared__ double smem[];
   __shared__ int s_task;
@@ -2086,6 +2258,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_ASM: run_asm(ra, t, smem); break;
       case T_FRONT: run_front(ra, t, smem); break;
       case T_PFRONT: run_pfront(ra, t, smem); break;
+      case T_SUBTREE:
+      case T_PSUBTREE: run_subtrees(ra, t, smem); break;
       case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t); break;

@@ -23,6 +23,10 @@ namespace chb {
 
 constexpr int TILE = 64;          // tile edge (rows/cols of a C tile)
 constexpr int NTHREADS = 128;     // threads per CTA (4 warps)
+// Fronts of a small-subtree bundle (T_SUBTREE / T_PSUBTREE) have at most
+// SUB_NJ rows: one row per lane of the warp that owns the range.
+constexpr int SUB_NJ = 32;
+constexpr int SUB_LD = SUB_NJ + 1;     // row stride of a warp's shared-memory front
 constexpr int KC = 16;            // K chunk staged through shared memory
 constexpr int LDS = TILE + 4;     // padded leading dimension of staged tiles
 constexpr int MAX_BASES = 64;     // base-pointer slots (see Base below)
@@ -80,7 +84,9 @@ enum TaskOp : uint8_t {
   T_SIGNAL = 13,  // host-visible flag io_out[aux[0]] = 1 (a chunk of the values is final)
   T_ARRIVAL = 14, // waits (bounded) until the host's copy raised io_in[aux[0]] (a chunk arrived)
   T_FRONT = 15,   // a whole small cholesky front (nj <= TILE) in shared memory (front aux[0])
-  T_PFRONT = 16   // a whole small projected-inverse front (nj <= TILE) in shared memory (front aux[0])
+  T_PFRONT = 16,  // a whole small projected-inverse front (nj <= TILE) in shared memory (front aux[0])
+  T_SUBTREE = 17, // cholesky of up to four ranges of small complete subtrees, one per warp (see bundle_last)
+  T_PSUBTREE = 18 // projected_inverse of such ranges, one per warp, parents first
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the

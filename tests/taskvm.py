@@ -24,6 +24,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
 T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL, T_FRONT, T_PFRONT = 8, 9, 10, 11, 12, 13, 14, 15, 16
+T_SUBTREE, T_PSUBTREE = 17, 18
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -184,6 +185,10 @@ class VM(object):
             self._front(t)
         elif op == T_PFRONT:
             self._pfront(t)
+        elif op == T_SUBTREE:
+            self._subtrees(t, False)
+        elif op == T_PSUBTREE:
+            self._subtrees(t, True)
         elif op == T_EXTRACT:
             self._extract(t)
         elif op == T_VEC:
@@ -272,14 +277,33 @@ class VM(object):
                     Ub[Uof + (col - nn) * ldu + (rows - nn)] += v
 
     def _front(self, t):
+        """A whole small cholesky front (T_FRONT)."""
+        self._front_k(int(t["aux"][0]), self.bases[int(t["a"]["base"])], int(t["a"]["off"]),
+                      self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
+
+    def _bundle_ranges(self, t):
+        ends = (int(t["m"]), int(t["n"]), int(t["k"]), int(t["cdiag"]))
+        return [(int(t["aux"][w]), ends[w]) for w in range(4) if int(t["aux"][w]) >= 0]
+
+    def _subtrees(self, t, pinv):
+        """A small-subtree bundle: each range's fronts in postorder
+        (cholesky) or parents first (projected_inverse), values at their
+        blocks and updates at their usual workspace offsets."""
+        WS = self.bases[B_WS]
+        for lo, hi in self._bundle_ranges(t):
+            for k in (range(hi, lo - 1, -1) if pinv else range(lo, hi + 1)):
+                f = self.p.fronts[k]
+                args = (k, self.bases[B_X], int(f["blk"]), WS, int(f["upd"]), max(int(f["na"]), 1))
+                self._pfront_k(*args) if pinv else self._front_k(*args)
+
+    def _front_k(self, k, X, off, Ub, Uof, ldu):
         """A whole small cholesky front: extend-add of the children (last
         to first), partial Cholesky of the nj x nj front, the Schur
         complement into the update matrix, and the off-diagonal block
         stored as L21 L11^{-1} (the reference's layout)."""
-        f = self.p.fronts[int(t["aux"][0])]
+        f = self.p.fronts[k]
         nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
         WS = self.bases[B_WS]
-        X, off = self.bases[int(t["a"]["base"])], int(t["a"]["off"])
         r = np.arange(nj)[:, None]
         c = np.arange(nn)[None, :]
         F = np.zeros((nj, nj))
@@ -305,21 +329,24 @@ class VM(object):
         X[(off + c * nj + r)[low]] = blk[low]
         if na > 0:
             U = S[nn:, nn:] - L21 @ L21.T
-            Ub, Uof, ldu = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
             ri = np.arange(na)[:, None]
             ci = np.arange(na)[None, :]
             lw = ri >= ci
             Ub[(Uof + ci * ldu + ri)[lw]] = U[lw]
 
     def _pfront(self, t):
+        """A whole small projected-inverse front (T_PFRONT)."""
+        self._pfront_k(int(t["aux"][0]), self.bases[int(t["a"]["base"])], int(t["a"]["off"]),
+                       self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"]))
+
+    def _pfront_k(self, k, X, off, Ub, Uof, ldu):
         """A whole small projected-inverse front: M = L11^{-1}, Y11 = M^T M,
         S21 = -V W, Y11 -= S21^T W, the children's updates extracted from
         the front [Y11, S21^T; S21, V], the block written back as [Y11
         (strict upper part zeroed); S21]."""
-        f = self.p.fronts[int(t["aux"][0])]
+        f = self.p.fronts[k]
         nn, na, nj = int(f["nn"]), int(f["na"]), int(f["nj"])
         WS = self.bases[B_WS]
-        X, off = self.bases[int(t["a"]["base"])], int(t["a"]["off"])
         r = np.arange(nj)[:, None]
         c = np.arange(nn)[None, :]
         blk = X[off + c * nj + r]
@@ -330,7 +357,6 @@ class VM(object):
         Y11 = M.T @ M
         F = np.zeros((nj, nj))
         if na > 0:
-            Ub, Uof, ldu = self.bases[int(t["c"]["base"])], int(t["c"]["off"]), int(t["c"]["ld"])
             ri = np.arange(na)[:, None]
             ci = np.arange(na)[None, :]
             Vl = np.where(ri >= ci, Ub[Uof + ci * ldu + ri], 0.0)

@@ -175,8 +175,20 @@ def test_small_front_threshold(nj, order, seed):
             os.environ["CHB_SMALL_FRONT_NJ"] = old
     fronts = np.diff(np.asarray(s.sncolptr))
     want = int(np.sum(fronts <= int(nj)))
-    assert int(np.sum(progs[N.OP_CHOLESKY][0].tasks["op"] == taskvm.T_FRONT)) == want
-    assert int(np.sum(progs[N.OP_PROJECTED_INVERSE][0].tasks["op"] == taskvm.T_PFRONT)) == want
+
+    def bundled(prog, op):
+        """Fronts inside small-subtree bundles (one warp per range)."""
+        tot = 0
+        for t in prog.tasks[prog.tasks["op"] == op]:
+            ends = (int(t["m"]), int(t["n"]), int(t["k"]), int(t["cdiag"]))
+            tot += sum(ends[w] - int(t["aux"][w]) + 1 for w in range(4) if int(t["aux"][w]) >= 0)
+        return tot
+    pc, pp = progs[N.OP_CHOLESKY][0], progs[N.OP_PROJECTED_INVERSE][0]
+    assert int(np.sum(pc.tasks["op"] == taskvm.T_FRONT)) + bundled(pc, taskvm.T_SUBTREE) == want
+    assert int(np.sum(pp.tasks["op"] == taskvm.T_PFRONT)) + bundled(pp, taskvm.T_PSUBTREE) == want
+    assert bundled(pc, taskvm.T_SUBTREE) == bundled(pp, taskvm.T_PSUBTREE)
+    if nj == "32":
+        assert bundled(pc, taskvm.T_SUBTREE) > 0
     if nj == "32":
         assert 0 < want < len(fronts)
     x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
