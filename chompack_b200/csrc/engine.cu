@@ -637,6 +637,190 @@ __device__ void gemm_acc_p(const Opnd& A, const Opnd& B, int m, int n, int K, co
   }
 }
 
+// ------------------------------------------------------ tcgen05 TF32 tiles
+// TF32 GEMM tiles of the mixed-precision sweeps on the fifth-generation
+// tensor cores: tcgen05.mma.cta_group::1.kind::tf32 with M = N = 64 and
+// K = 8 per instruction, FP32 accumulators in tensor memory (64 columns per
+// CTA, allocated once per launch when the program has such tiles).  K goes
+// through the FP64 cp.async ring as for the other tiles (three stages here);
+// per chunk of KC = 16 the 128 threads round the stage to TF32 (cvt.rna, as
+// the mma.sync tiles do) into one of two shared-memory buffers in the
+// canonical K-major layout without swizzle: core matrices of 8 rows x 16
+// bytes, element (r, k) of the chunk at byte ((r/8)*4 + k/4)*128 + (r%8)*16 +
+// (k%4)*4, so the next 4 columns start 128 bytes on (leading byte offset) and
+// the next 8 rows 512 bytes on (stride byte offset).  One thread issues the
+// chunk's two MMAs and commits them to the buffer's mbarrier; a buffer is
+// refilled once its last commit has arrived.  The epilogue reads the
+// accumulator with tcgen05.ld (for M = 64, row 16w + i lives in TMEM lane
+// 32w + i, so warp w reads its own sub-partition's lanes 0..15) and adds
+// alpha*acc + beta*C in FP64.
+constexpr int TC_STAGES = 3;                       // FP64 ring stages of a tcgen05 tile
+constexpr int TC_STAGE_FLOATS = 2 * TILE * KC;     // A then B of one chunk, TF32
+// instruction descriptor: F32 accumulator (bits 4-5 = 1), A and B TF32
+// (bits 7-9, 10-12 = 2), both K-major, N >> 3 (bits 17-22), M >> 4 (bits 24-28)
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TILE >> 3) << 17) |
+                              ((uint32_t)(TILE >> 4) << 24);
+static_assert(TC_STAGES * STAGE_DOUBLES * 8 + 2 * TC_STAGE_FLOATS * 4 <= ENGINE_SMEM_BASE_DOUBLES * 8,
+              "tcgen05 staging exceeds the engine's shared memory");
+
+struct TcState {
+  uint32_t tmem;        // accumulator: TMEM lane 0, first allocated column
+  uint64_t* mbar;       // two mbarriers in shared memory
+  uint32_t ncommit[2];  // commits issued to each mbarrier (same in every thread)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address >> 4 (bits 0-13), leading
+// byte offset 128 >> 4 (bits 16-29), stride byte offset 512 >> 4 (bits
+// 32-45), descriptor version 1 (bits 46-47), no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(512u >> 4) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint64_t* m) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(m)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the completion of the phase with the given parity; a
+// wait that runs out records DE_TIMEOUT and returns false.
+__device__ bool mbar_wait(const RunArgs& ra, uint64_t* m, uint32_t parity) {
+  int64_t spins = 0;
+  while (!mbar_test(m, parity)) {
+    if (++spins > ra.spin_limit) {
+      atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// One FP64 stage (A(r, k) at st[k*LDS + r], B at st + KC*LDS) rounded to
+// TF32 into a staging buffer in the canonical K-major layout; each thread
+// writes 16-byte rows of core matrices.
+__device__ __forceinline__ void tc_stage(const double* st, float* S) {
+#pragma unroll
+  for (int it = 0; it < 4; it++) {
+    const int idx = threadIdx.x + it * NTHREADS;  // (operand, 4-column group, row)
+    const int op = idx >> 8, q = (idx >> 6) & 3, r = idx & 63;
+    const double* src = st + op * KC * LDS + 4 * q * LDS + r;
+    float4 v;
+    v.x = __uint_as_float(to_tf32((float)src[0]));
+    v.y = __uint_as_float(to_tf32((float)src[LDS]));
+    v.z = __uint_as_float(to_tf32((float)src[2 * LDS]));
+    v.w = __uint_as_float(to_tf32((float)src[3 * LDS]));
+    *reinterpret_cast<float4*>(S + op * TILE * KC + ((r >> 3) * 4 + q) * 32 + (r & 7) * 4) = v;
+  }
+}
+
+// C = alpha * opA * opB^T + beta * C for an m x n tile (masked to r + cdiag
+// >= c when lower) with TF32 products on tcgen05 and FP32 accumulation.
+__device__ void gemm_tc_tf32(const RunArgs& ra, const Opnd& A, const Opnd& B, int m, int n, int K,
+                             const SmemLayout& sm, TcState& ts, double* __restrict__ C, int ldc, bool lower,
+                             int cdiag, double alpha, double beta) {
+  const int nch = (K + KC - 1) / KC;
+  double* const ring = sm.A;
+  float* const stg = reinterpret_cast<float*>(ring + TC_STAGES * STAGE_DOUBLES);
+#pragma unroll
+  for (int c = 0; c < TC_STAGES - 1; c++) {
+    if (c < nch) {
+      issue_chunk(A, m, c * KC, K, ring + c * STAGE_DOUBLES);
+      issue_chunk(B, n, c * KC, K, ring + c * STAGE_DOUBLES + KC * LDS);
+    }
+    cp_async_commit();
+  }
+  for (int c = 0; c < nch; c++) {
+    cp_async_wait_group<TC_STAGES - 2>();  // this thread's copies of chunk c
+    __syncthreads();                       // everyone's; and chunk c - 1 is converted
+    const int cn = c + TC_STAGES - 1;
+    if (cn < nch) {
+      double* d = ring + (cn % TC_STAGES) * STAGE_DOUBLES;
+      issue_chunk(A, m, cn * KC, K, d);
+      issue_chunk(B, n, cn * KC, K, d + KC * LDS);
+    }
+    cp_async_commit();
+    const int buf = c & 1;
+    if (c >= 2) mbar_wait(ra, ts.mbar + buf, (ts.ncommit[buf] - 1) & 1);  // chunk c - 2 has read it
+    float* S = stg + buf * TC_STAGE_FLOATS;
+    tc_stage(ring + (c % TC_STAGES) * STAGE_DOUBLES, S);
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      const uint32_t sa = smem_u32(S), sb = smem_u32(S + TILE * KC);
+      tc_mma(ts.tmem, tc_desc(sa), tc_desc(sb), c > 0 ? 1u : 0u);
+      tc_mma(ts.tmem, tc_desc(sa + 256), tc_desc(sb + 256), 1u);
+      tc_commit(ts.mbar + buf);
+    }
+    ts.ncommit[buf]++;
+  }
+  cp_async_wait_group<0>();
+  // the last commit covers every MMA of the tile
+  const int lb = (nch - 1) & 1;
+  mbar_wait(ra, ts.mbar + lb, (ts.ncommit[lb] - 1) & 1);
+  tc_fence_after();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = warp * 16 + lane;
+  const uint32_t taddr = ts.tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+  for (int c0 = 0; c0 < TILE; c0 += 16) {
+    uint32_t v[16];
+    tmem_ld16(taddr + c0, v);
+    if (lane < 16 && r < m) {
+      double old[16];
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int c = c0 + j;
+        const bool ok = c < n && !(lower && r + cdiag < c);
+        old[j] = (beta != 0.0 && ok) ? __ldcg(C + (int64_t)c * ldc + r) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int c = c0 + j;
+        if (c >= n || (lower && r + cdiag < c)) continue;
+        double x = alpha * (double)__uint_as_float(v[j]);
+        if (beta != 0.0) x += beta * old[j];
+        C[(int64_t)c * ldc + r] = x;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+}
+
 __device__ __forceinline__ void gemm_acc(const Opnd& A, const Opnd& B, int m, int n, int K, const SmemLayout& sm,
                                          Acc& acc) {
   gemm_acc_p<PREC_FP64>(A, B, m, n, K, sm, acc);
@@ -687,7 +871,7 @@ __device__ void store_acc(double* __restrict__ C, int ldc, int m, int n, bool lo
 //   pass 1: D -= L L^T (lower part), L read back from L2
 // Both passes share one inlined copy of the GEMM code: a second copy (or a
 // call) makes the persistent kernel spill.
-__device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
+__device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayout& sm, TcState& ts) {
   const bool la = t.op == T_LA;
   const int passes = la ? 2 : 1;
   for (int ph = 0; ph < passes; ph++) {
@@ -699,6 +883,10 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
     const int cdiag = la ? 0 : t.cdiag;
     const double alpha = la ? (ph == 0 ? 1.0 : -1.0) : t.alpha;
     const double beta = la ? (ph == 0 ? 0.0 : 1.0) : t.beta;
+    if (!la && t.c.prec == PREC_TF32 && ra.tmem) {
+      gemm_tc_tf32(ra, A, B, m, n, K, sm, ts, ra.bases[oc.base] + oc.off, oc.ld, lower, cdiag, alpha, beta);
+      continue;
+    }
     Acc acc;
     if (la || t.c.prec == PREC_FP64) gemm_acc_p<PREC_FP64>(A, B, m, n, K, sm, acc);
     else if (t.c.prec == PREC_TF32) gemm_acc_p<PREC_TF32>(A, B, m, n, K, sm, acc);
@@ -2171,9 +2359,33 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   static_assert(sizeof(Task) == 36 * 4, "task record is 36 words");
   SmemLayout sm{smem, smem + TILE * LDS};
   __shared__ int s_lo;        // dynamic: this CTA's copy of the finished frontier
+  __shared__ uint32_t s_tmem;                 // tensor-memory base of the TF32 tiles
+  __shared__ __align__(8) uint64_t s_mbar[2]; // their MMA-completion barriers
   if (threadIdx.x == 0) {
     s_next = -1;
     s_lo = 0;
+  }
+  TcState ts;
+  ts.mbar = s_mbar;
+  ts.ncommit[0] = ts.ncommit[1] = 0;
+  ts.tmem = 0;
+  if (ra.tmem) {
+    // 64 columns of tensor memory (a 64 x 64 FP32 accumulator) for the
+    // whole launch: two CTAs per SM take 128 of the 512 columns
+    if (threadIdx.x < 32) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&s_tmem))
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+      mbar_init(&s_mbar[0]);
+      mbar_init(&s_mbar[1]);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    ts.tmem = s_tmem;
   }
   for (;;) {
     if (ra.dynamic) {
@@ -2252,7 +2464,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     const Task& t = s_t;
     switch (t.op) {
       case T_GEMM:
-      case T_LA: run_gemm_or_la(ra, t, sm); break;
+      case T_LA: run_gemm_or_la(ra, t, sm, ts); break;
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem, ti); break;
       case T_ASM: run_asm(ra, t, smem); break;
@@ -2297,6 +2509,14 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     __syncthreads();
     if (threadIdx.x == 0 && atomicAdd(&ra.ctl[6], 1) == (int)gridDim.x - 1)
       for (int j = 0; j < ra.nio_out; j++) raise_io_flag(ra.io_out + j);
+  }
+  if (ra.tmem) {
+    // every tile waited for its last commit, so no MMA is in flight
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x < 32)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(ts.tmem) : "memory");
   }
 }
 

@@ -165,7 +165,7 @@ struct RunArgs {
   int dynamic;
   int nwords;                     // ready-bitmap words (64 tasks each)
   int nsumm;                      // summary words (64 bitmap words each)
-  int pad2;
+  int tmem;                       // 1: TF32 GEMM tiles run on tcgen05 (tensor memory allocated per CTA)
   int* pend;                      // unmet dependencies per task
   unsigned long long* ready;      // ready, unclaimed tasks
   unsigned long long* summ;       // nonzero ready words

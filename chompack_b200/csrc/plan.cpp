@@ -149,6 +149,7 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
   if (prec != PREC_FP64)
     for (Task& t : prog->tasks)
       if (t.op == T_GEMM) t.c.prec = prec;
+  prog->tf32_tiles = prec == PREC_TF32;
   for (const Task& t : prog->tasks)
     if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
   // Default schedule per sweep, by measurement on a 3-D grid of 64,000
@@ -236,6 +237,10 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.spin_limit = plan->spin_limit >= 0 ? plan->spin_limit : kDefaultSpinLimit;
   ra.trace = (plan->trace && plan->trace_cap >= (int64_t)prog->tasks.size()) ? plan->trace : nullptr;
   ra.perm = plan->d_perm;
+  // TF32 tiles on tcgen05 unless CHB_TF32_MMA_SYNC asks for the warp-level
+  // mma.sync tiles (kept for comparison)
+  static const bool tf32_mma_sync = std::getenv("CHB_TF32_MMA_SYNC") != nullptr;
+  ra.tmem = prog->tf32_tiles && !tf32_mma_sync ? 1 : 0;
   ra.ldb = run_ldb;
   ra.alpha = run_alpha;
   // The plan's schedule, else CHB_SCHEDULE (static | dynamic), else the

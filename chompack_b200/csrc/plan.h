@@ -37,6 +37,7 @@ struct Program {
   int64_t ws_doubles = 0;  // doubles of workspace (update matrices + scratch)
   int smem_doubles = ENGINE_SMEM_BASE_DOUBLES;  // dynamic shared memory per CTA
   bool static_default = false;  // list order unless the plan asks otherwise
+  bool tf32_tiles = false;      // some GEMM tile computes in TF32 (one product)
   IoSpec io;                    // streaming of the values (set before building)
   std::vector<int> out_order;   // chunks in the list order of their signals
   Task* d_tasks = nullptr;

@@ -85,3 +85,37 @@ def test_host_values_in_mixed_precision():
     cp.projected_inverse(Xh, precision="tf32x3")
     cp.projected_inverse(Xd, precision="tf32x3")
     assert torch.equal(Xh.blkval, Xd.blkval.cpu())
+
+
+def test_tcgen05_tiles_agree_with_mma_sync_tiles(tmp_path):
+    """The TF32 tiles run on tcgen05 (tensor-memory accumulators); with
+    CHB_TF32_MMA_SYNC set they run as warp-level mma.sync.  Both round the
+    same FP64 operands to TF32 and accumulate in FP32 (in different orders),
+    so the factors agree far below the TF32 error itself (which the FP64
+    comparison bounds), and both are far from garbage."""
+    import os
+    import subprocess
+    import sys
+    A, s = problem("grid3d", 14, merge=(32, 32), seed=5)
+    X = _dev(s, A)
+    L = cp.cspmatrix(s, blkval=X.blkval.clone())
+    cp.cholesky(L, precision="tf32")
+    L64 = cp.cspmatrix(s, blkval=X.blkval.clone())
+    cp.cholesky(L64)
+    out = tmp_path / "mma_sync.npy"
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r)\n"
+            "import chompack_b200 as cp\nfrom helpers import problem\n"
+            "A, s = problem('grid3d', 14, merge=(32, 32), seed=5)\n"
+            "X = cp.cspmatrix(s, device='cuda') + A\ncp.cholesky(X, precision='tf32')\n"
+            "np.save(%r, X.blkval.cpu().numpy())\n") % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                                        os.path.dirname(os.path.abspath(__file__)), str(out))
+    env = dict(os.environ, CHB_TF32_MMA_SYNC="1")
+    subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
+    other = np.load(out)
+    got = L.blkval.cpu().numpy()
+    ref64 = L64.blkval.cpu().numpy()
+    scale = np.abs(ref64).max()
+    e_tc = np.abs(got - ref64).max() / scale
+    e_ms = np.abs(other - ref64).max() / scale
+    assert 0.0 < e_tc <= 2e-3 and 0.0 < e_ms <= 2e-3, (e_tc, e_ms)
+    assert np.abs(got - other).max() / scale <= 0.5 * max(e_tc, e_ms), (e_tc, e_ms)
