@@ -351,7 +351,7 @@ def _event_ms(dev, fn, reps):
     return float(np.median(times))
 
 
-def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
+def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5, grid2d=None):
     """Mixed-precision form (GEMM tiles on TF32 tensor cores, FP64 diagonal
     tiles): log det forward + backward (cholesky + projected_inverse) on the
     3-D 7-point grid side^3 with merge_size_fill(merge), timed in FP64,
@@ -364,16 +364,24 @@ def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5):
     import chompack_b200 as cp
     from chompack_b200 import mixed
     from oracle import workload
-    A, s = build_problem(side=side, merge=merge)
+    if grid2d:
+        from chompack_b200 import grids
+        A = grids.grid2d(grid2d, seed=0)
+        s = cp.symbolic(A, p=cp.amd.order(A), merge_function=cp.merge_size_fill(*merge))
+        what = "2-D 5-point grid %d^2 (n=%d)" % (grid2d, s.n)
+    else:
+        A, s = build_problem(side=side, merge=merge)
+        what = "3-D 7-point grid %d^3 (n=%d)" % (side, s.n)
     fl = sweep_flops(s)
     flops = fl["cholesky"] + fl["projected_inverse"]
     X0 = cp.cspmatrix(s, device=dev) + A
     x0 = X0.blkval.cpu().numpy()
     Lr, Yr = reference_outputs(s, x0)
     ld_ref = _logdet_of_factor(s, Lr)
-    out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d); log det forward + backward "
-                       "(cholesky + projected_inverse)" % (side, s.n, merge[0], merge[1]),
-           "flops": flops, "errors_against": "reference C kernels (oracle/_ref), FP64, same inputs"}
+    out = {"workload": "%s, AMD, merge_size_fill(%d,%d); log det forward + backward (cholesky + "
+                       "projected_inverse)" % (what, merge[0], merge[1]),
+           "flops": flops, "nsn": int(s.Nsn), "values": int(s.blkptr[-1]),
+           "errors_against": "reference C kernels (oracle/_ref), FP64, same inputs"}
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for prec in ("fp64", "tf32", "tf32x3"):
         X = cp.cspmatrix(s, blkval=X0.blkval.clone())
@@ -841,6 +849,7 @@ def main():
         if not args.no_mixed and not args.no_other:
             try:
                 out["mixed_precision"] = mixed_precision_section(dev)
+                out["mixed_precision"]["grid2d_1000"] = mixed_precision_section(dev, grid2d=1000, reps=3)
             except Exception as exc:  # reported beside the headline, never required
                 out["mixed_precision"] = {"unavailable": str(exc)}
         if not args.no_batch and not args.no_other:

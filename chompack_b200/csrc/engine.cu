@@ -706,12 +706,15 @@ __device__ __forceinline__ bool mbar_test(uint64_t* m, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the completion of the phase with the given parity; a
-// wait that runs out records DE_TIMEOUT and returns false.
+// Bounded wait for the completion of the phase with the given parity (an
+// MMA chunk takes well under a microsecond; each try_wait may suspend the
+// thread for a while, so the bound is time, 2 s); a wait that runs out
+// records DE_TIMEOUT and returns false.
 __device__ bool mbar_wait(const RunArgs& ra, uint64_t* m, uint32_t parity) {
-  int64_t spins = 0;
+  if (mbar_test(m, parity)) return true;
+  const unsigned long long t0 = global_ns();
   while (!mbar_test(m, parity)) {
-    if (++spins > ra.spin_limit) {
+    if (global_ns() - t0 > 2000000000ull) {
       atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
       return false;
     }

@@ -96,3 +96,62 @@ def test_two_gloo_ranks_shard_a_batch():
         assert full == pytest.approx(serial, rel=1e-13)
         assert tmax == 2.0
         assert tsum == float(len(mats))
+
+
+def _worker_uneven(rank, world, port, root, q):
+    """The benchmark's sharded batch flow (bench.py batch_section) on gloo:
+    the uneven grids of grids.uneven_batch_specs (here 12 small ones),
+    shares by cholesky flops, per-matrix log dets gathered, the per-rank
+    breakdown exchanged with all_gather_object and the time reduced as the
+    max over ranks."""
+    import sys
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "tests"))
+    import torch.distributed as dist
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        specs = grids.uneven_batch_specs(count=12, lo=6, hi=14)
+        mats = []
+        for sd, seed in specs:
+            A = grids.grid2d_extra(sd, seed=seed)
+            mats.append((A, cp.symbolic(A, p=cp.amd.order(A))))
+        costs = [shard.cholesky_flops(s) for _, s in mats]
+        mine = shard.my_share(costs, rank, world)
+        lds = [_logdet_oracle(*mats[i]) for i in mine]
+        all_ld = shard.gather_results(mine, lds, len(mats))
+        per_rank = [None] * world
+        dist.all_gather_object(per_rank, {"rank": rank, "matrices": len(mine)})
+        t_max = shard.max_over_ranks(0.5 * (rank + 1))
+        q.put((rank, mine, all_ld, per_rank, t_max))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_the_uneven_batch_like_the_benchmark():
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_uneven, args=(r, 2, port, root, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=240) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    serial = []
+    for sd, seed in grids.uneven_batch_specs(count=12, lo=6, hi=14):
+        A = grids.grid2d_extra(sd, seed=seed)
+        serial.append(_logdet_oracle(A, cp.symbolic(A, p=cp.amd.order(A))))
+    assert sorted(i for r in results for i in r[1]) == list(range(12))
+    for rank, mine, all_ld, per_rank, t_max in results:
+        assert all_ld == pytest.approx(serial, rel=1e-13)
+        assert [d["rank"] for d in per_rank] == [0, 1]
+        assert sum(d["matrices"] for d in per_rank) == 12
+        assert t_max == 1.0
