@@ -119,3 +119,8 @@ syr2 = _sig("chb_syr2", ctypes.c_int, [PPLAN, vp, vp, vp, vp, vp, ctypes.c_doubl
 add_projection = _sig("chb_add_projection", ctypes.c_int, [PPLAN, vp, vp, vp, vp, i64, ctypes.c_double,
                                                            ctypes.c_double, ctypes.c_int, vp])
 diag = _sig("chb_diag", ctypes.c_int, [PPLAN, vp, vp, vp])
+
+# ---- program-build options (chb_plan_set_option)
+plan_set_option = _sig("chb_plan_set_option", ctypes.c_int, [PPLAN, ctypes.c_int, i64])
+plan_get_option = _sig("chb_plan_get_option", ctypes.c_int, [PPLAN, ctypes.c_int, ctypes.POINTER(i64)])
+OPTIONS = {"small_front_nj": 0, "subtrees": 1, "chol_ksplit": 2, "pinv_ksplit": 3, "fused_la": 4}

@@ -23,14 +23,14 @@ namespace chb {
 
 int build_cholesky(const chb_plan& P, Program& prog) {
   const int T = TILE;
-  const int small_nj = small_front_nj();
+  const int small_nj = small_front_nj(P);
   const int CH = 64;  // at most this many front columns per extend-add task
   const int64_t N = P.nsn;
   DagBuilder B;
 
   // workspace: update matrices first (shared layout), then per-front scratch
   int64_t ws = P.upd_total;
-  const int kc = chol_ksplit();
+  const int kc = chol_ksplit(P);
   std::vector<int64_t> scrS(N, -1), scrM(N, -1), scrK(N, -1);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
@@ -87,7 +87,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   for (int64_t k = 0; k < N; k++)
     if (P.fronts[k].nn > T) multi_block_fronts++;
   const int grid = P.grid > 0 ? P.grid : 296;
-  const bool fuse_la = 2 * multi_block_fronts < grid && std::getenv("CHB_NO_FUSED_LA") == nullptr;
+  const bool fuse_la = 2 * multi_block_fronts < grid && fused_la_allowed(P);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int nn = f.nn, na = f.na, nj = f.nj;

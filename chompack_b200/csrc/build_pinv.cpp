@@ -22,7 +22,7 @@ namespace chb {
 
 int build_projected_inverse(const chb_plan& P, Program& prog) {
   const int T = TILE;
-  const int small_nj = small_front_nj();
+  const int small_nj = small_front_nj(P);
   const int CH = 16;  // child columns per extract task
   const int64_t N = P.nsn;
   DagBuilder B;
@@ -42,7 +42,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     }
   }
   // split-K scratch, handed out as the long-K tiles are built
-  const int KSPLIT = pinv_ksplit();
+  const int KSPLIT = pinv_ksplit(P);
   auto scratch = [&ws](int K, int kc) {
     const int p = split_count(K, kc);
     if (p == 1) return (int64_t)0;

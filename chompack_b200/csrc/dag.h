@@ -536,33 +536,52 @@ struct DagBuilder {
   }
 };
 
+// Program-build options: the plan's value (chb_plan_set_option) when set,
+// else the environment variable, else the built-in default.
+inline int64_t plan_option(const chb_plan& P, int opt, const char* env, int64_t dflt) {
+  if (opt >= 0 && opt < CHB_OPT_COUNT && P.opt[opt] >= 0) return P.opt[opt];
+  const char* e = std::getenv(env);
+  return e ? (int64_t)std::atoll(e) : dflt;
+}
+
 // Largest K of one partial product of projected_inverse's long-K tiles
-// (CHB_PINV_KSPLIT, rounded down to a multiple of TILE, at least 2 TILE;
-// default 512: at 40^3 the sweep is bound by the CTAs' total work, and
-// 384 / 512 / 768 / 1024 / 1536 gave 6.01 / 5.64 / 5.74 / 5.72 / 6.09 ms).
-inline int pinv_ksplit() {
-  const char* e = std::getenv("CHB_PINV_KSPLIT");
-  const int v = e ? (std::atoi(e) / TILE) * TILE : 512;
+// (CHB_OPT_PINV_KSPLIT / CHB_PINV_KSPLIT, rounded down to a multiple of TILE,
+// at least 2 TILE; default 512: at 40^3 the sweep is bound by the CTAs'
+// total work, and 384 / 512 / 768 / 1024 / 1536 gave 6.01 / 5.64 / 5.74 /
+// 5.72 / 6.09 ms).
+inline int pinv_ksplit(const chb_plan& P) {
+  const int v = (int)(plan_option(P, CHB_OPT_PINV_KSPLIT, "CHB_PINV_KSPLIT", 512) / TILE) * TILE;
   return v < 2 * TILE ? 2 * TILE : v;
 }
 
 // Largest K of one partial product of cholesky's Schur-complement tiles
-// U_k -= S_k S_k^T (CHB_CHOL_KSPLIT, rounded down to a multiple of TILE;
-// 0, the default, leaves them whole).
-inline int chol_ksplit() {
-  const char* e = std::getenv("CHB_CHOL_KSPLIT");
-  const int v = e ? (std::atoi(e) / TILE) * TILE : 0;
+// U_k -= S_k S_k^T (CHB_OPT_CHOL_KSPLIT / CHB_CHOL_KSPLIT, rounded down to a
+// multiple of TILE; 0, the default, leaves them whole).
+inline int chol_ksplit(const chb_plan& P) {
+  const int v = (int)(plan_option(P, CHB_OPT_CHOL_KSPLIT, "CHB_CHOL_KSPLIT", 0) / TILE) * TILE;
   return v <= 0 ? 0 : (v < 2 * TILE ? 2 * TILE : v);
 }
 
 // Largest front order (nj) that a sweep runs as one shared-memory task
-// (cholesky, projected_inverse): TILE, or CHB_SMALL_FRONT_NJ when set
-// (0 turns the small-front tasks off).
-inline int small_front_nj() {
-  const char* e = std::getenv("CHB_SMALL_FRONT_NJ");
-  if (!e) return TILE;
-  const int v = std::atoi(e);
-  return v < 0 ? 0 : (v > TILE ? TILE : v);
+// (cholesky, projected_inverse): TILE, or CHB_OPT_SMALL_FRONT_NJ /
+// CHB_SMALL_FRONT_NJ when set (0 turns the small-front tasks off).
+inline int small_front_nj(const chb_plan& P) {
+  const int64_t v = plan_option(P, CHB_OPT_SMALL_FRONT_NJ, "CHB_SMALL_FRONT_NJ", TILE);
+  return v < 0 ? 0 : (v > TILE ? TILE : (int)v);
+}
+
+// Small-subtree bundles on (CHB_OPT_SUBTREES = 1, the default) or off (0;
+// also CHB_NO_SUBTREES in the environment).
+inline bool subtrees_on(const chb_plan& P) {
+  if (P.opt[CHB_OPT_SUBTREES] >= 0) return P.opt[CHB_OPT_SUBTREES] != 0;
+  return std::getenv("CHB_NO_SUBTREES") == nullptr;
+}
+
+// cholesky's fused diagonal task (CHB_OPT_FUSED_LA = 1, the default where it
+// is safe) or separate look-ahead tasks (0; also CHB_NO_FUSED_LA).
+inline bool fused_la_allowed(const chb_plan& P) {
+  if (P.opt[CHB_OPT_FUSED_LA] >= 0) return P.opt[CHB_OPT_FUSED_LA] != 0;
+  return std::getenv("CHB_NO_FUSED_LA") == nullptr;
 }
 
 // An operand advanced by k0 along its K dimension.
@@ -677,8 +696,8 @@ inline SplitTask add_split_gemm(DagBuilder& B, const Task& t, int kc, int64_t sc
 // Small-subtree bundles (T_SUBTREE / T_PSUBTREE).  A subtree qualifies when
 // every front in it has nj <= SUB_NJ (and the small-front tasks are on);
 // the maximal ones are cut into warp ranges (adjacent subtrees in postorder
-// merged up to a modelled cost), four ranges per task.  CHB_NO_SUBTREES
-// turns bundling off (every small front is then its own T_FRONT / T_PFRONT).
+// merged up to a modelled cost), four ranges per task.  CHB_OPT_SUBTREES = 0
+// (or CHB_NO_SUBTREES) turns bundling off (every small front is then its own T_FRONT / T_PFRONT).
 struct Bundles {
   // per task: up to four inclusive ranges [lo, hi] (lo < 0: no range)
   std::vector<std::array<int, 8>> tasks;
@@ -697,7 +716,7 @@ inline Bundles make_bundles(const chb_plan& P) {
   Bundles out;
   const int64_t N = P.nsn;
   out.of.assign(N, -1);
-  if (std::getenv("CHB_NO_SUBTREES") != nullptr || small_front_nj() < SUB_NJ || N == 0) return out;
+  if (!subtrees_on(P) || small_front_nj(P) < SUB_NJ || N == 0) return out;
   std::vector<char> all(N, 1);
   std::vector<int> size(N, 1);
   for (int64_t k = 0; k < N; k++) {

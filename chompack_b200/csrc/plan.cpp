@@ -1,5 +1,6 @@
 // Plan creation (symbolic upload), program cache and program launch.
 #include "plan.h"
+#include "dag.h"
 
 #include <cstdlib>
 
@@ -607,6 +608,32 @@ extern "C" int chb_plan_set_schedule(chb_plan* plan, int mode) {
   if (!plan) return set_error(-1, "null plan");
   if (mode < -1 || mode > 1) return set_error(-2, "schedule mode must be -1, 0 or 1");
   plan->schedule = mode;
+  return 0;
+}
+
+extern "C" int chb_plan_set_option(chb_plan* plan, int option, int64_t value) {
+  clear_error();
+  if (!plan) return set_error(-1, "null plan");
+  if (option < 0 || option >= CHB_OPT_COUNT) return set_error(-2, "unknown option %d", option);
+  const int64_t v = value < 0 ? -1 : value;
+  if (plan->opt[option] != v) {
+    plan->opt[option] = v;
+    plan->progs.clear();  // rebuilt with the new option by the next sweeps
+  }
+  return 0;
+}
+
+extern "C" int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value) {
+  clear_error();
+  if (!plan || !value) return set_error(-1, "null argument");
+  switch (option) {
+    case CHB_OPT_SMALL_FRONT_NJ: *value = small_front_nj(*plan); break;
+    case CHB_OPT_SUBTREES: *value = subtrees_on(*plan) ? 1 : 0; break;
+    case CHB_OPT_CHOL_KSPLIT: *value = chol_ksplit(*plan); break;
+    case CHB_OPT_PINV_KSPLIT: *value = pinv_ksplit(*plan); break;
+    case CHB_OPT_FUSED_LA: *value = fused_la_allowed(*plan) ? 1 : 0; break;
+    default: return set_error(-2, "unknown option %d", option);
+  }
   return 0;
 }
 

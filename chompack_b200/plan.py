@@ -103,6 +103,26 @@ class Plan(object):
         code = {None: -1, "dynamic": 0, "static": 1}[mode]
         N.check(N.plan_set_schedule(self.handle, code), "plan_set_schedule")
 
+    def set_option(self, name, value=None):
+        """Program-build option of this plan's sweeps (chb_plan_set_option):
+        "small_front_nj", "subtrees", "chol_ksplit", "pinv_ksplit" or
+        "fused_la"; None restores the default.  Drops the compiled programs
+        (the device is synchronised first, so no sweep of the plan is in
+        flight)."""
+        if self.device >= 0:
+            torch.cuda.synchronize(self.device)
+        v = -1 if value is None else int(value)
+        N.check(N.plan_set_option(self.handle, N.OPTIONS[name], v), "plan_set_option")
+
+    def option(self, name):
+        """The value the next program build uses for an option."""
+        v = ctypes.c_int64()
+        N.check(N.plan_get_option(self.handle, N.OPTIONS[name], ctypes.byref(v)), "plan_get_option")
+        return int(v.value)
+
+    def options(self):
+        return {k: self.option(k) for k in N.OPTIONS}
+
     def set_spin_limit(self, polls=None):
         """Bound of every wait inside this plan's sweeps, in polls (None:
         the default, about 10 s); a wait that runs out ends the sweep with

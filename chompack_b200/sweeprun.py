@@ -1,0 +1,58 @@
+"""Run one sweep of a synthetic grid a few times and print its CUDA-event
+times (for profiling a single kernel launch, e.g. under ncu):
+
+    python -m chompack_b200.sweeprun --side 40 --merge 32 --sweep cholesky --precision fp64 --reps 3
+
+The matrix is the seeded 3-D 7-point grid side^3 (or the 2-D 5-point grid
+with --grid2d) with AMD ordering and merge_size_fill(merge, merge); each
+repetition refreshes the values and launches the sweep once
+(projected_inverse runs on the factor of a preceding, untimed cholesky).
+"""
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from . import grids
+from . import cbase
+from .cspmatrix import cspmatrix
+from .symbolic import symbolic, merge_size_fill
+from . import amd
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--side", type=int, default=40)
+    ap.add_argument("--grid2d", action="store_true")
+    ap.add_argument("--merge", type=int, default=32)
+    ap.add_argument("--sweep", default="cholesky", choices=["cholesky", "projected_inverse"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32", "tf32x3"])
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    A = grids.grid2d(args.side, seed=0) if args.grid2d else grids.grid3d(args.side, seed=0)
+    s = symbolic(A, p=amd.order(A), merge_function=merge_size_fill(args.merge, args.merge))
+    X0 = cspmatrix(s) + A
+    base = X0.blkval
+    if args.sweep == "projected_inverse":
+        L = cspmatrix(s, blkval=base.clone())
+        cbase.cholesky(L, precision=args.precision)
+        base = L.blkval
+    X = cspmatrix(s, blkval=base.clone(), factor=args.sweep == "projected_inverse")
+    times = []
+    for _ in range(args.reps):
+        X.blkval.copy_(base)
+        X.is_factor = args.sweep == "projected_inverse"
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        getattr(cbase, args.sweep)(X, precision=args.precision)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"sweep": args.sweep, "precision": args.precision, "n": s.n, "nsn": s.Nsn,
+                      "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -329,6 +329,32 @@ int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
  * bit-identical results. */
 int chb_plan_set_schedule(chb_plan* plan, int mode);
 
+/* Program-build options of the plan's sweeps (no counterpart in the
+ * reference: they choose how a sweep is cut into tasks, not what it
+ * computes).  value < 0 restores the default (the environment variable of
+ * the same name, else the built-in value).  Setting an option drops the
+ * plan's compiled programs, so call it only while no sweep of the plan is
+ * in flight; the next sweeps rebuild them.
+ *   CHB_OPT_SMALL_FRONT_NJ  largest front order run as one shared-memory
+ *                           task (0..64, default 64)
+ *   CHB_OPT_SUBTREES        small complete subtrees (fronts of order <= 32)
+ *                           bundled four per task, one warp each (1/0)
+ *   CHB_OPT_CHOL_KSPLIT     cholesky: K chunk of the split Schur-complement
+ *                           tiles (multiple of 64, 0 = whole)
+ *   CHB_OPT_PINV_KSPLIT     projected_inverse: K chunk of its long-K tiles
+ *   CHB_OPT_FUSED_LA        cholesky: fused diagonal task (1/0)
+ * chb_plan_get_option gives the value the next program build uses. */
+enum chb_option {
+  CHB_OPT_SMALL_FRONT_NJ = 0,
+  CHB_OPT_SUBTREES = 1,
+  CHB_OPT_CHOL_KSPLIT = 2,
+  CHB_OPT_PINV_KSPLIT = 3,
+  CHB_OPT_FUSED_LA = 4,
+  CHB_OPT_COUNT = 5
+};
+int chb_plan_set_option(chb_plan* plan, int option, int64_t value);
+int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value);
+
 /* Bound of every wait inside the plan's sweeps: a task's wait on its
  * dependencies, on an incoming chunk or for ready work gives up after
  * `polls` polls (with a back-off of up to ~1 us each); the sweep then ends
