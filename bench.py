@@ -493,6 +493,13 @@ def batch_section(dev, rank, world, count=256, value_sets=64, reps=5):
                          v is not None for v in all_ld), "sharding": "chompack_b200.shard.partition by cholesky flops"}
         if rank == 0 and name == "uneven_grids":
             entry.update(_batch_reference(Bs, x0, x, B, dev))
+        if world == 1:
+            # the task cutting picked by the autotuner for this batch, timed again
+            tr = cp.tune(B, x0, reps=2)
+            tms = _event_ms(dev, step, reps)
+            entry["tuned"] = {"choice": tr["choice"], "ms": round(tms, 3),
+                              "achieved_gbs": round(alg / tms / 1e6, 1), "hbm_frac": round(alg / tms / 1e6 / peak, 4),
+                              "trials": len(tr["trials"])}
         out[name] = entry
     return out
 

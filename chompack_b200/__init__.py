@@ -27,6 +27,7 @@ from . import mixed  # noqa: E402,F401
 from .pfcholesky import pfcholesky  # noqa: E402,F401
 from .base import syr2  # noqa: E402,F401
 from .completions import psdcompletion, mrcompletion  # noqa: E402,F401
+from .autotune import tune  # noqa: E402,F401
 
 __all__ += ["cholesky", "llt", "projected_inverse", "completion", "hessian", "trsm", "trmm", "dot", "autograd", "batch",
-            "pfcholesky", "syr2", "psdcompletion", "mrcompletion"]
+            "pfcholesky", "syr2", "psdcompletion", "mrcompletion", "tune"]
