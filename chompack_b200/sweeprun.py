@@ -4,8 +4,10 @@ times (for profiling a single kernel launch, e.g. under ncu):
     python -m chompack_b200.sweeprun --side 40 --merge 32 --sweep cholesky --precision fp64 --reps 3
 
 The matrix is the seeded 3-D 7-point grid side^3 (or the 2-D 5-point grid
-with --grid2d) with AMD ordering and merge_size_fill(merge, merge); each
-repetition refreshes the values and launches the sweep once
+with --grid2d) with AMD ordering and merge_size_fill(merge, merge), or with
+--batch N the first N matrices of the uneven batch (2-D grids of side 20..120
+with two extra neighbours per node, AMD, no merging) in one merged plan;
+each repetition refreshes the values and launches the sweep once
 (projected_inverse runs on the factor of a preceding, untimed cholesky).
 """
 import argparse
@@ -29,7 +31,10 @@ def main():
     ap.add_argument("--sweep", default="cholesky", choices=["cholesky", "projected_inverse"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32", "tf32x3"])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=0)
     args = ap.parse_args()
+    if args.batch:
+        return run_batch(args)
     A = grids.grid2d(args.side, seed=0) if args.grid2d else grids.grid3d(args.side, seed=0)
     s = symbolic(A, p=amd.order(A), merge_function=merge_size_fill(args.merge, args.merge))
     X0 = cspmatrix(s) + A
@@ -51,6 +56,31 @@ def main():
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     print(json.dumps({"sweep": args.sweep, "precision": args.precision, "n": s.n, "nsn": s.Nsn,
+                      "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
+
+
+def run_batch(args):
+    from .batch import batch
+    specs = grids.uneven_batch_specs()[:args.batch]
+    As = [grids.grid2d_extra(sd, seed=seed) for sd, seed in specs]
+    B = batch([symbolic(A, p=amd.order(A)) for A in As])
+    x0 = B.assemble(As)
+    base = x0
+    if args.sweep == "projected_inverse":
+        base = x0.clone()
+        B.cholesky(base)
+    x = base.clone()
+    times = []
+    for _ in range(args.reps):
+        x.copy_(base)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        getattr(B, args.sweep)(x)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"sweep": args.sweep, "batch": args.batch, "values": B.size,
                       "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
 
 
