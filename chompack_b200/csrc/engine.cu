@@ -874,6 +874,7 @@ __device__ void store_acc(double* __restrict__ C, int ldc, int m, int n, bool lo
 //   pass 1: D -= L L^T (lower part), L read back from L2
 // Both passes share one inlined copy of the GEMM code: a second copy (or a
 // call) makes the persistent kernel spill.
+template <bool TC>
 __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayout& sm, TcState& ts) {
   const bool la = t.op == T_LA;
   const int passes = la ? 2 : 1;
@@ -886,7 +887,7 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
     const int cdiag = la ? 0 : t.cdiag;
     const double alpha = la ? (ph == 0 ? 1.0 : -1.0) : t.alpha;
     const double beta = la ? (ph == 0 ? 0.0 : 1.0) : t.beta;
-    if (!la && t.c.prec == PREC_TF32 && ra.tmem) {
+    if (TC && !la && t.c.prec == PREC_TF32) {
       gemm_tc_tf32(ra, A, B, m, n, K, sm, ts, ra.bases[oc.base] + oc.off, oc.ld, lower, cdiag, alpha, beta);
       continue;
     }
@@ -2351,6 +2352,11 @@ __device__ void run_subtrees(const RunArgs& ra, const Task& t, double* smem) {
 static_assert(NTHREADS == 128, "a bundle has one range per warp of a 4-warp CTA");
 static_assert(8 * SUB_NJ * SUB_LD <= ENGINE_SMEM_BASE_DOUBLES, "bundle fronts exceed the engine's shared memory");
 
+// TC: the instantiation launched for programs with TF32 tiles, which run on
+// tcgen05 with tensor memory; the other one contains no tcgen05 code at all
+// (with that code present, a launch of the FP64 sweeps measured 17-60 %
+// slower at 40^3, although no tcgen05 instruction ran).
+template <bool TC>
 __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   extern __shared__ double smem[];
   __shared__ int s_task;
@@ -2372,7 +2378,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
   ts.mbar = s_mbar;
   ts.ncommit[0] = ts.ncommit[1] = 0;
   ts.tmem = 0;
-  if (ra.tmem) {
+  if (TC) {
     // 64 columns of tensor memory (a 64 x 64 FP32 accumulator) for the
     // whole launch: two CTAs per SM take 128 of the 512 columns
     if (threadIdx.x < 32) {
@@ -2467,7 +2473,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     const Task& t = s_t;
     switch (t.op) {
       case T_GEMM:
-      case T_LA: run_gemm_or_la(ra, t, sm, ts); break;
+      case T_LA: run_gemm_or_la<TC>(ra, t, sm, ts); break;
       case T_MROW: run_mrow(ra, t, sm); break;
       case T_POTRF: run_potrf(ra, t, smem, ti); break;
       case T_ASM: run_asm(ra, t, smem); break;
@@ -2513,7 +2519,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
     if (threadIdx.x == 0 && atomicAdd(&ra.ctl[6], 1) == (int)gridDim.x - 1)
       for (int j = 0; j < ra.nio_out; j++) raise_io_flag(ra.io_out + j);
   }
-  if (ra.tmem) {
+  if (TC) {
     // every tile waited for its last commit, so no MMA is in flight
     tc_fence_before();
     __syncthreads();
@@ -2548,15 +2554,22 @@ size_t engine_smem_bytes() { return (size_t)ENGINE_SMEM_DOUBLES * sizeof(double)
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream) {
   if (ra.smem_doubles < ENGINE_SMEM_BASE_DOUBLES || ra.smem_doubles > ENGINE_SMEM_DOUBLES) return cudaErrorInvalidValue;
   size_t smem = (size_t)ra.smem_doubles * sizeof(double);
-  engine_kernel<<<grid, NTHREADS, smem, stream>>>(ra);
+  if (ra.tmem) engine_kernel<true><<<grid, NTHREADS, smem, stream>>>(ra);
+  else engine_kernel<false><<<grid, NTHREADS, smem, stream>>>(ra);
   return cudaGetLastError();
 }
 
 int engine_occupancy(int* blocks_per_sm) {
   size_t smem = engine_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -1;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel, NTHREADS, smem);
+  int other = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<false>, NTHREADS, smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&other, engine_kernel<true>, NTHREADS, smem);
+  if (e == cudaSuccess && other < *blocks_per_sm) *blocks_per_sm = other;
   return e == cudaSuccess ? 0 : -1;
 }
 
