@@ -383,7 +383,9 @@ def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5, grid2d
            "flops": flops, "nsn": int(s.Nsn), "values": int(s.blkptr[-1]),
            "errors_against": "reference C kernels (oracle/_ref), FP64, same inputs"}
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for prec in ("fp64", "tf32", "tf32x3"):
+    for key in ("fp64", "tf32", "tf32x3", "tf32_tcgen05"):
+        prec = "tf32" if key == "tf32_tcgen05" else key
+        s.plan().set_option("tf32_tcgen05", 1 if key == "tf32_tcgen05" else None)
         X = cp.cspmatrix(s, blkval=X0.blkval.clone())
         times = []
         for it in range(reps + 2):
@@ -409,6 +411,8 @@ def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5, grid2d
         entry["factor_rel_error"] = float(np.abs(Lh - Lr).max() / np.abs(Lr).max())
         if prec == "fp64":
             entry["parity_scaled_error"] = max(workload.block_errors(s, Lh, Lr), workload.block_errors(s, Yh, Yr))
+        elif key == "tf32_tcgen05":
+            entry["tiles"] = "tcgen05.mma kind::tf32, accumulators in tensor memory"
         else:
             B = torch.from_numpy(np.asfortranarray(np.random.default_rng(11).standard_normal((s.n, nrhs)))).to(dev)
             mixed.solve(X0, Lm, B, tol=1e-12, maxiter=40)     # warm-up: builds the solve programs
@@ -420,8 +424,10 @@ def mixed_precision_section(dev, side=48, merge=(64, 64), nrhs=8, reps=5, grid2d
             sms = ev0.elapsed_time(ev1)
             entry["solve"] = {"nrhs": nrhs, "iterations": srep["iterations"], "residual": srep["residuals"][-1],
                               "ms": round(sms, 3), "ms_per_iteration": round(sms / srep["iterations"], 3)}
-        out[prec] = entry
+        out[key] = entry
+    s.plan().set_option("tf32_tcgen05", None)
     out["speedup_tf32"] = round(out["fp64"]["ms"] / out["tf32"]["ms"], 3)
+    out["speedup_tf32_tcgen05"] = round(out["fp64"]["ms"] / out["tf32_tcgen05"]["ms"], 3)
     out["speedup_tf32x3"] = round(out["fp64"]["ms"] / out["tf32x3"]["ms"], 3)
     return out
 
@@ -588,6 +594,18 @@ def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
             "gradient_rel_error_vs_reference": abs(gU - want) / abs(want),
             "gradient_fd_rel_error": abs(gU - fd) / abs(fd), "fd_step": h,
             "hvp_rel_error_vs_reference": abs(second - second_ref) / abs(second_ref)}
+
+
+def _engine_occupancy():
+    """Resident CTAs per SM of the persistent kernel's two builds (FP64 and
+    the one with tcgen05 TF32 tiles)."""
+    import ctypes
+    from chompack_b200 import _native as N
+    out = {}
+    for name, tc in (("fp64", 0), ("tcgen05", 1)):
+        v = ctypes.c_int()
+        out[name] = v.value if N.engine_occupancy(tc, ctypes.byref(v)) == 0 else None
+    return out
 
 
 # ------------------------------------------------------------------- main
@@ -844,6 +862,7 @@ def main():
                          "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (FP64; MEASURED_PEAKS.json "
                                         "lists bf16 and HBM only)"},
             "parity": parity,
+            "engine_ctas_per_sm": _engine_occupancy(),
             "kernel_ms": {o: round(kern[o] * 1e3, 4) for o in ops},
             "other_sweeps": other,
         }

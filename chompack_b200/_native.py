@@ -123,4 +123,6 @@ diag = _sig("chb_diag", ctypes.c_int, [PPLAN, vp, vp, vp])
 # ---- program-build options (chb_plan_set_option)
 plan_set_option = _sig("chb_plan_set_option", ctypes.c_int, [PPLAN, ctypes.c_int, i64])
 plan_get_option = _sig("chb_plan_get_option", ctypes.c_int, [PPLAN, ctypes.c_int, ctypes.POINTER(i64)])
-OPTIONS = {"small_front_nj": 0, "subtrees": 1, "chol_ksplit": 2, "pinv_ksplit": 3, "fused_la": 4}
+OPTIONS = {"small_front_nj": 0, "subtrees": 1, "chol_ksplit": 2, "pinv_ksplit": 3, "fused_la": 4,
+           "tf32_tcgen05": 5}
+engine_occupancy = _sig("chb_engine_occupancy", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int)])

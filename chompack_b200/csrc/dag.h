@@ -577,6 +577,13 @@ inline bool subtrees_on(const chb_plan& P) {
   return std::getenv("CHB_NO_SUBTREES") == nullptr;
 }
 
+// TF32 tiles on tcgen05 (CHB_OPT_TF32_TCGEN05 = 1, or CHB_TF32_TCGEN05 in
+// the environment) instead of the warp-level mma.sync tiles (the default).
+inline bool tf32_tcgen05(const chb_plan& P) {
+  if (P.opt[CHB_OPT_TF32_TCGEN05] >= 0) return P.opt[CHB_OPT_TF32_TCGEN05] != 0;
+  return std::getenv("CHB_TF32_TCGEN05") != nullptr;
+}
+
 // cholesky's fused diagonal task (CHB_OPT_FUSED_LA = 1, the default where it
 // is safe) or separate look-ahead tasks (0; also CHB_NO_FUSED_LA).
 inline bool fused_la_allowed(const chb_plan& P) {

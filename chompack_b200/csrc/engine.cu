@@ -2559,17 +2559,16 @@ cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-int engine_occupancy(int* blocks_per_sm) {
+// Resident CTAs per SM of one instantiation (tc: the tcgen05 one).  The
+// dynamic shared-memory attribute is raised on both.
+int engine_occupancy(int* blocks_per_sm, bool tc) {
   size_t smem = engine_smem_bytes();
   cudaError_t e = cudaFuncSetAttribute(engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -1;
-  int other = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<false>, NTHREADS, smem);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&other, engine_kernel<true>, NTHREADS, smem);
-  if (e == cudaSuccess && other < *blocks_per_sm) *blocks_per_sm = other;
+  e = tc ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<true>, NTHREADS, smem)
+         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<false>, NTHREADS, smem);
   return e == cudaSuccess ? 0 : -1;
 }
 

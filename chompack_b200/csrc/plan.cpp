@@ -238,10 +238,9 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.spin_limit = plan->spin_limit >= 0 ? plan->spin_limit : kDefaultSpinLimit;
   ra.trace = (plan->trace && plan->trace_cap >= (int64_t)prog->tasks.size()) ? plan->trace : nullptr;
   ra.perm = plan->d_perm;
-  // TF32 tiles on tcgen05 unless CHB_TF32_MMA_SYNC asks for the warp-level
-  // mma.sync tiles (kept for comparison)
-  static const bool tf32_mma_sync = std::getenv("CHB_TF32_MMA_SYNC") != nullptr;
-  ra.tmem = prog->tf32_tiles && !tf32_mma_sync ? 1 : 0;
+  // TF32 tiles as warp-level mma.sync, or on tcgen05 with tensor-memory
+  // accumulators when the plan asks for it
+  ra.tmem = prog->tf32_tiles && tf32_tcgen05(*plan) ? 1 : 0;
   ra.ldb = run_ldb;
   ra.alpha = run_alpha;
   // The plan's schedule, else CHB_SCHEDULE (static | dynamic), else the
@@ -285,7 +284,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
     if (rs) return rs;
     CUDA_TRY(cudaEventRecord(plan->ev_start, stream));
   }
-  int grid = std::min<int64_t>(plan->grid, (int64_t)prog->tasks.size());
+  int grid = std::min<int64_t>(ra.tmem ? plan->grid_tc : plan->grid, (int64_t)prog->tasks.size());
   CUDA_TRY(engine_launch(ra, grid, stream));
   if (!io) return 0;
   if (io_in) {
@@ -361,6 +360,9 @@ static int upload_plan(chb_plan* P) {
   if (engine_occupancy(&per_sm) != 0 || per_sm <= 0) return set_error(-12, "engine kernel cannot be resident");
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
   P->grid = per_sm * nsm;
+  int per_sm_tc = 0;
+  if (engine_occupancy(&per_sm_tc, true) != 0 || per_sm_tc <= 0) return set_error(-12, "engine kernel cannot be resident");
+  P->grid_tc = per_sm_tc * nsm;
   return 0;
 }
 
@@ -632,8 +634,16 @@ extern "C" int chb_plan_get_option(const chb_plan* plan, int option, int64_t* va
     case CHB_OPT_CHOL_KSPLIT: *value = chol_ksplit(*plan); break;
     case CHB_OPT_PINV_KSPLIT: *value = pinv_ksplit(*plan); break;
     case CHB_OPT_FUSED_LA: *value = fused_la_allowed(*plan) ? 1 : 0; break;
+    case CHB_OPT_TF32_TCGEN05: *value = tf32_tcgen05(*plan) ? 1 : 0; break;
     default: return set_error(-2, "unknown option %d", option);
   }
+  return 0;
+}
+
+extern "C" int chb_engine_occupancy(int tcgen05, int* blocks_per_sm) {
+  clear_error();
+  if (!blocks_per_sm) return set_error(-1, "null argument");
+  if (engine_occupancy(blocks_per_sm, tcgen05 != 0) != 0) return set_error(-12, "occupancy query failed");
   return 0;
 }
 

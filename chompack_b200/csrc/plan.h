@@ -99,10 +99,11 @@ struct chb_plan {
   int64_t* d_perm = nullptr;    // p (trsm row gather)
   std::vector<int64_t> seg;     // matrices of a merged plan: supernodes [seg[m], seg[m+1])
   int64_t* d_seg = nullptr;
-  int grid = 0;                 // persistent grid size
+  int grid = 0;                 // persistent grid size (the FP64 instantiation)
+  int grid_tc = 0;              // persistent grid size of the tcgen05 instantiation
   int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
   int64_t spin_limit = -1;      // polls before a wait gives up; -1: the default (kDefaultSpinLimit)
-  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1};  // program-build options (-1: default)
+  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1, -1};  // program-build options (-1: default)
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;
@@ -150,7 +151,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
 // Device entry points implemented in engine.cu.
 size_t engine_smem_bytes();
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream);
-int engine_occupancy(int* blocks_per_sm);
+int engine_occupancy(int* blocks_per_sm, bool tc = false);
 cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, double* partial, double* out,
                           cudaStream_t stream);
 cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,

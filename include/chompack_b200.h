@@ -343,6 +343,9 @@ int chb_plan_set_schedule(chb_plan* plan, int mode);
  *                           tiles (multiple of 64, 0 = whole)
  *   CHB_OPT_PINV_KSPLIT     projected_inverse: K chunk of its long-K tiles
  *   CHB_OPT_FUSED_LA        cholesky: fused diagonal task (1/0)
+ *   CHB_OPT_TF32_TCGEN05    mixed precision: TF32 tiles on tcgen05 with
+ *                           tensor-memory accumulators (1) or warp-level
+ *                           mma.sync (0, the default)
  * chb_plan_get_option gives the value the next program build uses. */
 enum chb_option {
   CHB_OPT_SMALL_FRONT_NJ = 0,
@@ -350,7 +353,8 @@ enum chb_option {
   CHB_OPT_CHOL_KSPLIT = 2,
   CHB_OPT_PINV_KSPLIT = 3,
   CHB_OPT_FUSED_LA = 4,
-  CHB_OPT_COUNT = 5
+  CHB_OPT_TF32_TCGEN05 = 5,
+  CHB_OPT_COUNT = 6
 };
 int chb_plan_set_option(chb_plan* plan, int option, int64_t value);
 int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value);
@@ -361,6 +365,12 @@ int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value);
  * early and chb_info returns -30.  polls < 0 restores the default (about
  * 10 s of polling).  Small values are for tests of that failure path. */
 int chb_plan_set_spin_limit(chb_plan* plan, int64_t polls);
+
+/* Diagnostics: resident CTAs per SM of the persistent sweep kernel on the
+ * current device, for the FP64 build of the kernel (tcgen05 = 0) or the one
+ * with the TF32 tiles on tcgen05 (tcgen05 = 1); a sweep launches that many
+ * per SM. */
+int chb_engine_occupancy(int tcgen05, int* blocks_per_sm);
 
 /* Allocation-free Cholesky.  No counterpart in the reference: an addition for
  * callers that cannot call cudaMalloc when they factor (frameworks whose

@@ -88,8 +88,8 @@ def test_host_values_in_mixed_precision():
 
 
 def test_tcgen05_tiles_agree_with_mma_sync_tiles(tmp_path):
-    """The TF32 tiles run on tcgen05 (tensor-memory accumulators); with
-    CHB_TF32_MMA_SYNC set they run as warp-level mma.sync.  Both round the
+    """The TF32 tiles run as warp-level mma.sync; with CHB_TF32_TCGEN05 set
+    they run on tcgen05 (tensor-memory accumulators).  Both round the
     same FP64 operands to TF32 and accumulate in FP32 (in different orders),
     so the factors agree far below the TF32 error itself (which the FP64
     comparison bounds), and both are far from garbage."""
@@ -102,14 +102,14 @@ def test_tcgen05_tiles_agree_with_mma_sync_tiles(tmp_path):
     cp.cholesky(L, precision="tf32")
     L64 = cp.cspmatrix(s, blkval=X.blkval.clone())
     cp.cholesky(L64)
-    out = tmp_path / "mma_sync.npy"
+    out = tmp_path / "tcgen05.npy"
     code = ("import sys, numpy as np; sys.path.insert(0, %r); sys.path.insert(0, %r)\n"
             "import chompack_b200 as cp\nfrom helpers import problem\n"
             "A, s = problem('grid3d', 14, merge=(32, 32), seed=5)\n"
             "X = cp.cspmatrix(s, device='cuda') + A\ncp.cholesky(X, precision='tf32')\n"
             "np.save(%r, X.blkval.cpu().numpy())\n") % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
                                                         os.path.dirname(os.path.abspath(__file__)), str(out))
-    env = dict(os.environ, CHB_TF32_MMA_SYNC="1")
+    env = dict(os.environ, CHB_TF32_TCGEN05="1")
     subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
     other = np.load(out)
     got = L.blkval.cpu().numpy()
