@@ -222,8 +222,8 @@ extern "C" int chb_symv(chb_plan* plan, const double* blkval, const int64_t* snc
   if (rc) return rc;
   if (!blkval || !sncolptr || !snrowidx || !x || !y) return set_error(-1, "null argument");
   if (nrhs < 0 || ld < plan->n) return set_error(-1, "symv: nrhs >= 0 and ld >= n required");
-  cudaError_t e = symv_launch(blkval, plan->d_fronts, sncolptr, snrowidx, plan->d_perm, x, y, (int)plan->nsn,
-                              (int)nrhs, ld, alpha, (cudaStream_t)stream);
+  cudaError_t e = symv_launch(blkval, plan->d_fronts, plan->d_symv_items, plan->n_symv_items, sncolptr, snrowidx,
+                              plan->d_perm, x, y, (int)nrhs, ld, alpha, (cudaStream_t)stream);
   if (e != cudaSuccess) return set_error(-100 - (int)e, "symv launch failed: %s", cudaGetErrorString(e));
   return 0;
 }

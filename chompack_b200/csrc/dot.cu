@@ -99,68 +99,106 @@ __global__ void __launch_bounds__(DOT_THREADS) seg_final(const double* __restric
 }
 // y += alpha X x for the symmetric chordal matrix X in blkval (lower
 // trapezoid of each supernode block; both triangles applied), nrhs columns
-// of leading dimension ld, rows in the original order through perm.  One
-// CTA per supernode k (nn columns, nj rows):
-//   rows: y[row i] += sum_j X(i, j) x[col j] with one thread per row (the
-//         diagonal block read symmetrically), one atomic per row;
-//   columns: y[col j] += sum_{i >= nn} X(i, j) x[row i] for the rows below
-//         the diagonal block, one warp per column, one atomic per column.
-// The atomics make the last bits of y depend on the schedule.
-constexpr int SYMV_RHS = 8;  // right-hand sides per pass
-__global__ void __launch_bounds__(DOT_THREADS) symv_blocks(const double* __restrict__ blkval,
+// of leading dimension ld, rows in the original order through perm.
+// One CTA per strip of 64 rows of a supernode block (items[] = (k, first
+// row)); the strip is walked in 64 x 64 tiles of its stored lower part,
+// staged in shared memory with coalesced loads, so every stored entry is
+// read from memory once.  From each tile:
+//   rows:    y[row i] += sum_j X(i, j) x[col j]   over stored j <= i,
+//   columns: y[col j] += sum_i X(i, j) x[row i]   over stored i >  j,
+// which together apply the symmetric matrix once.  Four threads share a
+// row (or column) and reduce through shared memory; each strip adds its
+// rows once and its columns once per right-hand side with atomics, so the
+// last bits of y depend on the schedule.
+constexpr int SYMV_RHS = 8;   // right-hand sides per pass
+constexpr int SYMV_T = 64;    // strip height and tile width
+constexpr int SYMV_LD = SYMV_T + 1;
+__global__ void __launch_bounds__(DOT_THREADS) symv_strips(const double* __restrict__ blkval,
                                                            const FrontDesc* __restrict__ fronts,
+                                                           const int2* __restrict__ items, int nitems,
                                                            const int64_t* __restrict__ sncolptr,
                                                            const int64_t* __restrict__ snrowidx,
                                                            const int64_t* __restrict__ perm, const double* __restrict__ x,
-                                                           double* __restrict__ y, int nsn, int nrhs, int64_t ld,
-                                                           double alpha) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = blockIdx.x; k < nsn; k += gridDim.x) {
-    const FrontDesc f = fronts[k];
-    const int nn = f.nn, nj = f.nj;
-    const int64_t* __restrict__ rows = snrowidx + sncolptr[k];
+                                                           double* __restrict__ y, int nrhs, int64_t ld, double alpha) {
+  // the tile, and (once its entries are consumed) the 4-way reductions
+  __shared__ double tile[SYMV_T * SYMV_LD];
+  __shared__ double xr[SYMV_RHS][SYMV_T];   // x at the strip's rows
+  __shared__ double xc[SYMV_RHS][SYMV_T];   // x at the tile's columns
+  static_assert(4 * SYMV_RHS * SYMV_T <= SYMV_T * SYMV_LD, "reduction buffer exceeds the tile");
+  double (*red)[SYMV_RHS][SYMV_T] = reinterpret_cast<double (*)[SYMV_RHS][SYMV_T]>(tile);
+  __shared__ int64_t grow[SYMV_T], gcol[SYMV_T];
+  const int t = threadIdx.x, lr = t & (SYMV_T - 1), q = t >> 6;  // q = 0..3
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = items[it];
+    const FrontDesc f = fronts[w.x];
+    const int nn = f.nn, nj = f.nj, i0 = w.y;
+    const int mi = min(SYMV_T, nj - i0);
+    const int64_t* __restrict__ rows = snrowidx + sncolptr[w.x];
     const double* __restrict__ b = blkval + f.blk;
+    const int jend = min(nn, i0 + mi);  // columns holding stored entries of the strip
     for (int r0 = 0; r0 < nrhs; r0 += SYMV_RHS) {
       const int nr = min(SYMV_RHS, nrhs - r0);
-      // rows
-      for (int i = threadIdx.x; i < nj; i += DOT_THREADS) {
-        double acc[SYMV_RHS];
-#pragma unroll
-        for (int r = 0; r < SYMV_RHS; r++) acc[r] = 0.0;
-        for (int j = 0; j < nn; j++) {
-          const double v = (i >= j) ? b[(int64_t)j * nj + i] : b[(int64_t)i * nj + j];
-          const int64_t C = perm[rows[j]];
-#pragma unroll
-          for (int r = 0; r < SYMV_RHS; r++)
-            if (r < nr) acc[r] = fma(v, x[C + (r0 + r) * ld], acc[r]);
-        }
-        const int64_t R = perm[rows[i]];
-#pragma unroll
-        for (int r = 0; r < SYMV_RHS; r++)
-          if (r < nr) atomicAdd(y + R + (r0 + r) * ld, alpha * acc[r]);
+      __syncthreads();
+      if (t < SYMV_T) grow[t] = t < mi ? perm[rows[i0 + t]] : 0;
+      __syncthreads();
+      for (int e = t; e < SYMV_RHS * SYMV_T; e += DOT_THREADS) {
+        const int r = e / SYMV_T, ii = e % SYMV_T;
+        xr[r][ii] = (r < nr && ii < mi) ? x[grow[ii] + (r0 + r) * ld] : 0.0;
       }
-      // columns, from the rows below the diagonal block
-      for (int j = warp; j < nn; j += DOT_THREADS / 32) {
-        double acc[SYMV_RHS];
+      double racc[SYMV_RHS];
 #pragma unroll
-        for (int r = 0; r < SYMV_RHS; r++) acc[r] = 0.0;
-        for (int i = nn + lane; i < nj; i += 32) {
-          const double v = b[(int64_t)j * nj + i];
-          const int64_t R = perm[rows[i]];
-#pragma unroll
-          for (int r = 0; r < SYMV_RHS; r++)
-            if (r < nr) acc[r] = fma(v, x[R + (r0 + r) * ld], acc[r]);
+      for (int r = 0; r < SYMV_RHS; r++) racc[r] = 0.0;
+      for (int j0 = 0; j0 < jend; j0 += SYMV_T) {
+        const int mj = min(SYMV_T, jend - j0);
+        __syncthreads();
+        if (t < SYMV_T) gcol[t] = t < mj ? perm[rows[j0 + t]] : 0;
+        // tile(ii, jj) = X(i0 + ii, j0 + jj) where stored (row >= column)
+        for (int c = q; c < SYMV_T; c += 4) {
+          const int gi = i0 + lr, gj = j0 + c;
+          tile[c * SYMV_LD + lr] = (lr < mi && c < mj && gi >= gj) ? b[(int64_t)gj * nj + gi] : 0.0;
         }
-#pragma unroll
-        for (int r = 0; r < SYMV_RHS; r++) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+        __syncthreads();
+        for (int e = t; e < SYMV_RHS * SYMV_T; e += DOT_THREADS) {
+          const int r = e / SYMV_T, jj = e % SYMV_T;
+          xc[r][jj] = (r < nr && jj < mj) ? x[gcol[jj] + (r0 + r) * ld] : 0.0;
         }
-        if (lane == 0) {
-          const int64_t C = perm[rows[j]];
+        __syncthreads();
+        // rows: thread (row lr, columns c = q mod 4)
+        for (int c = q; c < mj; c += 4) {
+          const double v = tile[c * SYMV_LD + lr];
 #pragma unroll
-          for (int r = 0; r < SYMV_RHS; r++)
-            if (r < nr) atomicAdd(y + C + (r0 + r) * ld, alpha * acc[r]);
+          for (int r = 0; r < SYMV_RHS; r++) racc[r] = fma(v, xc[r][c], racc[r]);
+        }
+        // columns: thread (column lr, rows ii = q mod 4), strictly below the diagonal
+        double cacc[SYMV_RHS];
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++) cacc[r] = 0.0;
+        for (int ii = q; ii < mi; ii += 4) {
+          const double v = (i0 + ii > j0 + lr) ? tile[lr * SYMV_LD + ii] : 0.0;
+#pragma unroll
+          for (int r = 0; r < SYMV_RHS; r++) cacc[r] = fma(v, xr[r][ii], cacc[r]);
+        }
+        __syncthreads();  // every thread is done with the tile's entries
+#pragma unroll
+        for (int r = 0; r < SYMV_RHS; r++) red[q][r][lr] = cacc[r];
+        __syncthreads();
+        for (int e = t; e < SYMV_RHS * SYMV_T; e += DOT_THREADS) {
+          const int r = e / SYMV_T, jj = e % SYMV_T;
+          if (r < nr && jj < mj) {
+            const double s = red[0][r][jj] + red[1][r][jj] + red[2][r][jj] + red[3][r][jj];
+            if (s != 0.0) atomicAdd(y + gcol[jj] + (r0 + r) * ld, alpha * s);
+          }
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < SYMV_RHS; r++) red[q][r][lr] = racc[r];
+      __syncthreads();
+      for (int e = t; e < SYMV_RHS * SYMV_T; e += DOT_THREADS) {
+        const int r = e / SYMV_T, ii = e % SYMV_T;
+        if (r < nr && ii < mi) {
+          const double s = red[0][r][ii] + red[1][r][ii] + red[2][r][ii] + red[3][r][ii];
+          atomicAdd(y + grow[ii] + (r0 + r) * ld, alpha * s);
         }
       }
     }
@@ -169,11 +207,13 @@ __global__ void __launch_bounds__(DOT_THREADS) symv_blocks(const double* __restr
 
 }  // namespace
 
-cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int64_t* sncolptr,
-                        const int64_t* snrowidx, const int64_t* perm, const double* x, double* y, int nsn, int nrhs,
-                        int64_t ld, double alpha, cudaStream_t stream) {
-  if (nsn <= 0 || nrhs <= 0) return cudaSuccess;
-  symv_blocks<<<nsn, DOT_THREADS, 0, stream>>>(blkval, fronts, sncolptr, snrowidx, perm, x, y, nsn, nrhs, ld, alpha);
+cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int2* items, int nitems,
+                        const int64_t* sncolptr, const int64_t* snrowidx, const int64_t* perm, const double* x,
+                        double* y, int nrhs, int64_t ld, double alpha, cudaStream_t stream) {
+  if (nitems <= 0 || nrhs <= 0) return cudaSuccess;
+  const int grid = nitems < 65535 ? nitems : 65535;
+  symv_strips<<<grid, DOT_THREADS, 0, stream>>>(blkval, fronts, items, nitems, sncolptr, snrowidx, perm, x, y, nrhs,
+                                                 ld, alpha);
   return cudaGetLastError();
 }
 

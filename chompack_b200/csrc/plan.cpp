@@ -354,6 +354,17 @@ static int upload_plan(chb_plan* P) {
     CUDA_TRY(cudaMalloc(&P->d_perm, n * sizeof(int64_t)));
     CUDA_TRY(cudaMemcpy(P->d_perm, P->perm.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
   }
+  {
+    // the strips of the chordal SYMV (chb_symv): 64 rows of a block each
+    std::vector<int2> items;
+    for (int64_t k = 0; k < P->nsn; k++)
+      for (int i0 = 0; i0 < P->fronts[k].nj; i0 += 64) items.push_back(make_int2((int)k, i0));
+    P->n_symv_items = (int)items.size();
+    if (!items.empty()) {
+      CUDA_TRY(cudaMalloc(&P->d_symv_items, items.size() * sizeof(int2)));
+      CUDA_TRY(cudaMemcpy(P->d_symv_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    }
+  }
   CUDA_TRY(cudaMalloc(&P->d_seg, P->seg.size() * sizeof(int64_t)));
   CUDA_TRY(cudaMemcpy(P->d_seg, P->seg.data(), P->seg.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
   int per_sm = 0, nsm = 0;
@@ -516,6 +527,7 @@ extern "C" int chb_plan_destroy(chb_plan* plan) {
   if (plan->d_chidx) cudaFree(plan->d_chidx);
   if (plan->d_perm) cudaFree(plan->d_perm);
   if (plan->d_seg) cudaFree(plan->d_seg);
+  if (plan->d_symv_items) cudaFree(plan->d_symv_items);
   delete plan;
   return 0;
 }

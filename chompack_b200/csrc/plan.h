@@ -99,6 +99,8 @@ struct chb_plan {
   int64_t* d_perm = nullptr;    // p (trsm row gather)
   std::vector<int64_t> seg;     // matrices of a merged plan: supernodes [seg[m], seg[m+1])
   int64_t* d_seg = nullptr;
+  int2* d_symv_items = nullptr;  // 64-row strips of the supernode blocks (supernode, first row)
+  int n_symv_items = 0;
   int grid = 0;                 // persistent grid size (the FP64 instantiation)
   int grid_tc = 0;              // persistent grid size of the tcgen05 instantiation
   int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
@@ -157,9 +159,9 @@ cudaError_t logdet_launch(const double* l, const FrontDesc* fronts, int nsn, dou
 cudaError_t symw_launch(const double* x, double* y, double alpha, const FrontDesc* fronts, int nsn,
                         cudaStream_t stream);
 cudaError_t segment_sums(const double* partial, const int64_t* seg, int count, double* out, cudaStream_t stream);
-cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int64_t* sncolptr,
-                        const int64_t* snrowidx, const int64_t* perm, const double* x, double* y, int nsn, int nrhs,
-                        int64_t ld, double alpha, cudaStream_t stream);
+cudaError_t symv_launch(const double* blkval, const FrontDesc* fronts, const int2* items, int nitems,
+                        const int64_t* sncolptr, const int64_t* snrowidx, const int64_t* perm, const double* x,
+                        double* y, int nrhs, int64_t ld, double alpha, cudaStream_t stream);
 cudaError_t logdet_partials(const double* l, const FrontDesc* fronts, int nsn, double* partial, cudaStream_t stream);
 cudaError_t dot_partials(const double* x, const double* y, const FrontDesc* fronts, int nsn, double* partial,
                          cudaStream_t stream);
