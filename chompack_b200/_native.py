@@ -119,6 +119,8 @@ syr2 = _sig("chb_syr2", ctypes.c_int, [PPLAN, vp, vp, vp, vp, vp, ctypes.c_doubl
 add_projection = _sig("chb_add_projection", ctypes.c_int, [PPLAN, vp, vp, vp, vp, i64, ctypes.c_double,
                                                            ctypes.c_double, ctypes.c_int, vp])
 diag = _sig("chb_diag", ctypes.c_int, [PPLAN, vp, vp, vp])
+add_sparse = _sig("chb_add_sparse", ctypes.c_int, [PPLAN, vp, vp, vp, i64, vp, vp, vp, ctypes.c_double, ctypes.c_int,
+                                                   vp, vp])
 
 # ---- program-build options (chb_plan_set_option)
 plan_set_option = _sig("chb_plan_set_option", ctypes.c_int, [PPLAN, ctypes.c_int, i64])

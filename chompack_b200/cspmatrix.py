@@ -161,6 +161,10 @@ class cspmatrix(object):
         (symbolic.py:1138-1174)."""
         assert self.is_factor is False, "cannot add spmatrix to a cspmatrix factor"
         X = as_spmatrix(X)
+        if X.size[0] != self.symb.n or X.size[1] != self.symb.n:
+            raise ValueError("sparse matrix must be of order n")
+        if self.blkval.device.type == "cuda":
+            return self._iadd_spmatrix_device(X, alpha)
         Xs = symmetrize(X)
         ip = self.symb.ip
         I, J, V = ip[Xs._I], ip[Xs._J], Xs._V
@@ -173,6 +177,27 @@ class cspmatrix(object):
         dev = self.blkval.device
         self.blkval.index_add_(0, torch.from_numpy(np.ascontiguousarray(idx, dtype=np.int64)).to(dev),
                                torch.from_numpy(np.ascontiguousarray(alpha * V, dtype=np.float64)).to(dev))
+
+    def _iadd_spmatrix_device(self, X, alpha):
+        """The same addition on the device (chb_add_sparse): the triplets of
+        X's lower triangle are copied over and placed by one thread each."""
+        from . import _native as N
+        s = self.symb
+        dev = self.blkval.device
+        lo = X._I >= X._J
+        I = torch.from_numpy(np.ascontiguousarray(X._I[lo], dtype=np.int64)).to(dev)
+        J = torch.from_numpy(np.ascontiguousarray(X._J[lo], dtype=np.int64)).to(dev)
+        V = torch.from_numpy(np.ascontiguousarray(X._V[lo], dtype=np.float64)).to(dev)
+        colptr, rowidx = _symbolic_arrays(s, dev)
+        bad = torch.zeros(1, dtype=torch.int64, device=dev)
+        plan = s.plan(dev.index)
+        rc = N.add_sparse(plan.handle, self.blkval.data_ptr(), colptr.data_ptr(), rowidx.data_ptr(), int(I.numel()),
+                          I.data_ptr(), J.data_ptr(), V.data_ptr(), float(alpha), 0, bad.data_ptr(),
+                          torch.cuda.current_stream(dev).cuda_stream)
+        if rc < 0:
+            raise RuntimeError("add_sparse failed: %s" % N.last_error().decode())
+        if int(bad.item()) != 0:
+            raise ValueError("sparse matrix entry outside the chordal pattern")
 
     def add_projection(self, A, alpha=1.0, beta=1.0, reordered=False):
         """X := alpha*proj(A) + beta*X for a dense symmetric A

@@ -13,9 +13,13 @@
 // * projection — X := alpha P(A) + beta X for a dense A (symbolic.py:1176-1210):
 //   every entry of each block (the reference updates whole blocks).
 // * diag       — the diagonal entries (symbolic.py:1113-1128).
+// * add_sparse — X += alpha tril(P(symmetrize(A))) for a sparse A given as
+//   (I, J, V) triplets in the original numbering (cspmatrix += spmatrix,
+//   symbolic.py:1138-1174).
 //
-// One CTA per supernode block (grid-stride), columns across warps, rows
-// across lanes: reads and writes of blkval are coalesced column segments.
+// The block kernels run one CTA per supernode block (grid-stride), columns
+// across warps, rows across lanes: reads and writes of blkval are coalesced
+// column segments.  add_sparse runs one thread per triplet.
 #include <cuda_runtime.h>
 
 #include "../../include/chompack_b200.h"
@@ -112,6 +116,63 @@ __global__ void __launch_bounds__(EX_THREADS) diag_blocks(const double* __restri
   }
 }
 
+// One thread per triplet (grid-stride).  symmetrize() reads only the lower
+// entries (i >= j) of A and mirrors them, perm() renumbers through p and
+// tril() keeps the lower copy, so each lower entry of A lands once, at
+// (max, min) of (ip[i], ip[j]).  The supernode holding column j is the last
+// k with col0 <= j (binary search over the fronts, which are in column
+// order), the row's position the index of i in the clique's ascending row
+// list (binary search); the entry is added at
+// blk + (j - col0) nj + position.  An entry whose row is not in the list
+// (outside the chordal pattern) or whose index is out of range is counted
+// in *bad and not written.  Values are added with atomics, so duplicated
+// triplets are summed; a duplicate-free A (an spmatrix) adds each position
+// once, alpha * v as the reference does.
+__global__ void __launch_bounds__(EX_THREADS) add_sparse_entries(
+    double* __restrict__ blkval, const FrontDesc* __restrict__ fronts, int nsn, int64_t n,
+    const int64_t* __restrict__ sncolptr, const int64_t* __restrict__ snrowidx, const int64_t* __restrict__ iperm,
+    int64_t nnz, const int64_t* __restrict__ I, const int64_t* __restrict__ J, const double* __restrict__ V,
+    double alpha, unsigned long long* __restrict__ bad) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    int64_t i = I[e], j = J[e];
+    if (i < 0 || j < 0 || i >= n || j >= n) {
+      atomicAdd(bad, 1ull);
+      continue;
+    }
+    if (i < j) continue;
+    if (iperm) {
+      i = iperm[i];
+      j = iperm[j];
+    }
+    if (i < j) {
+      const int64_t t = i;
+      i = j;
+      j = t;
+    }
+    int lo = 0, hi = nsn - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (fronts[mid].col0 <= j) lo = mid;
+      else hi = mid - 1;
+    }
+    const int64_t col0 = fronts[lo].col0, blk = fronts[lo].blk;
+    const int nj = fronts[lo].nj, nn = fronts[lo].nn;
+    const int64_t* __restrict__ ri = snrowidx + sncolptr[lo];
+    int a = 0, b = nj;
+    while (a < b) {
+      const int m = (a + b) >> 1;
+      if (ri[m] < i) a = m + 1;
+      else b = m;
+    }
+    if (j - col0 >= nn || a == nj || ri[a] != i) {
+      atomicAdd(bad, 1ull);
+      continue;
+    }
+    atomicAdd(blkval + blk + (j - col0) * nj + a, alpha * V[e]);
+  }
+}
+
 int grid_for(int nsn) { return nsn < 8192 ? nsn : 8192; }
 
 }  // namespace
@@ -180,4 +241,24 @@ extern "C" int chb_diag(chb_plan* plan, const double* blkval, double* d, void* s
   diag_blocks<<<grid_for((int)plan->nsn), EX_THREADS, 0, (cudaStream_t)stream>>>(blkval, plan->d_fronts,
                                                                                    (int)plan->nsn, d);
   return ex_done("diag");
+}
+
+extern "C" int chb_add_sparse(chb_plan* plan, double* blkval, const int64_t* sncolptr, const int64_t* snrowidx,
+                              int64_t nnz, const int64_t* I, const int64_t* J, const double* V, double alpha,
+                              int reordered, unsigned long long* bad, void* stream) {
+  clear_error();
+  int rc = ex_check(plan);
+  if (rc) return rc;
+  if (nnz < 0) return set_error(-1, "negative nnz");
+  if (!blkval || !sncolptr || !snrowidx || !bad || (nnz > 0 && (!I || !J || !V)))
+    return set_error(-1, "null argument");
+  if (cudaMemsetAsync(bad, 0, sizeof(unsigned long long), (cudaStream_t)stream) != cudaSuccess)
+    return ex_done("add_sparse");
+  if (nnz == 0 || plan->nsn == 0) return 0;
+  const int64_t want = (nnz + EX_THREADS - 1) / EX_THREADS;
+  const int grid = (int)(want < 148 * 64 ? want : 148 * 64);
+  add_sparse_entries<<<grid, EX_THREADS, 0, (cudaStream_t)stream>>>(
+      blkval, plan->d_fronts, (int)plan->nsn, plan->n, sncolptr, snrowidx, reordered ? nullptr : plan->d_iperm, nnz,
+      I, J, V, alpha, bad);
+  return ex_done("add_sparse");
 }

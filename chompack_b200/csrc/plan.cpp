@@ -353,6 +353,10 @@ static int upload_plan(chb_plan* P) {
   if (n > 0) {
     CUDA_TRY(cudaMalloc(&P->d_perm, n * sizeof(int64_t)));
     CUDA_TRY(cudaMemcpy(P->d_perm, P->perm.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    std::vector<int64_t> ip(n);
+    for (int64_t i = 0; i < n; i++) ip[P->perm[i]] = i;
+    CUDA_TRY(cudaMalloc(&P->d_iperm, n * sizeof(int64_t)));
+    CUDA_TRY(cudaMemcpy(P->d_iperm, ip.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
   }
   {
     // the strips of the chordal SYMV (chb_symv): 64 rows of a block each
@@ -395,6 +399,14 @@ extern "C" int chb_plan_create(int64_t n, int64_t nsn, const int64_t* snptr, con
   P->snptr.assign(snptr, snptr + nsn + 1);
   P->snode.assign(snode, snode + n);
   P->perm.assign(p, p + n);
+  {
+    std::vector<char> seen(n, 0);
+    for (int64_t i = 0; i < n; i++) {
+      const int64_t v = P->perm[i];
+      if (v < 0 || v >= n || seen[v]) return set_error(-5, "p is not a permutation of 0..n-1");
+      seen[v] = 1;
+    }
+  }
   const int64_t nrel = relptr[nsn];
   P->relidx.resize(nrel);
   for (int64_t i = 0; i < nrel; i++) {
@@ -526,6 +538,7 @@ extern "C" int chb_plan_destroy(chb_plan* plan) {
   if (plan->d_relidx) cudaFree(plan->d_relidx);
   if (plan->d_chidx) cudaFree(plan->d_chidx);
   if (plan->d_perm) cudaFree(plan->d_perm);
+  if (plan->d_iperm) cudaFree(plan->d_iperm);
   if (plan->d_seg) cudaFree(plan->d_seg);
   if (plan->d_symv_items) cudaFree(plan->d_symv_items);
   delete plan;

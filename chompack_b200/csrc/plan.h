@@ -97,6 +97,7 @@ struct chb_plan {
   int32_t* d_relidx = nullptr;
   int32_t* d_chidx = nullptr;
   int64_t* d_perm = nullptr;    // p (trsm row gather)
+  int64_t* d_iperm = nullptr;   // inverse of p (sparse assembly)
   std::vector<int64_t> seg;     // matrices of a merged plan: supernodes [seg[m], seg[m+1])
   int64_t* d_seg = nullptr;
   int2* d_symv_items = nullptr;  // 64-row strips of the supernode blocks (supernode, first row)

@@ -10,10 +10,11 @@ release and claim delay (a ready task that no CTA had taken yet: under the
 static list order its list position had not been reached, under the
 dynamic schedule every CTA was busy).
 
-    python -m chompack_b200.trace --side 40 --merge 32 32
+    python -m chompack_b200.trace --side 40 --merge 32 32 [--trsm 8]
 
 prints the summary for cholesky and projected_inverse on the 3-D 7-point
-grid side^3 (AMD order, merge_size_fill(merge)); it needs a GPU.
+grid side^3 (AMD order, merge_size_fill(merge)), and with --trsm R for the
+triangular solves 'N' and 'T' with R right-hand sides; it needs a GPU.
 """
 import argparse
 import ctypes
@@ -35,7 +36,7 @@ TASK = np.dtype({
 })
 
 OP_NAMES = ["GEMM", "POTRF", "ASM", "MROW", "EXTRACT", "COPY", "INV", "RPOTRF", "QL", "VEC", "NOP", "LA",
-            "SUM", "SIGNAL", "ARRIVAL", "FRONT", "PFRONT"]
+            "SUM", "SIGNAL", "ARRIVAL", "FRONT", "PFRONT", "SUBTREE", "PSUBTREE"]
 T_POTRF, T_LA = 1, 11
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
@@ -154,6 +155,7 @@ def main():
     ap.add_argument("--merge", type=int, nargs=2, default=(32, 32))
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--path", action="store_true", help="also list the path's tasks")
+    ap.add_argument("--trsm", type=int, default=0, help="also trace trsm with this many right-hand sides")
     args = ap.parse_args()
     import torch
     import chompack_b200 as cp
@@ -168,13 +170,20 @@ def main():
     sweeps = (("cholesky", N.OP_CHOLESKY, lambda: cp.cholesky(cp.cspmatrix(s, blkval=x0.clone(), factor=False))),
               ("projected_inverse", N.OP_PROJECTED_INVERSE,
                lambda: cp.projected_inverse(cp.cspmatrix(s, blkval=l0.clone(), factor=True))))
+    if args.trsm > 0:
+        L = cp.cspmatrix(s, blkval=l0, factor=True)
+        B0 = torch.randn(args.trsm, s.n, dtype=torch.float64, device="cuda").t()   # column-major
+        for trans in ("N", "T"):
+            sweeps += (("trsm_" + trans, N.OP_TRSM, lambda tr=trans: cp.trsm(L, B0.clone().t().contiguous().t(),
+                                                                              trans=tr)),)
     out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d)"
                        % (args.side, s.n, args.merge[0], args.merge[1])}
     for name, op, fn in sweeps:
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
-        tasks, waits, tr = record(plan, op, fn)
+        k, flags = (args.trsm, int(name == "trsm_T")) if op == N.OP_TRSM else (0, 0)
+        tasks, waits, tr = record(plan, op, fn, k, flags)
         res = critical_path(tasks, waits, tr)
         if not args.path:
             res.pop("path")

@@ -243,6 +243,19 @@ int chb_add_projection(chb_plan* plan, double* blkval, const int64_t* sncolptr, 
                        void* stream);
 int chb_diag(chb_plan* plan, const double* blkval, double* d, void* stream);
 
+/* chb_add_sparse — X += alpha tril(P(symmetrize(A))) for a sparse A of order
+ *   n given as nnz (I, J, V) triplets in device memory (cspmatrix +=
+ *   spmatrix, symbolic.py:1138-1174): only A's lower entries (I >= J) are
+ *   read; each is renumbered through p (unless `reordered`), swapped into the
+ *   lower triangle and added into the block that holds it.  Triplets outside
+ *   the chordal pattern or with an index outside [0, n) are skipped and
+ *   counted in *bad (a device word, zeroed first); the caller reads it after
+ *   the stream's work and raises, as the reference's lookup would.  Repeated
+ *   triplets are summed. */
+int chb_add_sparse(chb_plan* plan, double* blkval, const int64_t* sncolptr, const int64_t* snrowidx, int64_t nnz,
+                   const int64_t* I, const int64_t* J, const double* V, double alpha, int reordered,
+                   unsigned long long* bad, void* stream);
+
 /* Product-form Cholesky factor of I + V diag(a) V^T = L_1...L_k L_k^T...L_1^T
  * (V n x k), each L_i held as column i of V, L and B (pfcholesky.c:52-136;
  * the reference's pfcholesky class composes them with the chordal factor,
