@@ -700,6 +700,22 @@ inline SplitTask add_split_gemm(DagBuilder& B, const Task& t, int kc, int64_t sc
   return st;
 }
 
+// Column groups of the vector extend-add and extract tasks (T_VEC with
+// VEC_ASM / VEC_EXTRACT, columns [aux[2], aux[3])): the right-hand sides of
+// a front are split so that a task moves about 2,048 elements (sixteen per
+// thread, loaded eight at a time), and so that the columns of [x_k; u_k]
+// an extend-add stages fit the base shared memory.  Returns the columns per
+// task.
+inline int vec_cols_per_task(int64_t elems_per_col, int64_t nrhs, int64_t staged_per_col) {
+  int64_t g = (elems_per_col * nrhs + 2047) / 2048;
+  g = std::max<int64_t>(1, std::min<int64_t>(g, nrhs));
+  if (staged_per_col > 0) {
+    const int64_t fit = std::max<int64_t>(1, ENGINE_SMEM_BASE_DOUBLES / staged_per_col);
+    g = std::max<int64_t>(g, (nrhs + fit - 1) / fit);
+  }
+  return (int)((nrhs + g - 1) / g);
+}
+
 // Small-subtree bundles (T_SUBTREE / T_PSUBTREE).  A subtree qualifies when
 // every front in it has nj <= SUB_NJ (and the small-front tasks are on);
 // the maximal ones are cut into warp ranges (adjacent subtrees in postorder

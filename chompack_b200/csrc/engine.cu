@@ -922,20 +922,31 @@ __device__ void run_sum(const RunArgs& ra, const Task& t) {
   const int64_t stride = (int64_t)(uint32_t)t.aux[1];
   const bool lower = t.cmode == CM_LOWER;
   constexpr int E = TILE * TILE / NTHREADS / 2;  // elements per thread and half
-  // a thread's elements of one partial are loaded together (E loads in
-  // flight), partial after partial; two halves keep the registers in check
+  constexpr int U = 4;                            // partials loaded together
+  // a thread's elements of U partials are loaded together (up to U E loads
+  // in flight), then added partial after partial in index order; two halves
+  // keep the registers in check
 #pragma unroll 1
   for (int half = 0; half < 2; half++) {
     double acc[E];
 #pragma unroll
     for (int e = 0; e < E; e++) acc[e] = 0.0;
-    for (int q = 0; q < np; q++) {
-      const double* Pq = P + q * stride;
+    for (int q0 = 0; q0 < np; q0 += U) {
+      double v[U][E];
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
-        if (r < m && c < n) acc[e] += __ldcg(Pq + (int64_t)c * ldp + r);
+      for (int u = 0; u < U; u++) {
+        const double* Pq = P + (q0 + u) * stride;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
+          v[u][e] = (q0 + u < np && r < m && c < n) ? __ldcg(Pq + (int64_t)c * ldp + r) : 0.0;
+        }
       }
+#pragma unroll
+      for (int u = 0; u < U; u++)
+#pragma unroll
+        for (int e = 0; e < E; e++)
+          if (q0 + u < np) acc[e] += v[u][e];
     }
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -2107,7 +2118,7 @@ __device__ void run_ql(const RunArgs& ra, const Task& t, double* smem) {
 // aux[0], nrhs = t.n right-hand sides).  Bp / x_k live at operand a or c
 // with leading dimension n; the per-front vector updates u_k (na x nrhs,
 // ld na) start at WS + b.off + vpos[k] * nrhs.
-__device__ void run_vec(const RunArgs& ra, const Task& t) {
+__device__ void run_vec(const RunArgs& ra, const Task& t, double* smem) {
   const int mode = t.aux[0], nrhs = t.n;
   if (mode == VEC_GATHER || mode == VEC_SCATTER) {
     const int r0 = t.aux[1], r1 = t.aux[2];
@@ -2140,24 +2151,92 @@ __device__ void run_vec(const RunArgs& ra, const Task& t) {
   }
   double* __restrict__ WS = ra.bases[B_WS];
   const int64_t vbase = t.b.off;
+  // right-hand-side columns [j0, j1) of this task (aux[3] == 0: all)
+  const int j0 = t.aux[2], j1 = t.aux[3] > 0 ? t.aux[3] : nrhs, nc = j1 - j0;
+  constexpr int E = 8;  // elements per thread with their loads in flight together
   if (mode == VEC_ASM) {
     const FrontDesc f = ra.fronts[t.aux[1]];
     double* __restrict__ xk = ra.bases[t.a.base] + t.a.off;
     const int ldx = t.a.ld;
     double* __restrict__ uk = ra.bases[t.c.base] + t.c.off;
-    for (int idx = threadIdx.x; idx < f.na * nrhs; idx += NTHREADS) uk[idx] = 0.0;
+    const int nj = f.nj;
+    if ((int64_t)nj * nc <= ENGINE_SMEM_BASE_DOUBLES) {
+      // [x_k; u_k] columns staged in shared memory (u_k part zero), the
+      // children added there, the result stored once
+      for (int base = 0; base < nj * nc; base += E * NTHREADS) {
+        double v[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int idx = base + threadIdx.x + e * NTHREADS;
+          const int i = idx % nj, j = j0 + idx / nj;
+          v[e] = (idx < nj * nc && i < f.nn) ? __ldcg(xk + i + (int64_t)j * ldx) : 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int idx = base + threadIdx.x + e * NTHREADS;
+          if (idx < nj * nc) smem[idx] = v[e];
+        }
+      }
+      __syncthreads();
+      for (int l = f.chend - 1; l >= f.chbeg; l--) {
+        const FrontDesc ch = ra.fronts[ra.chidx[l]];
+        const int Nc = ch.na, tot = Nc * nc;
+        const int32_t* __restrict__ r = ra.relidx + ch.relptr;
+        const double* __restrict__ uc = WS + vbase + ch.vpos * nrhs + (int64_t)j0 * Nc;
+        for (int base = 0; base < tot; base += E * NTHREADS) {
+          int dst[E];
+          double v[E];
+#pragma unroll
+          for (int e = 0; e < E; e++) {
+            const int idx = base + threadIdx.x + e * NTHREADS;
+            const int i = idx % max(Nc, 1), j = idx / max(Nc, 1);
+            dst[e] = (idx < tot) ? __ldg(r + i) + j * nj : -1;
+            v[e] = (idx < tot) ? __ldcg(uc + idx) : 0.0;
+          }
+          // a child's relative indices are distinct: no two elements of one
+          // pass meet in shared memory
+#pragma unroll
+          for (int e = 0; e < E; e++)
+            if (dst[e] >= 0) smem[dst[e]] += v[e];
+        }
+        __syncthreads();
+      }
+      for (int idx = threadIdx.x; idx < nj * nc; idx += NTHREADS) {
+        const int i = idx % nj, j = j0 + idx / nj;
+        if (i < f.nn) xk[i + (int64_t)j * ldx] = smem[idx];
+        else uk[(i - f.nn) + (int64_t)j * f.na] = smem[idx];
+      }
+      return;
+    }
+    // too tall for shared memory: zero u_k's columns, add in global memory
+    for (int idx = threadIdx.x; idx < f.na * nc; idx += NTHREADS)
+      uk[(idx % f.na) + (int64_t)(j0 + idx / f.na) * f.na] = 0.0;
     __syncthreads();
     for (int l = f.chend - 1; l >= f.chbeg; l--) {
       const FrontDesc ch = ra.fronts[ra.chidx[l]];
-      const int Nc = ch.na;
+      const int Nc = ch.na, tot = Nc * nc;
       const int32_t* __restrict__ r = ra.relidx + ch.relptr;
-      const double* __restrict__ uc = WS + vbase + ch.vpos * nrhs;
-      for (int idx = threadIdx.x; idx < Nc * nrhs; idx += NTHREADS) {
-        const int i = idx % Nc, j = idx / Nc;
-        const int row = __ldg(r + i);
-        const double v = __ldcg(uc + idx);
-        if (row < f.nn) xk[row + (int64_t)j * ldx] += v;
-        else uk[(row - f.nn) + (int64_t)j * f.na] += v;
+      const double* __restrict__ uc = WS + vbase + ch.vpos * nrhs + (int64_t)j0 * Nc;
+      for (int base = 0; base < tot; base += E * NTHREADS) {
+        double* dst[E];
+        double v[E], old[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int idx = base + threadIdx.x + e * NTHREADS;
+          const int i = idx % max(Nc, 1), j = j0 + idx / max(Nc, 1);
+          dst[e] = nullptr;
+          v[e] = 0.0;
+          if (idx < tot) {
+            const int row = __ldg(r + i);
+            dst[e] = (row < f.nn) ? xk + row + (int64_t)j * ldx : uk + (row - f.nn) + (int64_t)j * f.na;
+            v[e] = __ldcg(uc + idx);
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) old[e] = dst[e] ? __ldcg(dst[e]) : 0.0;
+#pragma unroll
+        for (int e = 0; e < E; e++)
+          if (dst[e]) *dst[e] = old[e] + v[e];
       }
       __syncthreads();
     }
@@ -2169,13 +2248,30 @@ __device__ void run_vec(const RunArgs& ra, const Task& t) {
   const double* __restrict__ xp = ra.bases[t.a.base] + t.a.off;
   const int ldx = t.a.ld;
   const double* __restrict__ up = ra.bases[t.c.base] + t.c.off;
-  const int Nc = ch.na;
+  const int Nc = ch.na, tot = Nc * nc;
   const int32_t* __restrict__ r = ra.relidx + ch.relptr;
-  double* __restrict__ uc = WS + vbase + ch.vpos * nrhs;
-  for (int idx = threadIdx.x; idx < Nc * nrhs; idx += NTHREADS) {
-    const int i = idx % Nc, j = idx / Nc;
-    const int row = __ldg(r + i);
-    uc[idx] = (row < f.nn) ? __ldcg(xp + row + (int64_t)j * ldx) : __ldcg(up + (row - f.nn) + (int64_t)j * f.na);
+  double* __restrict__ uc = WS + vbase + ch.vpos * nrhs + (int64_t)j0 * Nc;
+  for (int base = 0; base < tot; base += E * NTHREADS) {
+    int row[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int idx = base + threadIdx.x + e * NTHREADS;
+      row[e] = (idx < tot) ? __ldg(r + idx % max(Nc, 1)) : -1;
+    }
+    double v[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int idx = base + threadIdx.x + e * NTHREADS;
+      const int j = j0 + idx / max(Nc, 1);
+      v[e] = row[e] < 0 ? 0.0
+                        : (row[e] < f.nn ? __ldcg(xp + row[e] + (int64_t)j * ldx)
+                                         : __ldcg(up + (row[e] - f.nn) + (int64_t)j * f.na));
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int idx = base + threadIdx.x + e * NTHREADS;
+      if (row[e] >= 0) uc[idx] = v[e];
+    }
   }
 }
 
@@ -2483,7 +2579,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_PSUBTREE: run_subtrees(ra, t, smem); break;
       case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
-      case T_VEC: run_vec(ra, t); break;
+      case T_VEC: run_vec(ra, t, smem); break;
       case T_QL: run_ql(ra, t, smem); break;
       case T_NOP: break;
       case T_SUM: run_sum(ra, t); break;

@@ -396,16 +396,20 @@ class VM(object):
         vbase = int(t["b"]["off"])
         xb, xo, ldx = self.bases[int(t["a"]["base"])], int(t["a"]["off"]), int(t["a"]["ld"])
         ub, uo = self.bases[int(t["c"]["base"])], int(t["c"]["off"])
+        # right-hand-side columns [aux[2], aux[3]) (aux[3] == 0: all)
+        j0 = int(t["aux"][2])
+        j1 = int(t["aux"][3]) if int(t["aux"][3]) > 0 else nrhs
         if mode == 2:
             f = self.p.fronts[int(t["aux"][1])]
             nn, na = int(f["nn"]), int(f["na"])
-            ub[uo: uo + na * nrhs] = 0.0
+            for j in range(j0, j1):
+                ub[uo + j * na: uo + (j + 1) * na] = 0.0
             for l in range(int(f["chend"]) - 1, int(f["chbeg"]) - 1, -1):
                 ch = self.p.fronts[self.chidx[l]]
                 Nc = int(ch["na"])
                 r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
                 uc = WS[vbase + int(ch["vpos"]) * nrhs: vbase + int(ch["vpos"]) * nrhs + Nc * nrhs].reshape((Nc, nrhs), order="F")
-                for j in range(nrhs):
+                for j in range(j0, j1):
                     top = r < nn
                     xb[xo + r[top] + j * ldx] += uc[top, j]
                     ub[uo + (r[~top] - nn) + j * na] += uc[~top, j]
@@ -415,7 +419,7 @@ class VM(object):
         nn, na, Nc = int(f["nn"]), int(f["na"]), int(ch["na"])
         r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
         base = vbase + int(ch["vpos"]) * nrhs
-        for j in range(nrhs):
+        for j in range(j0, j1):
             top = r < nn
             vals = np.empty(Nc)
             vals[top] = xb[xo + r[top] + j * ldx]

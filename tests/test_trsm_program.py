@@ -1,0 +1,78 @@
+"""The triangular-solve task program (csrc/build_trsm.cpp) on fronts large
+enough for every one of its forms, run by the interpreter (taskvm) in
+random and dynamic orders and compared with the reference's trsm
+(src/C/trsm.c, oracle/_ref) on the same factor:
+
+* diagonal blocks of several 64-row tiles, so that the substitution steps
+  carry the neighbouring block's update ([-G_c | M_c] for 'N', [M_c; -H_c]
+  for 'T');
+* long products W x_k (K = nn) and W^T u_k (K = na) beyond 128, split
+  into partial tiles and one T_SUM;
+* extend-add and extract tasks split by right-hand-side columns.
+
+Tolerance: 1e-12 relative to the largest entry of the column (the GPU
+tests use the same measure)."""
+import numpy as np
+import pytest
+
+import chompack_b200 as cp
+from chompack_b200 import _native as N
+from chompack_b200.plan import Plan
+import taskvm
+from helpers import problem
+from oracle import ref
+
+
+@pytest.fixture(scope="module")
+def grid16():
+    if not ref.available():
+        pytest.skip("reference kernels not built")
+    # merge_size_fill(300, 300) on the 16^3 grid: 12 supernodes, fronts with
+    # nn up to 525 and na up to 303, ten with nn > 256 below the root
+    A, s = problem("grid3d", 16, merge=(300, 300), seed=1)
+    x = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    assert ref.cholesky(s, x) == 0
+    return s, x
+
+
+def _tasks(s, nrhs, trans):
+    pl = Plan(s, device=-1)
+    return taskvm.Program(pl.handle, N.OP_TRSM, k=nrhs, flags=1 if trans == "T" else 0, nsn=s.Nsn)
+
+
+def test_program_has_every_form(grid16):
+    s, _ = grid16
+    nn = np.diff(np.asarray(s.snptr))
+    na = np.diff(np.asarray(s.sncolptr)) - nn
+    assert np.any((nn > 256) & (na > 0)) and na.max() > 256
+    for trans in ("N", "T"):
+        prog = _tasks(s, 8, trans)
+        t = prog.tasks
+        assert int(np.sum(t["op"] == taskvm.T_SUM)) > 0, trans
+        gemm = t[t["op"] == taskvm.T_GEMM]
+        assert int(np.sum(gemm["k"] > 64)) > 0, trans          # fused substitution steps
+        vec = t[(t["op"] == taskvm.T_VEC) & (t["aux"][:, 0] >= 2)]
+        assert int(np.sum(vec["aux"][:, 3] - vec["aux"][:, 2] < 8)) > 0, trans   # column-split tasks
+
+
+@pytest.mark.parametrize("trans", ["N", "T"])
+@pytest.mark.parametrize("nrhs", [1, 8, 70])
+@pytest.mark.parametrize("order", ["random", "dynamic"])
+def test_program_matches_reference(grid16, trans, nrhs, order):
+    s, L = grid16
+    B0 = np.asfortranarray(np.random.default_rng(nrhs).standard_normal((s.n, nrhs)))
+    want = B0.copy(order="F")
+    ref.trsm(s, L.copy(), want, alpha=0.5, trans=trans)
+    pl = Plan(s, device=-1)
+    flags = 1 if trans == "T" else 0
+    prog = taskvm.Program(pl.handle, N.OP_TRSM, k=nrhs, flags=flags, nsn=s.Nsn)
+    Bf = B0.reshape(-1, order="F").copy()
+    bases = {0: L.copy(), 1: np.full(prog.ws_doubles, np.nan), 4: Bf}
+    vm = taskvm.VM(prog, bases, s.relidx, s.chidx, perm=s.p, ldb=s.n, alpha=0.5)
+    if order == "dynamic":
+        vm.run("dynamic", seed=nrhs, schedule=taskvm.Schedule(pl.handle, N.OP_TRSM, k=nrhs, flags=flags))
+    else:
+        vm.run("random", seed=nrhs)
+    got = Bf.reshape(B0.shape, order="F")
+    err = np.max(np.abs(got - want) / np.maximum(np.abs(want).max(axis=0), 1e-300))
+    assert err <= 1e-12, err
