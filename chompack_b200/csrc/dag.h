@@ -249,7 +249,12 @@ struct DagBuilder {
       case T_GEMM: return 3.0 + 6.0 * mnk;
       case T_MROW: return 11.0 + 6.0 * mnk;
       case T_LA: return 15.0;
-      case T_POTRF: return t.aux[2] ? 11.0 : 27.0;  // invert-only : factor + inverse
+      case T_POTRF: {
+        // invert-only : factor + inverse, for the 16-column blocks that meet
+        // the tile (a full tile has four)
+        const double nb = (double)((t.m + 15) / 16);
+        return (t.aux[2] ? 11.0 : 27.0) * (0.25 + 0.1875 * nb);
+      }
       case T_SUM: return 3.0 + 0.5 * t.aux[0];
       case T_COPY: return 3.5;
       default: return 6.0;

@@ -495,6 +495,45 @@ __device__ __forceinline__ void mma_block(const double* sA, const double* sB, in
   mma_block_ld<LDS, LDS>(sA, sB, kn, acc);
 }
 
+// The m16 and n8 tiles of the calling warp's 32x32 sub-tile that meet an
+// m x n product (warp-uniform): mi in 0..2, nj in 0..4.
+__device__ __forceinline__ void warp_tiles(int m, int n, int& mi, int& nj) {
+  const int warp = threadIdx.x >> 5;
+  const int r = m - (warp >> 1) * 32, c = n - (warp & 1) * 32;
+  mi = r <= 0 ? 0 : (r >= 32 ? 2 : (r + 15) >> 4);
+  nj = c <= 0 ? 0 : (c >= 32 ? 4 : (c + 7) >> 3);
+}
+
+// mma_block for a partial tile: only the warp's first mi m16 and nj n8
+// tiles are multiplied (the others hold rows or columns outside the
+// product, which the epilogue does not store).  A narrow product (a few
+// right-hand sides, the edge tiles of a front) then issues a fraction of
+// the MMAs of a full 64x64 tile.
+__device__ __forceinline__ void mma_block_part(const double* sA, const double* sB, int kn, Acc& acc, int mi,
+                                               int nj) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int r0 = (warp >> 1) * 32 + g, c0 = (warp & 1) * 32 + g;
+#pragma unroll 2
+  for (int kk = 0; kk < kn; kk += 4) {
+    double a[2][2], b[4];
+    const double* ak = sA + (kk + q) * LDS + r0;
+    const double* bk = sB + (kk + q) * LDS + c0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      a[i][0] = i < mi ? ak[16 * i] : 0.0;
+      a[i][1] = i < mi ? ak[16 * i + 8] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) b[j] = j < nj ? bk[8 * j] : 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (i < mi && j < nj) dmma16(acc[i][j], a[i][0], a[i][1], b[j]);
+  }
+}
+
 __device__ __forceinline__ void zero_acc(Acc& acc) {
 #pragma unroll
   for (int i = 0; i < 2; i++)
@@ -597,6 +636,9 @@ __device__ void gemm_acc_p(const Opnd& A, const Opnd& B, int m, int n, int K, co
   zero_acc(acc);
   const int nch = (K + KC - 1) / KC;
   double* const ring = sm.A;
+  int wmi, wnj;
+  warp_tiles(m, n, wmi, wnj);
+  const bool full = wmi == 2 && wnj == 4;
 #pragma unroll
   for (int c = 0; c < GEMM_STAGES - 1; c++) {
     if (c < nch) {
@@ -619,7 +661,8 @@ __device__ void gemm_acc_p(const Opnd& A, const Opnd& B, int m, int n, int K, co
     int kn = min(KC, K - c * KC);
     if (PREC == PREC_FP64) {
       kn = (kn + 3) & ~3;
-      mma_block(st, st + KC * LDS, kn, acc);
+      if (full) mma_block(st, st + KC * LDS, kn, acc);
+      else if (wmi > 0 && wnj > 0) mma_block_part(st, st + KC * LDS, kn, acc, wmi, wnj);
     } else {
       kn = (kn + 7) & ~7;
       mma_block_tf32<PREC == PREC_TF32X3>(st, st + KC * LDS, kn, accf);
@@ -921,13 +964,15 @@ __device__ void run_sum(const RunArgs& ra, const Task& t) {
   const int ldp = t.a.ld, ldc = t.c.ld, m = t.m, n = t.n, np = t.aux[0];
   const int64_t stride = (int64_t)(uint32_t)t.aux[1];
   const bool lower = t.cmode == CM_LOWER;
-  constexpr int E = TILE * TILE / NTHREADS / 2;  // elements per thread and half
+  constexpr int NQ = 4;                            // quarters of the tile
+  constexpr int E = TILE * TILE / NTHREADS / NQ;  // elements per thread and quarter
   constexpr int U = 4;                            // partials loaded together
   // a thread's elements of U partials are loaded together (up to U E loads
-  // in flight), then added partial after partial in index order; two halves
+  // in flight), then added partial after partial in index order; quarters
   // keep the registers in check
 #pragma unroll 1
-  for (int half = 0; half < 2; half++) {
+  for (int qt = 0; qt < NQ; qt++) {
+    if (qt * E * NTHREADS / TILE >= n) break;  // the quarter's columns start at or after n
     double acc[E];
 #pragma unroll
     for (int e = 0; e < E; e++) acc[e] = 0.0;
@@ -938,7 +983,7 @@ __device__ void run_sum(const RunArgs& ra, const Task& t) {
         const double* Pq = P + (q0 + u) * stride;
 #pragma unroll
         for (int e = 0; e < E; e++) {
-          const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
+          const int idx = threadIdx.x + (qt * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
           v[u][e] = (q0 + u < np && r < m && c < n) ? __ldcg(Pq + (int64_t)c * ldp + r) : 0.0;
         }
       }
@@ -950,7 +995,7 @@ __device__ void run_sum(const RunArgs& ra, const Task& t) {
     }
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int idx = threadIdx.x + (half * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
+      const int idx = threadIdx.x + (qt * E + e) * NTHREADS, r = idx % TILE, c = idx / TILE;
       if (r >= m || c >= n || (lower && r + t.cdiag < c)) continue;
       double v = t.alpha * acc[e];
       if (t.beta != 0.0) v += t.beta * __ldcg(C + (int64_t)c * ldc + r);
@@ -1364,10 +1409,13 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   __syncthreads();
   POTRF_STAMP(0);
 #pragma unroll 1
-  for (int J = 0; J < 4; J++) {
+  // only the 16-column blocks that meet the b x b tile (the padding is the
+  // identity and is neither factored nor inverted)
+  const int NJ = (b + 15) >> 4, NB = 16 * NJ;
+  for (int J = 0; J < NJ; J++) {
     const int j0 = 16 * J, j1 = j0 + 16, jp = j0 - 16;
-    const bool panel = factor && J > 0;  // panel of block J-1 and the updates it feeds
-    const bool below = panel && J < 3;   // rows below block J to update
+    const bool panel = factor && J > 0;     // panel of block J-1 and the updates it feeds
+    const bool below = panel && J < NJ - 1; // rows below block J to update
     if (warp == 0) {
       if (panel) {
         potrf_panel_rows(sL, sM, jp, j0);
@@ -1456,10 +1504,10 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
     } else {
       if (below) {
         const int rb = j0 + 16 * warp;  // warps 1, 2: the panel rows below block J
-        if (rb < TILE) potrf_panel_rows(sL, sM, jp, rb);
+        if (rb < NB) potrf_panel_rows(sL, sM, jp, rb);
         named_bar_sync(1, NTHREADS);
         // rows >= j1, columns >= j0, lower part, from the panel of block J-1
-        const int nti = (TILE - j1) / 16, ntj = (TILE - j0) / 8;
+        const int nti = (NB - j1) / 16, ntj = (NB - j0) / 8;
         for (int tt = warp - 1; tt < nti * ntj; tt += NTHREADS / 32 - 1) {
           const int r0 = j1 + 16 * (tt / ntj), c0 = j0 + 8 * (tt % ntj);
           if (c0 <= r0 + 15) potrf_syrk_tile(sL, jp, r0, c0);
@@ -1480,8 +1528,8 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   }
   POTRF_STAMP(5);
   if (!want_inv) return;
-  // the last block row of the inverse (rows 1 and 2 were assembled above)
-  potrf_inv_row(sL, sM, sT + 128 * warp, 3, warp, NTHREADS / 32);
+  // the last block row of the inverse (rows 1 .. NJ-2 were assembled above)
+  if (NJ >= 2) potrf_inv_row(sL, sM, sT + 128 * warp, NJ - 1, warp, NTHREADS / 32);
   __syncthreads();
   POTRF_STAMP(6);
 #pragma unroll 8

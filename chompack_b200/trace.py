@@ -156,10 +156,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--path", action="store_true", help="also list the path's tasks")
     ap.add_argument("--trsm", type=int, default=0, help="also trace trsm with this many right-hand sides")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="trace the first BATCH matrices of the uneven 2-D batch in one merged plan instead")
+    ap.add_argument("--dump", default="", help="also save each sweep's task records and raw trace (.npz)")
     args = ap.parse_args()
     import torch
     import chompack_b200 as cp
     from chompack_b200 import grids
+    if args.batch:
+        return trace_batch(args)
     A = grids.grid3d(args.side, seed=0)
     s = cp.symbolic(A, p=cp.amd.order(A), merge_function=cp.merge_size_fill(*args.merge))
     x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.cuda()
@@ -184,6 +189,37 @@ def main():
         torch.cuda.synchronize()
         k, flags = (args.trsm, int(name == "trsm_T")) if op == N.OP_TRSM else (0, 0)
         tasks, waits, tr = record(plan, op, fn, k, flags)
+        if args.dump:
+            np.savez_compressed("%s_%s.npz" % (args.dump, name), tasks=tasks, waits=waits, trace=tr)
+        res = critical_path(tasks, waits, tr)
+        if not args.path:
+            res.pop("path")
+        out[name] = res
+    print(json.dumps(out, indent=1))
+
+
+def trace_batch(args):
+    """cholesky and projected_inverse over the first args.batch matrices of
+    the uneven batch (2-D grids of side 20..120 with two extra neighbours,
+    AMD, no merging), one merged plan."""
+    import torch
+    import chompack_b200 as cp
+    from chompack_b200 import grids
+    specs = grids.uneven_batch_specs()[:args.batch]
+    As = [grids.grid2d_extra(sd, seed=seed) for sd, seed in specs]
+    Bt = cp.batch([cp.symbolic(A, p=cp.amd.order(A)) for A in As])
+    x0 = Bt.assemble(As)
+    l0 = x0.clone()
+    Bt.cholesky(l0)
+    plan = Bt.plan
+    sweeps = (("cholesky", N.OP_CHOLESKY, lambda: Bt.cholesky(x0.clone())),
+              ("projected_inverse", N.OP_PROJECTED_INVERSE, lambda: Bt.projected_inverse(l0.clone())))
+    out = {"workload": "uneven 2-D batch, first %d matrices, one merged plan" % args.batch}
+    for name, op, fn in sweeps:
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        tasks, waits, tr = record(plan, op, fn)
         res = critical_path(tasks, waits, tr)
         if not args.path:
             res.pop("path")
