@@ -205,18 +205,28 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
     auto xop = [&](int c, int s, uint8_t mode) {
       return opnd(B_WS, xk + c * T + (int64_t)s * T * n, (int)n, mode);
     };
-    // the step of block c (K spans x_{c-1}, x_c for 'N'; x_c, x_{c+1} for 'T')
+    // the step of block c (K spans x_{c-1}, x_c for 'N'; x_c, x_{c+1} for
+    // 'T'), a T_TRSV task: its operand is staged before its mid waits
     auto step = [&](int c, int s) {
       const int ld = sld[k][c];
+      Task t;
       if (!trans) {
-        if (c == 0) return gemm(bw(0), rw(s), bw(0), 1.0, opnd(B_WS, soff[k][0], ld), xop(0, s, OM_T), 0.0,
-                                xop(0, s, OM_N));
-        return gemm(bw(c), rw(s), T + bw(c), 1.0, opnd(B_WS, soff[k][c], ld), xop(c - 1, s, OM_T), 0.0,
-                    xop(c, s, OM_N));
+        if (c == 0) t = gemm(bw(0), rw(s), bw(0), 1.0, opnd(B_WS, soff[k][0], ld), xop(0, s, OM_T), 0.0,
+                             xop(0, s, OM_N));
+        else t = gemm(bw(c), rw(s), T + bw(c), 1.0, opnd(B_WS, soff[k][c], ld), xop(c - 1, s, OM_T), 0.0,
+                      xop(c, s, OM_N));
+      } else {
+        const int K = bw(c) + (c + 1 < NBc ? bw(c + 1) : 0);
+        t = gemm(bw(c), rw(s), K, 1.0, opnd(B_WS, soff[k][c], ld, OM_T), xop(c, s, OM_T), 0.0, xop(c, s, OM_N));
       }
-      const int K = bw(c) + (c + 1 < NBc ? bw(c + 1) : 0);
-      return gemm(bw(c), rw(s), K, 1.0, opnd(B_WS, soff[k][c], ld, OM_T), xop(c, s, OM_T), 0.0, xop(c, s, OM_N));
+      t.op = T_TRSV;
+      return t;
     };
+    // Waits of a step: the operand's producers (and the inputs every step
+    // shares) before it starts, with the step two back, so that at most two
+    // steps of a chain hold a CTA; the step before and the last update of
+    // its own x tile in the middle, after its operand copies are issued.
+    const double STEP_US = 3.0;
     std::vector<int> last(NBc * nrt, -1);
     if (!trans) {
       // children's updates into x_k and u_k (u_k zeroed first), by columns
@@ -254,16 +264,20 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
         }
       // x_k := L^{-1} x_k, block forward substitution: the step of block c
       // takes the update from block c-1; the other updates are tile products
-      std::vector<int> prev(nrt, -1);
+      std::vector<int> prev(nrt, -1), prev2(nrt, -1);
       for (int c = 0; c < NBc; c++) {
         for (int s = 0; s < nrt; s++) {
           const int sol = B.add(step(c, s), {lv, 2 + 2 * c, 0, (int)k, s, c}, xfinal);
           B.wait_task(sol, inv[k][c]);
           B.wait_task(sol, coup[k][c]);
           B.wait_group(sol, agrp);
-          for (int id : readers) B.wait_task(sol, id);
-          B.wait_task(sol, last[c * nrt + s]);
-          B.wait_task(sol, prev[s]);
+          if (c == 0)
+            for (int id : readers) B.wait_task(sol, id);  // the later steps follow this one
+          B.wait_task(sol, prev2[s]);
+          B.wait_mid(sol, last[c * nrt + s]);
+          B.wait_mid(sol, prev[s]);
+          B.split_task(sol, STEP_US, true);
+          prev2[s] = prev[s];
           prev[s] = sol;
           for (int r = c + 2; r < NBc; r++) {
             Operand a = opnd(B_X, blk + (int64_t)(c * T) * nj + r * T, nj);
@@ -278,15 +292,18 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
     } else {
       const int from_parent = (f.parent != (int)k) ? ugrp[k] : -1;  // u_k, written by the parent
       // x_k := L^{-T} x_k, block backward substitution
-      std::vector<int> prev(nrt, -1);
+      std::vector<int> prev(nrt, -1), prev2(nrt, -1);
       for (int c = NBc - 1; c >= 0; c--) {
         for (int s = 0; s < nrt; s++) {
           const int sol = B.add(step(c, s), {lv, 2 * (NBc - c), 0, (int)k, s, c}, (c == 0 && na == 0) ? xfinal : -1);
           B.wait_task(sol, inv[k][c]);
           B.wait_task(sol, coup[k][c]);
           B.wait_group(sol, gath);
-          B.wait_task(sol, last[c * nrt + s]);
-          B.wait_task(sol, prev[s]);
+          B.wait_task(sol, prev2[s]);
+          B.wait_mid(sol, last[c * nrt + s]);
+          B.wait_mid(sol, prev[s]);
+          B.split_task(sol, STEP_US, true);
+          prev2[s] = prev[s];
           prev[s] = sol;
           for (int r = 0; r + 1 < c; r++) {
             Operand a = opnd(B_X, blk + (int64_t)(r * T) * nj + c * T, nj, OM_T);

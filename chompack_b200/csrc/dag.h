@@ -57,6 +57,9 @@ struct DagBuilder {
   // the dynamic schedule releases the task on the first ones only.
   std::vector<std::vector<int>> mid_waits;
   std::vector<double> post_cost;
+  // A split task whose own counter is raised only at its end (T_TRSV): its
+  // waiters follow the second part.
+  std::vector<char> late_release;
   // Early signals: a task may publish a one-member group part-way through
   // (the counter index goes to its aux[3] as index + 1), so that waiters on
   // its first result do not wait for all of it.
@@ -77,6 +80,7 @@ struct DagBuilder {
     waits.emplace_back();
     mid_waits.emplace_back();
     post_cost.push_back(0.0);
+    late_release.push_back(0);
     group_of.push_back(group);
     early_of.push_back(-1);
     early_at.push_back(0.0);
@@ -103,7 +107,10 @@ struct DagBuilder {
   void wait_mid(int task, int dep) {
     if (dep >= 0) mid_waits[task].push_back(dep);
   }
-  void split_task(int task, double post_us) { post_cost[task] = post_us; }
+  void split_task(int task, double post_us, bool own_at_end = false) {
+    post_cost[task] = post_us;
+    late_release[task] = own_at_end ? 1 : 0;
+  }
   // Wait for all members of a group (the group must be complete when the
   // program is finished).
   void wait_group(int task, int group) {
@@ -256,6 +263,7 @@ struct DagBuilder {
         return (t.aux[2] ? 11.0 : 27.0) * (0.25 + 0.1875 * nb);
       }
       case T_SUM: return 3.0 + 0.5 * t.aux[0];
+      case T_TRSV: return 1.0;  // the operand copies issued before its mid waits
       case T_COPY: return 3.5;
       default: return 6.0;
     }
@@ -293,8 +301,9 @@ struct DagBuilder {
             for (int u : members[wt.id])
               if (u < t) rank[u] = std::max(rank[u], rank[t]);
           } else if (wt.id < t) {
-            // a split task's own waiters follow its first part only
-            rank[wt.id] = std::max(rank[wt.id], rank[t] - post_cost[wt.id]);
+            // a split task's own waiters follow its first part only (its
+            // end, for a task that raises its counter at the end)
+            rank[wt.id] = std::max(rank[wt.id], rank[t] - (late_release[wt.id] ? 0.0 : post_cost[wt.id]));
           }
         }
       }
@@ -363,7 +372,8 @@ struct DagBuilder {
           if (e.second < -ng) {  // first part of a split task done: its own waiters go
             const int t = -1 - ng - e.second;
             first_done[t] = 1;
-            for (int w : task_waiters[t]) release(w);
+            if (!late_release[t])
+              for (int w : task_waiters[t]) release(w);
             if (mid_unmet[t] == 0) second_part(t);
             continue;
           }
@@ -374,7 +384,7 @@ struct DagBuilder {
           free_slots++;
           done++;
           const int t = e.second;
-          if (post_cost[t] <= 0.0)
+          if (post_cost[t] <= 0.0 || late_release[t])
             for (int w : task_waiters[t]) release(w);
           for (int w : mid_waiters[t])
             if (--mid_unmet[w] == 0 && first_done[w]) second_part(w);
@@ -514,6 +524,9 @@ struct DagBuilder {
     prog.succ_off.assign(nc + 1, 0);
     prog.ctarget.assign(nc, 1);
     for (size_t g = 0; g < group_size.size(); g++) prog.ctarget[nt + g] = std::max(group_size[g], 1);
+    // (a T_TRSV task is released on all its waits: under the dynamic
+    // schedule it never spins on its mid waits, so ready steps cannot hold
+    // every CTA while their predecessors wait for one)
     auto npre = [](const Task& tk) { return (tk.op == T_POTRF && tk.k > 0) ? (int)tk.cdiag : (int)tk.nwait; };
     for (int i = 0; i < nt; i++) {
       const Task& tk = prog.tasks[i];

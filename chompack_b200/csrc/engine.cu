@@ -1007,6 +1007,108 @@ __device__ void run_sum(const RunArgs& ra, const Task& t) {
 // C = alpha * M2 * (opA * opB^T), M2 = lower-triangular m x m tile (operand
 // `c` of the task holds C; M2 is described by aux: base aux[0], ld aux[1],
 // offset (aux[2] | aux[3] << 32)).
+// One step of a block substitution (the triangular solves):
+// C (m x n) = alpha A (m x K) B (K x n) + beta C, m <= 64, K <= TRSV_KMAX,
+// with A a step operand computed before the sweep's chain ([-G_c | M_c] or
+// [M_c; -H_c] stored transposed) and B adjacent x tiles, C one of them.
+// A's copies into shared memory (sA[k*TRSV_LA + r], zero outside m x K) are
+// issued before the task's mid waits [cdiag, nwait) (the x tiles it reads,
+// written by the chain), so that they overlap the wait; then B is read in
+// groups of 8 right-hand sides (sB[k*8 + j]) and each warp multiplies its
+// 16 rows with FP64 MMAs.  A wait that runs out sets the timeout status
+// and returns once the copies have landed.
+__device__ void run_trsv(const RunArgs& ra, const Task& t, double* smem) {
+  __shared__ int s_trsv_abort;
+  constexpr int LA = TRSV_LA;
+  double* sA = smem;
+  double* sB = smem + TRSV_KMAX * LA;
+  const int m = t.m, n = t.n, K = t.k, K4 = (K + 3) & ~3;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+  {
+    const double* __restrict__ X = ra.bases[t.a.base] + t.a.off;
+    const int ld = t.a.ld;
+    if (t.a.mode == OM_T) {
+      // A(r, k) = X[r*ld + k]: consecutive threads take consecutive k
+      for (int idx = tid; idx < TILE * K4; idx += NTHREADS) {
+        const int k = idx % K4, r = idx / K4;
+        const bool ok = r < m && k < K;
+        cp_async8_zfill(sA + k * LA + r, ok ? X + (int64_t)r * ld + k : X, ok);
+      }
+    } else {
+      for (int idx = tid; idx < TILE * K4; idx += NTHREADS) {
+        const int r = idx % TILE, k = idx / TILE;
+        const bool ok = r < m && k < K;
+        cp_async8_zfill(sA + k * LA + r, ok ? X + (int64_t)k * ld + r : X, ok);
+      }
+    }
+    cp_async_commit();
+  }
+  if (tid == 0) {
+    int abort = 0;
+    for (int w = t.cdiag; w < t.nwait && !abort; w++) {
+      const int2 wt = ra.waits[t.wait_off + w];
+      int64_t spins = 0;
+      unsigned ns = 16;
+      while (ld_acquire(ra.counters + wt.x) < wt.y) {
+        if (++spins > ra.spin_limit) {
+          atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+          atomicAdd(&ra.ctl[3], 1);
+          abort = 1;
+          break;
+        }
+        if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
+        __nanosleep(ns);
+        if (ns < 128) ns <<= 1;
+      }
+    }
+    s_trsv_abort = abort;
+  }
+  __syncthreads();
+  if (s_trsv_abort) {
+    cp_async_wait_all();
+    return;
+  }
+  const double* __restrict__ Xb = ra.bases[t.b.base] + t.b.off;
+  const int ldb = t.b.ld;  // B(j, k) = Xb[j*ldb + k] (x tiles, operand mode OM_T)
+  double* __restrict__ C = ra.bases[t.c.base] + t.c.off;
+  const int ldc = t.c.ld;
+  for (int j0 = 0; j0 < n; j0 += 8) {
+    const int nb = min(8, n - j0);
+    for (int base = 0; base < K4 * 8; base += 4 * NTHREADS) {
+      double v[4];
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int idx = base + tid + e * NTHREADS, k = idx % K4, j = idx / K4;
+        v[e] = (idx < K4 * 8 && k < K && j < nb) ? __ldcg(Xb + (int64_t)(j0 + j) * ldb + k) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int idx = base + tid + e * NTHREADS, k = idx % K4, j = idx / K4;
+        if (idx < K4 * 8) sB[k * 8 + j] = v[e];
+      }
+    }
+    if (j0 == 0) cp_async_wait_all();
+    __syncthreads();
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (16 * warp < m) {
+      const double* ar = sA + 16 * warp + g;
+#pragma unroll 4
+      for (int k = 0; k < K4; k += 4) dmma16(acc, ar[(k + q) * LA], ar[(k + q) * LA + 8], sB[(k + q) * 8 + g]);
+    }
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int r = 16 * warp + g + ((h & 2) ? 8 : 0), j = 2 * q + (h & 1);
+      if (r < m && j < nb) {
+        double* cp = C + (int64_t)(j0 + j) * ldc + r;
+        double val = t.alpha * acc[h];
+        if (t.beta != 0.0) val += t.beta * __ldcg(cp);
+        *cp = val;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 __device__ void run_mrow(const RunArgs& ra, const Task& t, const SmemLayout& sm) {
   const Opnd A = make_opnd(ra, t.a), B = make_opnd(ra, t.b);
   double* C = ra.bases[t.c.base] + t.c.off;
@@ -1666,27 +1768,46 @@ __device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
     }
     __syncthreads();
   }
+  // Pivots with one barrier each: pivot j updates the trailing part with
+  // its unscaled column, F(i, c) -= F(i, j) F(c, j) / d_j, and the column
+  // itself is scaled by 1 / L(j, j) in the next pivot's phase (nobody reads
+  // it then); 1 / L(j, j) = rsqrt(d_j), kept for the solve below.
+  // The diagonal entries L(j, j) = d_j / sqrt(d_j) are written after the
+  // loop (every thread reads d_j in pivot j's phase).
+  double* rl = F + TILE * FLD;  // 1 / L(j, j)
+  double* lj = rl + TILE;       // L(j, j)
   int first_bad = -1;
   for (int j = 0; j < nn; j++) {
     const double d = F[j * FLD + j];
     const bool bad = !(d > 0.0);
     if (bad && first_bad < 0) first_bad = j;
-    const double lj = sqrt(bad ? 1.0 : d), rl = 1.0 / lj;
-    for (int i = j + 1 + tid; i < nj; i += NTHREADS) F[j * FLD + i] *= rl;
-    __syncthreads();
-    if (tid == 0) F[j * FLD + j] = lj;  // nobody reads it in the update below
+    const double rs = rsqrt(bad ? 1.0 : d), rd = rs * rs;
+    if (j > 0) {
+      const double rp = rl[j - 1];
+      for (int i = j + tid; i < nj; i += NTHREADS) F[(j - 1) * FLD + i] *= rp;
+    }
+    if (tid == 0) {
+      rl[j] = rs;  // read from the next phase on
+      lj[j] = (bad ? 1.0 : d) * rs;
+    }
     for (int c = j + 1 + warp; c < nj; c += NW) {
-      const double fc = F[j * FLD + c];
+      const double fc = F[j * FLD + c] * rd;
       for (int i = c + lane; i < nj; i += 32) F[c * FLD + i] -= F[j * FLD + i] * fc;
     }
     __syncthreads();
   }
+  if (nn > 0)
+    for (int i = nn + tid; i < nj; i += NTHREADS) F[(nn - 1) * FLD + i] *= rl[nn - 1];
+  for (int j = tid; j < nn; j += NTHREADS) F[j * FLD + j] = lj[j];
   if (tid == 0 && first_bad >= 0) atomicCAS(&ra.ctl[2], 0, first_bad + 1);
+  __syncthreads();
+  // W = L21 L11^{-1}, one row per thread, right-looking: w_j = t_j / L(j, j),
+  // then t_j' -= w_j L(j, j') for j' < j (independent updates)
   for (int i = nn + tid; i < nj; i += NTHREADS)
     for (int j = nn - 1; j >= 0; j--) {
-      double v = F[j * FLD + i];
-      for (int l2 = j + 1; l2 < nn; l2++) v -= F[l2 * FLD + i] * F[j * FLD + l2];
-      F[j * FLD + i] = v / F[j * FLD + j];
+      const double v = F[j * FLD + i] * rl[j];
+      F[j * FLD + i] = v;
+      for (int l2 = 0; l2 < j; l2++) F[l2 * FLD + i] -= v * F[l2 * FLD + j];
     }
   __syncthreads();
   for (int c = warp; c < nn; c += NW)
@@ -2589,7 +2710,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       if (threadIdx.x == 0) {
         if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
         int abort = 0;
-        const int npre = (s_t.op == T_POTRF && s_t.k > 0) ? (int)s_t.cdiag : (int)s_t.nwait;
+        const int npre = ((s_t.op == T_POTRF && s_t.k > 0) || s_t.op == T_TRSV) ? (int)s_t.cdiag : (int)s_t.nwait;
         for (int w = 0; w < npre && !abort; w++) {
           const int2 wt = ra.waits[s_t.wait_off + w];
           int64_t spins = 0;
@@ -2628,6 +2749,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
       case T_EXTRACT: run_extract(ra, t, smem); break;
       case T_COPY: run_copy(ra, t); break;
       case T_VEC: run_vec(ra, t, smem); break;
+      case T_TRSV: run_trsv(ra, t, smem); break;
       case T_QL: run_ql(ra, t, smem); break;
       case T_NOP: break;
       case T_SUM: run_sum(ra, t); break;

@@ -37,6 +37,10 @@ constexpr int MAX_BASES = 64;     // base-pointer slots (see Base below)
 // carve-out, which leaves more L1 for the register spills.
 constexpr int ENGINE_SMEM_BASE_DOUBLES = 9472;
 constexpr int ENGINE_SMEM_DOUBLES = 14336;
+// T_TRSV: the largest K, and the leading dimension of its staged operand
+constexpr int TRSV_KMAX = 128;
+constexpr int TRSV_LA = TILE + 2;
+static_assert(TRSV_KMAX * TRSV_LA + TRSV_KMAX * 8 <= ENGINE_SMEM_BASE_DOUBLES, "T_TRSV staging exceeds shared memory");
 // Shared-memory doubles a Householder panel of h rows and nb columns needs
 // (panel, then its nb x nb T factor, plus scalars).
 CHB_HD constexpr int ql_panel_doubles(int h, int nb) { return h * nb + nb * nb + 192; }
@@ -86,7 +90,9 @@ enum TaskOp : uint8_t {
   T_FRONT = 15,   // a whole small cholesky front (nj <= TILE) in shared memory (front aux[0])
   T_PFRONT = 16,  // a whole small projected-inverse front (nj <= TILE) in shared memory (front aux[0])
   T_SUBTREE = 17, // cholesky of up to four ranges of small complete subtrees, one per warp (see bundle_last)
-  T_PSUBTREE = 18 // projected_inverse of such ranges, one per warp, parents first
+  T_PSUBTREE = 18, // projected_inverse of such ranges, one per warp, parents first
+  T_TRSV = 19     // a block-substitution step C = alpha opA opB^T (+ beta C), m <= 64, K <= TRSV_KMAX:
+                  // opA (independent of the chain) staged before the mid waits [cdiag, nwait)
 };
 
 // Sub-operations of T_QL (child aux[0], columns [aux[1], aux[2]) of the

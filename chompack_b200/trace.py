@@ -36,7 +36,7 @@ TASK = np.dtype({
 })
 
 OP_NAMES = ["GEMM", "POTRF", "ASM", "MROW", "EXTRACT", "COPY", "INV", "RPOTRF", "QL", "VEC", "NOP", "LA",
-            "SUM", "SIGNAL", "ARRIVAL", "FRONT", "PFRONT", "SUBTREE", "PSUBTREE"]
+            "SUM", "SIGNAL", "ARRIVAL", "FRONT", "PFRONT", "SUBTREE", "PSUBTREE", "TRSV"]
 T_POTRF, T_LA = 1, 11
 
 N.lib.chb_program_info.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,

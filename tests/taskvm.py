@@ -24,7 +24,7 @@ FRONT = np.dtype([("nn", "<i4"), ("na", "<i4"), ("nj", "<i4"), ("relptr", "<i4")
 OM_N, OM_T, OM_TRI_N, OM_TRI_T, OM_SYM = range(5)
 T_GEMM, T_POTRF, T_ASM, T_MROW, T_EXTRACT, T_COPY = 0, 1, 2, 3, 4, 5
 T_QL, T_VEC, T_NOP, T_LA, T_SUM, T_SIGNAL, T_ARRIVAL, T_FRONT, T_PFRONT = 8, 9, 10, 11, 12, 13, 14, 15, 16
-T_SUBTREE, T_PSUBTREE = 17, 18
+T_SUBTREE, T_PSUBTREE, T_TRSV = 17, 18, 19
 QL_GATHER, QL_PANEL = 0, 1
 B_X, B_WS, B_RHS = 0, 1, 4
 
@@ -126,7 +126,7 @@ class VM(object):
 
     def run_task(self, t):
         op = int(t["op"])
-        if op == T_GEMM:
+        if op == T_GEMM or op == T_TRSV:  # a substitution step is a GEMM (its cdiag counts its first waits)
             m, n, K = int(t["m"]), int(t["n"]), int(t["k"])
             A = _operand(self.bases[int(t["a"]["base"])], t["a"], m, K)
             Bm = _operand(self.bases[int(t["b"]["base"])], t["b"], n, K)

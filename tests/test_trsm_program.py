@@ -4,8 +4,8 @@ random and dynamic orders and compared with the reference's trsm
 (src/C/trsm.c, oracle/_ref) on the same factor:
 
 * diagonal blocks of several 64-row tiles, so that the substitution steps
-  carry the neighbouring block's update ([-G_c | M_c] for 'N', [M_c; -H_c]
-  for 'T');
+  (T_TRSV tasks, their operand staged before their mid waits) carry the
+  neighbouring block's update ([-G_c | M_c] for 'N', [M_c; -H_c] for 'T');
 * long products W x_k (K = nn) and W^T u_k (K = na) beyond 128, split
   into partial tiles and one T_SUM;
 * extend-add and extract tasks split by right-hand-side columns.
@@ -49,8 +49,13 @@ def test_program_has_every_form(grid16):
         prog = _tasks(s, 8, trans)
         t = prog.tasks
         assert int(np.sum(t["op"] == taskvm.T_SUM)) > 0, trans
-        gemm = t[t["op"] == taskvm.T_GEMM]
-        assert int(np.sum(gemm["k"] > 64)) > 0, trans          # fused substitution steps
+        steps = t[t["op"] == taskvm.T_TRSV]
+        assert int(np.sum(steps["k"] > 64)) > 0, trans         # steps that take the neighbouring update
+        # a step starts on its operand's producers and is split: the x tiles
+        # it reads (after the first step of a chain) are mid waits, after the
+        # first cdiag waits
+        assert np.all(steps["cdiag"] <= steps["nwait"]), trans
+        assert int(np.sum(steps["cdiag"] < steps["nwait"])) > 0, trans
         vec = t[(t["op"] == taskvm.T_VEC) & (t["aux"][:, 0] >= 2)]
         assert int(np.sum(vec["aux"][:, 3] - vec["aux"][:, 2] < 8)) > 0, trans   # column-split tasks
 
