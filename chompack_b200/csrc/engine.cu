@@ -875,6 +875,20 @@ __device__ __forceinline__ void gemm_acc(const Opnd& A, const Opnd& B, int m, in
 // C = alpha*acc + beta*C (masked to m x n and, for lower, to r + cdiag >= c).
 // All old values are fetched before the first store so that the loads are
 // in flight together (the compiler cannot reorder them across stores to C).
+// C += alpha acc with atomic adds (CM_ATOMIC).
+__device__ void store_acc_atomic(double* __restrict__ C, int ldc, int m, int n, double alpha, const Acc& acc) {
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 4; h++) {
+        int r, c;
+        acc_coord(i, j, h, r, c);
+        if (r < m && c < n) atomicAdd(C + (int64_t)c * ldc + r, alpha * acc[i][j][h]);
+      }
+}
+
 __device__ void store_acc(double* __restrict__ C, int ldc, int m, int n, bool lower, int cdiag, double alpha,
                           double beta, const Acc& acc) {
   double old[2][4][4];
@@ -938,7 +952,8 @@ __device__ void run_gemm_or_la(const RunArgs& ra, const Task& t, const SmemLayou
     if (la || t.c.prec == PREC_FP64) gemm_acc_p<PREC_FP64>(A, B, m, n, K, sm, acc);
     else if (t.c.prec == PREC_TF32) gemm_acc_p<PREC_TF32>(A, B, m, n, K, sm, acc);
     else gemm_acc_p<PREC_TF32X3>(A, B, m, n, K, sm, acc);
-    store_acc(ra.bases[oc.base] + oc.off, oc.ld, m, n, lower, cdiag, alpha, beta, acc);
+    if (!la && t.cmode == CM_ATOMIC) store_acc_atomic(ra.bases[oc.base] + oc.off, oc.ld, m, n, alpha, acc);
+    else store_acc(ra.bases[oc.base] + oc.off, oc.ld, m, n, lower, cdiag, alpha, beta, acc);
     if (la && ph == 0) {
       __syncthreads();
       if (t.aux[3] > 0) {
@@ -2411,36 +2426,58 @@ __device__ void run_vec(const RunArgs& ra, const Task& t, double* smem) {
     }
     return;
   }
-  // VEC_EXTRACT for child aux1 of the front p described by operands a, c
+  if (mode == VEC_ZERO) {
+    double* __restrict__ z = ra.bases[t.c.base] + t.c.off;
+    const int64_t cnt = (int64_t)t.m * t.n;
+    for (int64_t i = threadIdx.x; i < cnt; i += NTHREADS) z[i] = 0.0;
+    return;
+  }
+  // VEC_EXTRACT / VEC_ADD for child aux1 of the front p described by
+  // operands a (x_p) and c (u_p): rows [i0, i1) of u_c, columns [j0, j1)
   const FrontDesc ch = ra.fronts[t.aux[1]];
   const FrontDesc f = ra.fronts[ch.parent];
-  const double* __restrict__ xp = ra.bases[t.a.base] + t.a.off;
+  double* __restrict__ xp = ra.bases[t.a.base] + t.a.off;
   const int ldx = t.a.ld;
-  const double* __restrict__ up = ra.bases[t.c.base] + t.c.off;
-  const int Nc = ch.na, tot = Nc * nc;
+  double* __restrict__ up = ra.bases[t.c.base] + t.c.off;
+  const int Nc = ch.na;
+  const int i0 = t.m, i1 = t.k > 0 ? t.k : Nc, ni = max(i1 - i0, 0), tot = ni * nc;
   const int32_t* __restrict__ r = ra.relidx + ch.relptr;
-  double* __restrict__ uc = WS + vbase + ch.vpos * nrhs + (int64_t)j0 * Nc;
+  double* __restrict__ uc = WS + vbase + ch.vpos * nrhs;
   for (int base = 0; base < tot; base += E * NTHREADS) {
-    int row[E];
+    int row[E], ui[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int idx = base + threadIdx.x + e * NTHREADS;
-      row[e] = (idx < tot) ? __ldg(r + idx % max(Nc, 1)) : -1;
+      const int i = i0 + idx % max(ni, 1), j = j0 + idx / max(ni, 1);
+      row[e] = (idx < tot) ? __ldg(r + i) : -1;
+      ui[e] = i + j * Nc;
+    }
+    if (mode == VEC_ADD) {
+      // rows of one child are distinct, but other children add into the
+      // same rows at the same time: atomic adds
+      double v[E];
+#pragma unroll
+      for (int e = 0; e < E; e++) v[e] = row[e] >= 0 ? __ldcg(uc + ui[e]) : 0.0;
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        if (row[e] < 0) continue;
+        const int j = j0 + (base + threadIdx.x + e * NTHREADS) / max(ni, 1);
+        double* dst = row[e] < f.nn ? xp + row[e] + (int64_t)j * ldx : up + (row[e] - f.nn) + (int64_t)j * f.na;
+        atomicAdd(dst, v[e]);
+      }
+      continue;
     }
     double v[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int idx = base + threadIdx.x + e * NTHREADS;
-      const int j = j0 + idx / max(Nc, 1);
+      const int j = j0 + (base + threadIdx.x + e * NTHREADS) / max(ni, 1);
       v[e] = row[e] < 0 ? 0.0
                         : (row[e] < f.nn ? __ldcg(xp + row[e] + (int64_t)j * ldx)
                                          : __ldcg(up + (row[e] - f.nn) + (int64_t)j * f.na));
     }
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const int idx = base + threadIdx.x + e * NTHREADS;
-      if (row[e] >= 0) uc[idx] = v[e];
-    }
+    for (int e = 0; e < E; e++)
+      if (row[e] >= 0) uc[ui[e]] = v[e];
   }
 }
 

@@ -37,10 +37,11 @@ constexpr int MAX_BASES = 64;     // base-pointer slots (see Base below)
 // carve-out, which leaves more L1 for the register spills.
 constexpr int ENGINE_SMEM_BASE_DOUBLES = 9472;
 constexpr int ENGINE_SMEM_DOUBLES = 14336;
-// T_TRSV: the largest K, and the leading dimension of its staged operand
-constexpr int TRSV_KMAX = 128;
+// T_TRSV: the largest K, and the leading dimension of its staged operand;
+// programs with such steps launch with ENGINE_SMEM_DOUBLES
+constexpr int TRSV_KMAX = 192;
 constexpr int TRSV_LA = TILE + 2;
-static_assert(TRSV_KMAX * TRSV_LA + TRSV_KMAX * 8 <= ENGINE_SMEM_BASE_DOUBLES, "T_TRSV staging exceeds shared memory");
+static_assert(TRSV_KMAX * TRSV_LA + TRSV_KMAX * 8 <= ENGINE_SMEM_DOUBLES, "T_TRSV staging exceeds shared memory");
 // Shared-memory doubles a Householder panel of h rows and nb columns needs
 // (panel, then its nb x nb T factor, plus scalars).
 CHB_HD constexpr int ql_panel_doubles(int h, int nb) { return h * nb + nb * nb + 192; }
@@ -68,7 +69,9 @@ enum OpMode : uint8_t {
 
 enum CMode : uint8_t {
   CM_FULL = 0,   // write the whole m x n tile
-  CM_LOWER = 1   // write only entries with r + cdiag >= c (lower triangle)
+  CM_LOWER = 1,  // write only entries with r + cdiag >= c (lower triangle)
+  CM_ATOMIC = 2  // C += alpha op(A) op(B)^T with atomic adds (beta is 1): tiles that several
+                 // tasks update at once, in any order
 };
 
 enum TaskOp : uint8_t {
@@ -193,8 +196,12 @@ enum VecOp : int {
   VEC_GATHER = 0,   // Bp[i, :] = alpha * B[p[i], :] for i in [aux1, aux2)
   VEC_SCATTER = 1,  // B[p[i], :] = Bp[i, :]
   VEC_ASM = 2,      // front aux1: zero u_k, add the children's updates into x_k / u_k
-  VEC_EXTRACT = 3   // child aux1: u_c = [x_p; u_p](r_c)
+  VEC_EXTRACT = 3,  // child aux1: u_c = [x_p; u_p](r_c), rows [m, k) of u_c (k == 0: all)
+  VEC_ADD = 4,      // child aux1: [x_p; u_p](r_c) += u_c with atomic adds, rows [m, k) of u_c
+  VEC_ZERO = 5      // operand c: m * n doubles set to zero
 };
+// VEC_ASM, VEC_EXTRACT and VEC_ADD take the right-hand-side columns
+// [aux2, aux3) (aux3 == 0: all n).
 
 // Error codes written to ctl[1].
 enum DeviceError : int {

@@ -152,7 +152,7 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
       if (t.op == T_GEMM) t.c.prec = prec;
   prog->tf32_tiles = prec == PREC_TF32;
   for (const Task& t : prog->tasks)
-    if (t.op == T_QL) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels
+    if (t.op == T_QL || t.op == T_TRSV) prog->smem_doubles = ENGINE_SMEM_DOUBLES;  // Householder panels, step operands
   // Default schedule per sweep, by measurement on a 3-D grid of 64,000
   // unknowns: the chains of small dependent tasks of cholesky, llt and trsm
   // run faster in static list order (a CTA already waits on the next task;

@@ -414,17 +414,28 @@ class VM(object):
                     xb[xo + r[top] + j * ldx] += uc[top, j]
                     ub[uo + (r[~top] - nn) + j * na] += uc[~top, j]
             return
+        if mode == 5:  # VEC_ZERO: m * n doubles of operand c
+            ub[uo: uo + int(t["m"]) * nrhs] = 0.0
+            return
         ch = self.p.fronts[int(t["aux"][1])]
         f = self.p.fronts[int(ch["parent"])]
         nn, na, Nc = int(f["nn"]), int(f["na"]), int(ch["na"])
-        r = self.relidx[int(ch["relptr"]): int(ch["relptr"]) + Nc]
+        i0 = int(t["m"])
+        i1 = int(t["k"]) if int(t["k"]) > 0 else Nc
+        r = self.relidx[int(ch["relptr"]) + i0: int(ch["relptr"]) + i1]
         base = vbase + int(ch["vpos"]) * nrhs
+        top = r < nn
         for j in range(j0, j1):
-            top = r < nn
-            vals = np.empty(Nc)
+            seg = slice(base + j * Nc + i0, base + j * Nc + i1)
+            if mode == 4:  # VEC_ADD: [x_p; u_p](r_c) += u_c (rows i0..i1)
+                v = WS[seg].copy()
+                np.add.at(xb, xo + r[top] + j * ldx, v[top])
+                np.add.at(ub, uo + (r[~top] - nn) + j * na, v[~top])
+                continue
+            vals = np.empty(i1 - i0)
             vals[top] = xb[xo + r[top] + j * ldx]
             vals[~top] = ub[uo + (r[~top] - nn) + j * na]
-            WS[base + j * Nc: base + (j + 1) * Nc] = vals
+            WS[seg] = vals
 
     def _ql(self, t):
         """Blocked Householder QL of update_factor (engine.cu run_ql) with

@@ -5,10 +5,13 @@ random and dynamic orders and compared with the reference's trsm
 
 * diagonal blocks of several 64-row tiles, so that the substitution steps
   (T_TRSV tasks, their operand staged before their mid waits) carry the
-  neighbouring block's update ([-G_c | M_c] for 'N', [M_c; -H_c] for 'T');
-* long products W x_k (K = nn) and W^T u_k (K = na) beyond 128, split
-  into partial tiles and one T_SUM;
-* extend-add and extract tasks split by right-hand-side columns.
+  updates of the two neighbouring blocks ([-G2_c | -G_c | M_c] for 'N',
+  [M_c; -H_c; -H2_c] for 'T');
+* long products W x_k (K = nn) and W^T u_k (K = na) beyond 128, in chunks
+  whose products add into the target with atomics, like the far updates of
+  the substitution;
+* extend-add (atomic adds) and extract tasks split by right-hand-side
+  columns and row chunks.
 
 Tolerance: 1e-12 relative to the largest entry of the column (the GPU
 tests use the same measure)."""
@@ -48,9 +51,12 @@ def test_program_has_every_form(grid16):
     for trans in ("N", "T"):
         prog = _tasks(s, 8, trans)
         t = prog.tasks
-        assert int(np.sum(t["op"] == taskvm.T_SUM)) > 0, trans
+        gemm = t[t["op"] == taskvm.T_GEMM]
+        assert int(np.sum(gemm["cmode"] == 2)) > 0, trans       # products that add with atomics
+        if trans == "N":
+            assert int(np.sum((t["op"] == taskvm.T_VEC) & (t["aux"][:, 0] == 4))) > 0   # atomic extend-add
         steps = t[t["op"] == taskvm.T_TRSV]
-        assert int(np.sum(steps["k"] > 64)) > 0, trans         # steps that take the neighbouring update
+        assert int(np.sum(steps["k"] > 128)) > 0, trans        # steps that take two neighbouring updates
         # a step starts on its operand's producers and is split: the x tiles
         # it reads (after the first step of a chain) are mid waits, after the
         # first cdiag waits
