@@ -776,6 +776,15 @@ def main():
         fb = 8.0 * int(s.blkptr[-1]) + 16.0 * s.n * nrhs     # factor read once, B read and written
         other["trsm_%s_nrhs%d" % (tr, nrhs)] = {"ms": round(ms, 4), "gflops": round(fl["trsm_rhs"] * nrhs / ms / 1e6, 3),
                                                 "achieved_gbs": round(fb / ms / 1e6, 1)}
+        # the bit-reproducible form (additions into vector blocks in a fixed order)
+        plan.set_option("ordered_sums", 1)
+        try:
+            wt, nbt = plan.workspace(N.OP_TRSM, nrhs, 1 if tr == "T" else 0)
+            ms = timed(lambda: N.trsm(plan.handle, tr.encode(), nrhs, 1.0, Lw.data_ptr(), Bt.data_ptr(), s.n, wt,
+                                      nbt, sp), reps)
+        finally:
+            plan.set_option("ordered_sums", None)
+        other["trsm_%s_nrhs%d" % (tr, nrhs)]["ordered_sums_ms"] = round(ms, 4)
     import ctypes
     Ud = Yw * torch.randn(Yw.shape, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(6))
     Uw = torch.empty_like(Ud)

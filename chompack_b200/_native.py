@@ -126,5 +126,5 @@ add_sparse = _sig("chb_add_sparse", ctypes.c_int, [PPLAN, vp, vp, vp, i64, vp, v
 plan_set_option = _sig("chb_plan_set_option", ctypes.c_int, [PPLAN, ctypes.c_int, i64])
 plan_get_option = _sig("chb_plan_get_option", ctypes.c_int, [PPLAN, ctypes.c_int, ctypes.POINTER(i64)])
 OPTIONS = {"small_front_nj": 0, "subtrees": 1, "chol_ksplit": 2, "pinv_ksplit": 3, "fused_la": 4,
-           "tf32_tcgen05": 5}
+           "tf32_tcgen05": 5, "ordered_sums": 6}
 engine_occupancy = _sig("chb_engine_occupancy", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int)])

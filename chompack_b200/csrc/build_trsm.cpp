@@ -87,6 +87,53 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
       ws += (int64_t)rows * cols;
     }
   }
+  const bool ordered = ordered_sums(P);
+  // Ordered mode: a long product split along K into partial tiles (ld 64,
+  // 64 x n apart) and one T_SUM into C; returns the sum task and appends
+  // the parts (parts = {sum} when K <= KC).
+  auto split_gemm = [&](const Task& t, const SchedKey& key, int group, std::vector<int>& parts) -> int {
+    const int p = split_count(t.k, KC);
+    if (p == 1) {
+      const int id = B.add(t, key, group);
+      parts.push_back(id);
+      return id;
+    }
+    const int64_t scr = ws;
+    ws += (int64_t)p * T * t.n;
+    const int chunk = (t.k + p - 1) / p;
+    std::vector<int> mine;
+    for (int q = 0; q < p; q++) {
+      const int k0 = q * chunk, kq = std::min(chunk, t.k - k0);
+      Task u = t;
+      u.k = kq;
+      u.a = shift_k(t.a, k0);
+      u.b = shift_k(t.b, k0);
+      u.alpha = 1.0;
+      u.beta = 0.0;
+      u.cmode = CM_FULL;
+      u.c = opnd(B_WS, scr + (int64_t)q * T * t.n, T);
+      SchedKey kk = key;
+      kk.rank = key.rank * 64 + q;
+      mine.push_back(B.add(u, kk));
+    }
+    Task sm = make_task(T_SUM);
+    sm.m = t.m;
+    sm.n = t.n;
+    sm.alpha = t.alpha;
+    sm.beta = t.beta;
+    sm.cmode = CM_FULL;
+    sm.a = opnd(B_WS, scr, T);
+    sm.c = t.c;
+    sm.aux[0] = p;
+    sm.aux[1] = T * t.n;
+    const int out = B.add(sm, key, group, 2.0 + 0.4 * p);
+    for (int id : mine) {
+      B.wait_task(out, id);
+      parts.push_back(id);
+    }
+    return out;
+  };
+
   // gather Bp = alpha B[p], 256 rows per task
   const int RCH = 256;
   const int gath = B.new_group();
@@ -189,16 +236,27 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
     // tile are independent tile products that add into it with atomics
     // (CM_ATOMIC), each as soon as its block is solved, so that no chain of
     // updates forms behind the steps; a group per tile collects them.
+    // (Ordered mode: the far updates of a tile form a chain, each waiting
+    // for the one before, and the step waits for the last one in the middle.)
     const double STEP_US = 3.0;
     std::vector<int> far(NBc * nrt, -1);
-    std::vector<int> nfar(NBc * nrt, 0);
-    for (int i = 0; i < NBc * nrt; i++) far[i] = B.new_group();
+    std::vector<int> nfar(NBc * nrt, 0), lastu(NBc * nrt, -1);
+    if (!ordered)
+      for (int i = 0; i < NBc * nrt; i++) far[i] = B.new_group();
     auto far_update = [&](const Operand& a, int r, int c, int s, const SchedKey& key, int sol) {
       Task u = gemm(bw(r), rw(s), bw(c), -1.0, a, xop(c, s, OM_T), 1.0, xop(r, s, OM_N));
-      u.cmode = CM_ATOMIC;
+      if (!ordered) u.cmode = CM_ATOMIC;
       const int uid = B.add(u, key, far[r * nrt + s]);
       nfar[r * nrt + s]++;
       B.wait_task(uid, sol);
+      if (ordered) {
+        B.wait_task(uid, lastu[r * nrt + s]);
+        lastu[r * nrt + s] = uid;
+      }
+    };
+    auto wait_far = [&](int sol, int c, int s) {
+      if (ordered) B.wait_mid(sol, lastu[c * nrt + s]);
+      else if (nfar[c * nrt + s] > 0) B.wait_group(sol, far[c * nrt + s]);
     };
     // Column groups and row chunks of the extract / add tasks of child c
     auto child_tasks = [&](int c, int mode, const SchedKey& key0, int group, const std::vector<int>& deps,
@@ -232,9 +290,37 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
       // u_k zeroed; the children's updates added into x_k and u_k with
       // atomics (one task per child, column group and row chunk, all at
       // once); u_k -= W x_k as partial products that add into u_k with
-      // atomics (no sum task), after x_k is complete
+      // atomics (no sum task), after x_k is complete.  Ordered mode: one
+      // extend-add task per column group adds the children in order, and
+      // the products go through partial tiles and a sum.
       int zero = -1;
-      if (na > 0) {
+      const int agrp = B.new_group();
+      int nadd = 0;
+      std::vector<int> readers;  // ordered mode: the products that read x_k
+      if (ordered) {
+        // the children's updates added in order (last child first, as the
+        // reference pops its stack), staged in shared memory per column
+        // group; the task zeroes u_k's columns first
+        int64_t elems = nj;
+        for (int l = f.chbeg; l < f.chend; l++) elems += P.fronts[P.chidx[l]].na;
+        const int cpt = vec_cols_per_task(elems, nrhs, nj);
+        for (int64_t j0 = 0; j0 < nrhs; j0 += cpt) {
+          Task t = make_task(T_VEC);
+          t.aux[0] = VEC_ASM;
+          t.aux[1] = (int32_t)k;
+          t.aux[2] = (int32_t)j0;
+          t.aux[3] = (int32_t)std::min<int64_t>(nrhs, j0 + cpt);
+          t.n = (int)nrhs;
+          t.a = opnd(B_WS, xk, (int)n);
+          t.b = opnd(B_WS, uoff[0], 0);
+          t.c = opnd(B_WS, uk, std::max(na, 1));
+          const int id = B.add(t, {lv, 0, 0, (int)k, (int)j0, 0}, agrp,
+                               1.5 + (double)elems * (t.aux[3] - t.aux[2]) / 1500.0);
+          B.wait_group(id, gath);
+          for (int l = f.chbeg; l < f.chend; l++) B.wait_group(id, ugrp[P.chidx[l]]);
+          nadd++;
+        }
+      } else if (na > 0) {
         Task t = make_task(T_VEC);
         t.aux[0] = VEC_ZERO;
         t.m = na;
@@ -242,9 +328,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
         t.c = opnd(B_WS, uk, na);
         zero = B.add(t, {-3, 1, 0, (int)k, 0, 0}, -1, 1.0 + (double)na * nrhs / 20000.0);
       }
-      const int agrp = B.new_group();
-      int nadd = 0;
-      for (int l = f.chbeg; l < f.chend; l++) {
+      for (int l = f.chbeg; l < f.chend && !ordered; l++) {
         const int c = P.chidx[l];
         std::vector<int> deps;
         if (zero >= 0) deps.push_back(zero);
@@ -259,7 +343,18 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
       // u_k -= W x_k (reads x_k before it is solved), K = nn in chunks of
       // KC, each chunk's product added into u_k
       int nread = 0;
-      for (int i = 0; i < NBb; i++)
+      for (int i = 0; i < NBb && ordered; i++)
+        for (int s = 0; s < nrt; s++) {
+          Operand a = opnd(B_X, blk + nn + i * T, nj);
+          Operand c = opnd(B_WS, uk + i * T + (int64_t)s * T * na, na);
+          std::vector<int> parts;
+          const int out = split_gemm(gemm(bh(i), rw(s), nn, -1.0, a, xop(0, s, OM_T), 1.0, c),
+                                     {lv, 1, 0, (int)k, s, i}, ugrp[k], parts);
+          for (int id : parts) wait_x(id);
+          wait_x(out);
+          readers.insert(readers.end(), parts.begin(), parts.end());
+        }
+      for (int i = 0; i < NBb && !ordered; i++)
         for (int s = 0; s < nrt; s++)
           for (int k0 = 0; k0 < nn; k0 += KC) {
             const int kq = std::min(KC, nn - k0);
@@ -284,8 +379,10 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
           B.wait_task(sol, coup[k][c][1]);
           wait_x(sol);
           if (c == 0 && nread > 0) B.wait_group(sol, ugrp[k]);  // the products that read x_k first
+          if (c == 0)
+            for (int id : readers) B.wait_task(sol, id);
           B.wait_task(sol, prev2[s]);
-          if (nfar[c * nrt + s] > 0) B.wait_group(sol, far[c * nrt + s]);
+          wait_far(sol, c, s);
           B.wait_mid(sol, prev[s]);
           B.split_task(sol, STEP_US, true);
           prev2[s] = prev[s];
@@ -307,7 +404,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
           B.wait_task(sol, coup[k][c][1]);
           B.wait_group(sol, gath);
           B.wait_task(sol, prev2[s]);
-          if (nfar[c * nrt + s] > 0) B.wait_group(sol, far[c * nrt + s]);
+          wait_far(sol, c, s);
           B.wait_mid(sol, prev[s]);
           B.split_task(sol, STEP_US, true);
           prev2[s] = prev[s];
@@ -321,7 +418,22 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
       // (every read and write of its x tiles by the chain precedes it)
       int xdone = -1;
       std::vector<int> chain_end;
-      if (na > 0) {
+      if (na > 0 && ordered) {
+        // x_k -= W^T u_k split along K = na into partial tiles and a sum
+        // per x tile, the last writer of the tile
+        for (int c = 0; c < NBc; c++)
+          for (int s = 0; s < nrt; s++) {
+            Operand a = opnd(B_X, blk + (int64_t)(c * T) * nj + nn, nj, OM_T);
+            Operand b = opnd(B_WS, uk + (int64_t)s * T * na, na, OM_T);
+            std::vector<int> parts;
+            const int out = split_gemm(gemm(bw(c), rw(s), na, -1.0, a, b, 1.0, xop(c, s, OM_N)),
+                                       {lv, 2 * NBc + 2, 0, (int)k, s, c}, xfinal, parts);
+            for (int id : parts) B.wait_group(id, from_parent);
+            B.wait_task(out, prev[s]);
+            B.wait_group(out, from_parent);
+            chain_end.push_back(out);
+          }
+      } else if (na > 0) {
         // x_k -= W^T u_k, K = na in chunks of KC, each chunk's product added
         // into the x tile after the chain; then one no-op marks x_k final
         xdone = B.new_group();

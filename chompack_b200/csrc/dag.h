@@ -602,6 +602,16 @@ inline bool tf32_tcgen05(const chb_plan& P) {
   return std::getenv("CHB_TF32_TCGEN05") != nullptr;
 }
 
+// The triangular solve's additions into vector blocks in a fixed order
+// (CHB_OPT_ORDERED_SUMS = 1, or CHB_ORDERED_SUMS in the environment: chains
+// of read-modify-write tasks and split-K sums, bit-reproducible) or as
+// independent tasks with atomic adds (0, the default: the order of the
+// additions, and so the last bits, vary from run to run).
+inline bool ordered_sums(const chb_plan& P) {
+  if (P.opt[CHB_OPT_ORDERED_SUMS] >= 0) return P.opt[CHB_OPT_ORDERED_SUMS] != 0;
+  return std::getenv("CHB_ORDERED_SUMS") != nullptr;
+}
+
 // cholesky's fused diagonal task (CHB_OPT_FUSED_LA = 1, the default where it
 // is safe) or separate look-ahead tasks (0; also CHB_NO_FUSED_LA).
 inline bool fused_la_allowed(const chb_plan& P) {

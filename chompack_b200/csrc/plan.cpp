@@ -660,6 +660,7 @@ extern "C" int chb_plan_get_option(const chb_plan* plan, int option, int64_t* va
     case CHB_OPT_PINV_KSPLIT: *value = pinv_ksplit(*plan); break;
     case CHB_OPT_FUSED_LA: *value = fused_la_allowed(*plan) ? 1 : 0; break;
     case CHB_OPT_TF32_TCGEN05: *value = tf32_tcgen05(*plan) ? 1 : 0; break;
+    case CHB_OPT_ORDERED_SUMS: *value = ordered_sums(*plan) ? 1 : 0; break;
     default: return set_error(-2, "unknown option %d", option);
   }
   return 0;

@@ -106,7 +106,7 @@ struct chb_plan {
   int grid_tc = 0;              // persistent grid size of the tcgen05 instantiation
   int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
   int64_t spin_limit = -1;      // polls before a wait gives up; -1: the default (kDefaultSpinLimit)
-  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1, -1};  // program-build options (-1: default)
+  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1, -1, -1};  // program-build options (-1: default)
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;

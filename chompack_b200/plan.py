@@ -105,8 +105,9 @@ class Plan(object):
 
     def set_option(self, name, value=None):
         """Program-build option of this plan's sweeps (chb_plan_set_option):
-        "small_front_nj", "subtrees", "chol_ksplit", "pinv_ksplit" or
-        "fused_la"; None restores the default.  Drops the compiled programs
+        "small_front_nj", "subtrees", "chol_ksplit", "pinv_ksplit",
+        "fused_la", "tf32_tcgen05" or "ordered_sums" (trsm's additions in a
+        fixed order, bit-reproducible); None restores the default.  Drops the compiled programs
         (the device is synchronised first, so no sweep of the plan is in
         flight)."""
         if self.device >= 0:

@@ -339,7 +339,9 @@ int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
  * static (CTAs take tasks in list order and wait for their dependencies),
  * -1 the default (CHB_SCHEDULE=static|dynamic from the environment, else
  * static for cholesky, llt and trsm and dynamic for the others).  Both give
- * bit-identical results. */
+ * bit-identical results, except for the triangular solve unless
+ * CHB_OPT_ORDERED_SUMS is set (its additions into vector blocks use atomics
+ * by default). */
 int chb_plan_set_schedule(chb_plan* plan, int mode);
 
 /* Program-build options of the plan's sweeps (no counterpart in the
@@ -359,6 +361,9 @@ int chb_plan_set_schedule(chb_plan* plan, int mode);
  *   CHB_OPT_TF32_TCGEN05    mixed precision: TF32 tiles on tcgen05 with
  *                           tensor-memory accumulators (1) or warp-level
  *                           mma.sync (0, the default)
+ *   CHB_OPT_ORDERED_SUMS    trsm: every addition into a vector block in a
+ *                           fixed order (1: bit-reproducible, slower) or
+ *                           with atomics as inputs arrive (0, the default)
  * chb_plan_get_option gives the value the next program build uses. */
 enum chb_option {
   CHB_OPT_SMALL_FRONT_NJ = 0,
@@ -367,7 +372,8 @@ enum chb_option {
   CHB_OPT_PINV_KSPLIT = 3,
   CHB_OPT_FUSED_LA = 4,
   CHB_OPT_TF32_TCGEN05 = 5,
-  CHB_OPT_COUNT = 6
+  CHB_OPT_ORDERED_SUMS = 6,
+  CHB_OPT_COUNT = 7
 };
 int chb_plan_set_option(chb_plan* plan, int option, int64_t value);
 int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value);

@@ -43,6 +43,18 @@ def _tasks(s, nrhs, trans):
     return taskvm.Program(pl.handle, N.OP_TRSM, k=nrhs, flags=1 if trans == "T" else 0, nsn=s.Nsn)
 
 
+def test_ordered_form_has_no_atomics(grid16):
+    s, _ = grid16
+    pl = Plan(s, device=-1)
+    pl.set_option("ordered_sums", 1)
+    assert pl.option("ordered_sums") == 1
+    for trans in ("N", "T"):
+        t = taskvm.Program(pl.handle, N.OP_TRSM, k=8, flags=1 if trans == "T" else 0, nsn=s.Nsn).tasks
+        assert int(np.sum(t["cmode"][t["op"] == taskvm.T_GEMM] == 2)) == 0, trans
+        assert int(np.sum((t["op"] == taskvm.T_VEC) & (t["aux"][:, 0] == 4))) == 0, trans
+        assert int(np.sum(t["op"] == taskvm.T_SUM)) > 0, trans
+
+
 def test_program_has_every_form(grid16):
     s, _ = grid16
     nn = np.diff(np.asarray(s.snptr))
@@ -69,12 +81,16 @@ def test_program_has_every_form(grid16):
 @pytest.mark.parametrize("trans", ["N", "T"])
 @pytest.mark.parametrize("nrhs", [1, 8, 70])
 @pytest.mark.parametrize("order", ["random", "dynamic"])
-def test_program_matches_reference(grid16, trans, nrhs, order):
+@pytest.mark.parametrize("ordered_sums", [0, 1])
+def test_program_matches_reference(grid16, trans, nrhs, order, ordered_sums):
+    """Both forms of the additions into vector blocks: atomic (default) and
+    ordered (CHB_OPT_ORDERED_SUMS: chains and split-K sums)."""
     s, L = grid16
     B0 = np.asfortranarray(np.random.default_rng(nrhs).standard_normal((s.n, nrhs)))
     want = B0.copy(order="F")
     ref.trsm(s, L.copy(), want, alpha=0.5, trans=trans)
     pl = Plan(s, device=-1)
+    pl.set_option("ordered_sums", ordered_sums)
     flags = 1 if trans == "T" else 0
     prog = taskvm.Program(pl.handle, N.OP_TRSM, k=nrhs, flags=flags, nsn=s.Nsn)
     Bf = B0.reshape(-1, order="F").copy()
