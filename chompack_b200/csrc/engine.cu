@@ -1757,7 +1757,7 @@ __device__ void run_asm(const RunArgs& ra, const Task& t, double* smem) {
 //   5. the block and the update matrix (operand c) written back.
 // A non-positive pivot records ctl[2] = j + 1 and continues with 1.
 constexpr int FLD = TILE + 1;
-static_assert(2 * TILE * FLD <= ENGINE_SMEM_BASE_DOUBLES, "small fronts exceed the engine's shared memory");
+static_assert(2 * TILE * FLD + TILE / 2 <= ENGINE_SMEM_BASE_DOUBLES, "small fronts exceed the engine's shared memory");
 
 __device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
   const FrontDesc f = ra.fronts[t.aux[0]];
@@ -1772,14 +1772,32 @@ __device__ void run_front(const RunArgs& ra, const Task& t, double* smem) {
     for (int r = lane; r < nj; r += 32)
       F[c * FLD + r] = (c < nn && r >= c) ? __ldcg(X + (int64_t)c * nj + r) : 0.0;
   __syncthreads();
+  // the children's update matrices, last child first: its relative indices
+  // staged in shared memory, then the lower triangle of U_c flattened over
+  // the threads with FRONT_E loads in flight per thread (a child's entries
+  // land on distinct front entries)
+  constexpr int FRONT_E = 8;
+  int* sr = reinterpret_cast<int*>(F + TILE * FLD + 2 * TILE);
   for (int l = f.chend - 1; l >= f.chbeg; l--) {
     const FrontDesc ch = ra.fronts[ra.chidx[l]];
-    const int Nc = ch.na;
+    const int Nc = ch.na, tot = Nc * Nc;
     const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
     const double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
-    for (int q = warp; q < Nc; q += NW) {
-      const int col = __ldg(rr + q);
-      for (int i = q + lane; i < Nc; i += 32) F[col * FLD + __ldg(rr + i)] += __ldcg(Uc + (int64_t)q * Nc + i);
+    if (tid < Nc) sr[tid] = __ldg(rr + tid);
+    __syncthreads();
+    for (int base = 0; base < tot; base += FRONT_E * NTHREADS) {
+      double v[FRONT_E];
+      int dst[FRONT_E];
+#pragma unroll
+      for (int e = 0; e < FRONT_E; e++) {
+        const int idx = base + tid + e * NTHREADS, q = idx / Nc, i = idx - q * Nc;
+        const bool ok = idx < tot && i >= q;
+        v[e] = ok ? __ldcg(Uc + idx) : 0.0;
+        dst[e] = ok ? sr[q] * FLD + sr[i] : -1;
+      }
+#pragma unroll
+      for (int e = 0; e < FRONT_E; e++)
+        if (dst[e] >= 0) F[dst[e]] += v[e];
     }
     __syncthreads();
   }
@@ -1904,15 +1922,21 @@ __device__ void run_pfront(const RunArgs& ra, const Task& t, double* smem) {
       for (int i = lane; i < na; i += 32) F[j * FLD + nn + i] = G[j * FLD + i];
     __syncthreads();
   }
+  // the children's updates V_c = F(r_c, r_c), lower triangle, the relative
+  // indices staged in shared memory per child
+  int* sr = reinterpret_cast<int*>(smem + 2 * TILE * FLD);
   for (int l = f.chbeg; l < f.chend; l++) {
     const FrontDesc ch = ra.fronts[ra.chidx[l]];
-    const int Nc = ch.na;
+    const int Nc = ch.na, tot = Nc * Nc;
     const int32_t* __restrict__ rr = ra.relidx + ch.relptr;
     double* __restrict__ Uc = ra.bases[B_WS] + t.off2 + ch.upd;
-    for (int q = warp; q < Nc; q += NW) {
-      const int col = __ldg(rr + q);
-      for (int i = q + lane; i < Nc; i += 32) Uc[(int64_t)q * Nc + i] = F[col * FLD + __ldg(rr + i)];
+    if (tid < Nc) sr[tid] = __ldg(rr + tid);
+    __syncthreads();
+    for (int idx = tid; idx < tot; idx += NTHREADS) {
+      const int q = idx / Nc, i = idx - q * Nc;
+      if (i >= q) Uc[idx] = F[sr[q] * FLD + sr[i]];
     }
+    __syncthreads();
   }
   for (int c = warp; c < nn; c += NW)
     for (int r = lane; r < nj; r += 32)
