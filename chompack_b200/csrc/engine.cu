@@ -1525,10 +1525,10 @@ __device__ void run_potrf(const RunArgs& ra, const Task& t, double* smem, int ti
   }
   __syncthreads();
   POTRF_STAMP(0);
-#pragma unroll 1
   // only the 16-column blocks that meet the b x b tile (the padding is the
   // identity and is neither factored nor inverted)
   const int NJ = (b + 15) >> 4, NB = 16 * NJ;
+#pragma unroll 1
   for (int J = 0; J < NJ; J++) {
     const int j0 = 16 * J, j1 = j0 + 16, jp = j0 - 16;
     const bool panel = factor && J > 0;     // panel of block J-1 and the updates it feeds
