@@ -2,13 +2,15 @@
 times (for profiling a single kernel launch, e.g. under ncu):
 
     python -m chompack_b200.sweeprun --side 40 --merge 32 --sweep cholesky --precision fp64 --reps 3
+    python -m chompack_b200.sweeprun --side 40 --merge 32 --sweep trsm --nrhs 8 --trans N --reps 3
 
 The matrix is the seeded 3-D 7-point grid side^3 (or the 2-D 5-point grid
 with --grid2d) with AMD ordering and merge_size_fill(merge, merge), or with
 --batch N the first N matrices of the uneven batch (2-D grids of side 20..120
 with two extra neighbours per node, AMD, no merging) in one merged plan;
 each repetition refreshes the values and launches the sweep once
-(projected_inverse runs on the factor of a preceding, untimed cholesky).
+(projected_inverse and trsm run on the factor of a preceding, untimed
+cholesky; trsm on --nrhs seeded N(0,1) right-hand sides).
 """
 import argparse
 import json
@@ -28,7 +30,9 @@ def main():
     ap.add_argument("--side", type=int, default=40)
     ap.add_argument("--grid2d", action="store_true")
     ap.add_argument("--merge", type=int, default=32)
-    ap.add_argument("--sweep", default="cholesky", choices=["cholesky", "projected_inverse"])
+    ap.add_argument("--sweep", default="cholesky", choices=["cholesky", "projected_inverse", "trsm"])
+    ap.add_argument("--nrhs", type=int, default=8)
+    ap.add_argument("--trans", default="N", choices=["N", "T"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32", "tf32x3"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--batch", type=int, default=0)
@@ -39,6 +43,8 @@ def main():
     s = symbolic(A, p=amd.order(A), merge_function=merge_size_fill(args.merge, args.merge))
     X0 = cspmatrix(s) + A
     base = X0.blkval
+    if args.sweep == "trsm":
+        return run_trsm(args, s, base)
     if args.sweep == "projected_inverse":
         L = cspmatrix(s, blkval=base.clone())
         cbase.cholesky(L, precision=args.precision)
@@ -56,6 +62,26 @@ def main():
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
     print(json.dumps({"sweep": args.sweep, "precision": args.precision, "n": s.n, "nsn": s.Nsn,
+                      "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
+
+
+def run_trsm(args, s, base):
+    L = cspmatrix(s, blkval=base.clone())
+    cbase.cholesky(L, precision=args.precision)
+    B0 = torch.randn(args.nrhs, s.n, dtype=torch.float64, device=base.device,
+                     generator=torch.Generator(base.device).manual_seed(5)).t()   # column-major n x nrhs
+    Bt = B0.clone().t().contiguous().t()
+    times = []
+    for _ in range(args.reps):
+        Bt.copy_(B0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        cbase.trsm(L, Bt, trans=args.trans)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(json.dumps({"sweep": "trsm", "trans": args.trans, "nrhs": args.nrhs, "n": s.n, "nsn": s.Nsn,
                       "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
 
 
