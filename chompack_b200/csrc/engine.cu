@@ -2768,29 +2768,41 @@ __global__ void __launch_bounds__(NTHREADS, 2) engine_kernel(RunArgs ra) {
         for (int w = threadIdx.x; w < 36; w += NTHREADS) dst[w] = __ldg(src + w);
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
-        if (ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
-        int abort = 0;
+      if (threadIdx.x < 32) {
+        // the task's waits, one per lane of warp 0 (32 at a time), so that
+        // the wait records and the counters are read in one round each
+        const int lane = threadIdx.x;
+        if (lane == 0 && ra.trace) ra.trace[4 * (int64_t)ti] = global_ns();
+        int abort = 0, timed_out = 0;
         const int npre = ((s_t.op == T_POTRF && s_t.k > 0) || s_t.op == T_TRSV) ? (int)s_t.cdiag : (int)s_t.nwait;
-        for (int w = 0; w < npre && !abort; w++) {
-          const int2 wt = ra.waits[s_t.wait_off + w];
-          int64_t spins = 0;
-          unsigned ns = 16;
-          while (ld_acquire(ra.counters + wt.x) < wt.y) {
-            if (++spins > ra.spin_limit) {
-              atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
-              atomicAdd(&ra.ctl[3], 1);
-              abort = 1;
-              break;
+        for (int w0 = 0; w0 < npre; w0 += 32) {
+          if (w0 + lane < npre) {
+            const int2 wt = ra.waits[s_t.wait_off + w0 + lane];
+            int64_t spins = 0;
+            unsigned ns = 16;
+            while (ld_acquire(ra.counters + wt.x) < wt.y) {
+              if (++spins > ra.spin_limit) {
+                atomicCAS(&ra.ctl[1], 0, DE_TIMEOUT);
+                abort = timed_out = 1;
+                break;
+              }
+              if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
+              __nanosleep(ns);
+              if (ns < 128) ns <<= 1;
             }
-            if ((spins & 15) == 0 && ld_volatile(&ra.ctl[1]) != 0) { abort = 1; break; }
-            __nanosleep(ns);
-            if (ns < 128) ns <<= 1;
+          }
+          if (__any_sync(0xffffffffu, abort)) {
+            abort = 1;
+            break;
           }
         }
-        if (!abort && ld_volatile(&ra.ctl[1]) != 0) abort = 1;
-        s_abort = abort;
-        if (ra.trace) ra.trace[4 * (int64_t)ti + 1] = global_ns();
+        timed_out = __any_sync(0xffffffffu, timed_out);
+        if (lane == 0) {
+          if (timed_out) atomicAdd(&ra.ctl[3], 1);  // CTAs whose wait ran out
+          if (!abort && ld_volatile(&ra.ctl[1]) != 0) abort = 1;
+          s_abort = abort;
+          if (ra.trace) ra.trace[4 * (int64_t)ti + 1] = global_ns();
+        }
       }
       __syncthreads();
       if (s_abort) break;
