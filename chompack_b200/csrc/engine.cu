@@ -2892,6 +2892,8 @@ size_t engine_smem_bytes() { return (size_t)ENGINE_SMEM_DOUBLES * sizeof(double)
 // uses ra.smem_doubles (at least the GEMM/POTRF staging).
 cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream) {
   if (ra.smem_doubles < ENGINE_SMEM_BASE_DOUBLES || ra.smem_doubles > ENGINE_SMEM_DOUBLES) return cudaErrorInvalidValue;
+  // the tcgen05 build is sized (engine_occupancy) for the base staging only
+  if (ra.tmem && ra.smem_doubles != ENGINE_SMEM_BASE_DOUBLES) return cudaErrorInvalidValue;
   size_t smem = (size_t)ra.smem_doubles * sizeof(double);
   if (ra.tmem) engine_kernel<true><<<grid, NTHREADS, smem, stream>>>(ra);
   else engine_kernel<false><<<grid, NTHREADS, smem, stream>>>(ra);
@@ -2899,14 +2901,20 @@ cudaError_t engine_launch(const RunArgs& ra, int grid, cudaStream_t stream) {
 }
 
 // Resident CTAs per SM of one instantiation (tc: the tcgen05 one).  The
-// dynamic shared-memory attribute is raised on both.
+// dynamic shared-memory attribute is raised on both.  The FP64 build is
+// sized for the largest staging (Householder panels, solve steps); the
+// tcgen05 build only runs the TF32 sweeps, which launch with the base
+// staging, and is queried at that size (the query still reports one CTA per
+// SM for it; the plan launches it as wide as the FP64 build, see
+// upload_plan).
 int engine_occupancy(int* blocks_per_sm, bool tc) {
   size_t smem = engine_smem_bytes();
   cudaError_t e = cudaFuncSetAttribute(engine_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(engine_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return -1;
-  e = tc ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<true>, NTHREADS, smem)
+  const size_t smem_tc = (size_t)ENGINE_SMEM_BASE_DOUBLES * sizeof(double);
+  e = tc ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<true>, NTHREADS, smem_tc)
          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, engine_kernel<false>, NTHREADS, smem);
   return e == cudaSuccess ? 0 : -1;
 }

@@ -375,9 +375,15 @@ static int upload_plan(chb_plan* P) {
   if (engine_occupancy(&per_sm) != 0 || per_sm <= 0) return set_error(-12, "engine kernel cannot be resident");
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
   P->grid = per_sm * nsm;
+  // The tcgen05 build has the FP64 build's registers and (at the base
+  // staging its TF32 sweeps use) shared memory; the occupancy query reports
+  // one CTA per SM for it, but two run side by side: launched with two per
+  // SM, the 48^3 TF32 sweeps on tcgen05 took 16.5 / 20.5 ms against 26.3 /
+  // 34.0 ms with one.  A CTA that is not resident claims nothing until it
+  // is, so the wider grid is safe either way.
   int per_sm_tc = 0;
   if (engine_occupancy(&per_sm_tc, true) != 0 || per_sm_tc <= 0) return set_error(-12, "engine kernel cannot be resident");
-  P->grid_tc = per_sm_tc * nsm;
+  P->grid_tc = std::max(per_sm_tc, per_sm) * nsm;
   return 0;
 }
 
