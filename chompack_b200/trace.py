@@ -13,7 +13,8 @@ dynamic schedule every CTA was busy).
     python -m chompack_b200.trace --side 40 --merge 32 32 [--trsm 8]
 
 prints the summary for cholesky and projected_inverse on the 3-D 7-point
-grid side^3 (AMD order, merge_size_fill(merge)), and with --trsm R for the
+grid side^3 (--grid2d: the 2-D 5-point grid side^2; AMD order,
+merge_size_fill(merge)), and with --trsm R for the
 triangular solves 'N' and 'T' with R right-hand sides; it needs a GPU.
 """
 import argparse
@@ -158,6 +159,7 @@ def main():
     ap.add_argument("--trsm", type=int, default=0, help="also trace trsm with this many right-hand sides")
     ap.add_argument("--batch", type=int, default=0,
                     help="trace the first BATCH matrices of the uneven 2-D batch in one merged plan instead")
+    ap.add_argument("--grid2d", action="store_true", help="the 2-D 5-point grid side^2 instead")
     ap.add_argument("--dump", default="", help="also save each sweep's task records and raw trace (.npz)")
     args = ap.parse_args()
     import torch
@@ -165,7 +167,7 @@ def main():
     from chompack_b200 import grids
     if args.batch:
         return trace_batch(args)
-    A = grids.grid3d(args.side, seed=0)
+    A = grids.grid2d(args.side, seed=0) if args.grid2d else grids.grid3d(args.side, seed=0)
     s = cp.symbolic(A, p=cp.amd.order(A), merge_function=cp.merge_size_fill(*args.merge))
     x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.cuda()
     plan = s.plan(0)
@@ -181,8 +183,9 @@ def main():
         for trans in ("N", "T"):
             sweeps += (("trsm_" + trans, N.OP_TRSM, lambda tr=trans: cp.trsm(L, B0.clone().t().contiguous().t(),
                                                                               trans=tr)),)
-    out = {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(%d,%d)"
-                       % (args.side, s.n, args.merge[0], args.merge[1])}
+    out = {"workload": "%s grid %d^%d (n=%d), AMD, merge_size_fill(%d,%d)"
+                       % ("2-D 5-point" if args.grid2d else "3-D 7-point", args.side, 2 if args.grid2d else 3, s.n,
+                          args.merge[0], args.merge[1])}
     for name, op, fn in sweeps:
         for _ in range(args.warmup):
             fn()
