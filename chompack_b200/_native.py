@@ -74,6 +74,8 @@ completion = _sig("chb_completion", ctypes.c_int, [PPLAN, vp, ctypes.c_int, vp, 
 hessian = _sig("chb_hessian", ctypes.c_int, [PPLAN, vp, vp, ctypes.POINTER(vp), i64, ctypes.c_int, ctypes.c_int,
                                              ctypes.c_int, vp, ctypes.c_size_t, vp])
 trsm = _sig("chb_trsm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
+trsm_reuse = _sig("chb_trsm_reuse", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp,
+                                                   ctypes.c_size_t, ctypes.c_int, vp])
 trmm = _sig("chb_trmm", ctypes.c_int, [PPLAN, ctypes.c_char, i64, ctypes.c_double, vp, vp, i64, vp, ctypes.c_size_t, vp])
 dot = _sig("chb_dot", ctypes.c_int, [PPLAN, vp, vp, vp, vp, ctypes.c_size_t, vp])
 plan_merge = _sig("chb_plan_merge", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,

@@ -242,6 +242,25 @@ def trsm(L, B, alpha=1.0, trans='N', nrhs=None, offsetB=0, ldB=None):
             host[:, :] = out.reshape(host.shape, order="F")
 
 
+def _trsm_reuse(L, B, trans, reuse, slot):
+    """trsm on a column-major CUDA tensor B through chb_trsm_reuse, with the
+    workspace of `slot`: with reuse the step operands are taken from that
+    workspace as the previous call on it (same factor, trans and number of
+    right-hand sides) left them.  For repeated solves (mixed.solve)."""
+    v = _values(L, "L")
+    dev = v.device
+    if B.dim() != 2 or B.stride(0) != 1 or B.device != dev or B.dtype != torch.float64:
+        raise ValueError("B must be a column-major float64 tensor on the device of L")
+    nrhs, ld = B.shape[1], B.stride(1)
+    plan = L.symb.plan(dev.index)
+    flags = (1 if trans == 'T' else 0) | 2
+    ws, nb = plan.workspace(N.OP_TRSM, nrhs, flags, slot=slot)
+    s = _stream(dev)
+    _check(N.trsm_reuse(plan.handle, trans.encode(), int(nrhs), 1.0, v.data_ptr(), B.data_ptr(), int(ld), ws, nb,
+                        1 if reuse else 0, s), "launch")
+    _check(N.info(plan.handle, ws, s), "sweep")
+
+
 def trmm(L, B, alpha=1.0, trans='N', nrhs=None, offsetB=0, ldB=None):
     """Multiplication with a cspmatrix factor (pybase/trmm.py:4-116):
     B := alpha L B (trans 'N') or alpha L^T B (trans 'T'), in place.

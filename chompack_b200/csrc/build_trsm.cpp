@@ -40,7 +40,7 @@
 
 namespace chb {
 
-int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
+int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool reuse) {
   const int T = TILE;
   const int64_t N = P.nsn;
   const int64_t n = P.n;
@@ -147,16 +147,18 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
     B.add(t, {-3, 0, 0, 0, (int)(r0 / RCH), 0}, gath, 1.5 + (double)RCH * nrhs / 4000.0);
   }
   // step operands of every diagonal block (independent of the sweep): the
-  // inverse M_c, then G_c, G2_c / H_c, H2_c from it
+  // inverse M_c, then G_c, G2_c / H_c, H2_c from it; with `reuse` they are
+  // left in the workspace by an earlier solve with the same factor, trans
+  // and nrhs (the layout depends on nothing else), and not computed again
   std::vector<std::vector<int>> inv(N);
   std::vector<std::vector<std::array<int, 2>>> coup(N);
   for (int64_t k = 0; k < N; k++) {
     const FrontDesc& f = P.fronts[k];
     const int nn = f.nn, nj = f.nj, NBc = ceil_div(nn, T);
     auto bw = [&](int c) { return std::min(T, nn - c * T); };
-    inv[k].resize(NBc);
+    inv[k].assign(NBc, -1);
     coup[k].assign(NBc, {-1, -1});
-    for (int c = 0; c < NBc; c++) {
+    for (int c = 0; c < NBc && !reuse; c++) {
       const int cT = c * T;
       Task t = make_task(T_POTRF);
       t.m = t.n = bw(c);
@@ -169,7 +171,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans) {
       t.aux[2] = 1;
       inv[k][c] = B.add(t, {-2, 0, 0, (int)k, c, 0});
     }
-    for (int c = 0; c < NBc; c++) {
+    for (int c = 0; c < NBc && !reuse; c++) {
       const int cT = c * T, ld = sld[k][c];
       for (int d = 1; d <= 2; d++) {
         if (!trans && c >= d) {

@@ -134,6 +134,15 @@ extern "C" int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, 
                 alpha);
 }
 
+extern "C" int chb_trsm_reuse(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval,
+                              double* B, int64_t ldB, void* work, size_t work_bytes, int reuse, void* stream) {
+  if (trans != 'N' && trans != 'T') return set_error(-1, "trans must be 'N' or 'T'");
+  if (nrhs < 0 || (plan && ldB < plan->n)) return set_error(-1, "invalid nrhs or ldB");
+  double* bases[B_RHS + 1] = {const_cast<double*>(blkval), nullptr, nullptr, nullptr, B};
+  const int flags = (trans == 'T' ? 1 : 0) | (reuse ? 2 : 0);
+  return run_op(plan, CHB_OP_TRSM, nrhs, flags, bases, B_RHS + 1, work, work_bytes, stream, ldB, alpha);
+}
+
 extern "C" int chb_trmm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
                         int64_t ldB, void* work, size_t work_bytes, void* stream) {
   if (trans != 'N' && trans != 'T') return set_error(-1, "trans must be 'N' or 'T'");

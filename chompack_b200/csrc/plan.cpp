@@ -140,7 +140,7 @@ Program* build_host_program(chb_plan* plan, int op, int64_t k, int flags) {
     case CHB_OP_PROJECTED_INVERSE: rc = build_projected_inverse(*plan, *prog); break;
     case CHB_OP_LLT: rc = build_llt(*plan, *prog); break;
     case CHB_OP_COMPLETION: rc = build_completion(*plan, *prog, k != 0); break;
-    case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, flags != 0); break;
+    case CHB_OP_TRSM: rc = build_trsm(*plan, *prog, k, (flags & 1) != 0, (flags & 2) != 0); break;
     case CHB_OP_TRMM: rc = build_trmm(*plan, *prog, k, flags != 0); break;
     case CHB_OP_HESSIAN: rc = build_hessian(*plan, *prog, (int)k, flags); break;
     case CHB_OP_CONVENTIONAL: rc = build_conventional(*plan, *prog); break;

@@ -175,7 +175,8 @@ int build_projected_inverse(const chb_plan& P, Program& prog);
 int build_llt(const chb_plan& P, Program& prog);
 int build_conventional(const chb_plan& P, Program& prog);
 int build_completion(const chb_plan& P, Program& prog, bool factored);
-int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans);
+// trsm flags: 1 trans 'T', 2 the step operands are already in the workspace
+int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool reuse = false);
 int build_trmm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans);
 // flags: adj | inv << 1 | factored_updates << 2; nu U matrices in base slots
 // B_U0 .. B_U0 + nu - 1.

@@ -81,10 +81,13 @@ def solve(X, L, B, tol=1e-12, maxiter=30):
     r = Bc.clone()
     history = []
     it = 0
+    # the solves' step operands (diagonal-tile inverses and their coupling
+    # products, from L alone) are computed by the first iteration and reused
+    slots = ("refine_N", "refine_T")
     for it in range(1, maxiter + 1):
         d = r.clone()
-        cbase.trsm(L, d, trans='N')
-        cbase.trsm(L, d, trans='T')
+        cbase._trsm_reuse(L, d, 'N', it > 1, slots[0])
+        cbase._trsm_reuse(L, d, 'T', it > 1, slots[1])
         x += d
         r = symv(X, x, alpha=-1.0, y=Bc)
         res = float((torch.linalg.vector_norm(r, dim=0) / bn).max())

@@ -203,6 +203,17 @@ int chb_hessian(chb_plan* plan, const double* lblkval, const double* yblkval, do
 int chb_trsm(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
              int64_t ldB, void* work, size_t work_bytes, void* stream);
 
+/* trsm for repeated solves with one factor (no counterpart in the
+ * reference; iterative refinement calls it twice per iteration).  A solve
+ * computes, from L alone, the inverses of the diagonal tiles and their
+ * coupling products into its workspace; with reuse != 0 they are taken
+ * from `work` as an earlier call left them, which must have had the same
+ * plan, trans, nrhs and unchanged blkval, with no other call using `work`
+ * in between (the caller keeps one workspace per trans).  reuse == 0 is
+ * chb_trsm. */
+int chb_trsm_reuse(chb_plan* plan, char trans, int64_t nrhs, double alpha, const double* blkval, double* B,
+                   int64_t ldB, void* work, size_t work_bytes, int reuse, void* stream);
+
 /* trmm — pybase/trmm.py:4-116 (Python only in the reference).  B :=
  * alpha*L*B (trans 'N') or alpha*L^T*B (trans 'T') with the factor that
  * chb_cholesky leaves in blkval; B as for chb_trsm.  Workspace

@@ -119,3 +119,22 @@ def test_tcgen05_tiles_agree_with_mma_sync_tiles(tmp_path):
     e_ms = np.abs(other - ref64).max() / scale
     assert 0.0 < e_tc <= 2e-3 and 0.0 < e_ms <= 2e-3, (e_tc, e_ms)
     assert np.abs(got - other).max() / scale <= 0.5 * max(e_tc, e_ms), (e_tc, e_ms)
+
+
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_trsm_reuse_matches_trsm(trans):
+    """chb_trsm_reuse (the refinement's solves): a first call computes the
+    step operands, later calls on the same workspace reuse them; every
+    result agrees with cbase.trsm to rounding."""
+    from chompack_b200 import cbase
+    A, s = problem("grid3d", 14, merge=(32, 32), seed=4)
+    L = cp.cspmatrix(s, device="cuda") + A
+    cp.cholesky(L)
+    for it in range(3):
+        B = torch.randn(5, s.n, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(it)).t()
+        want = B.clone()
+        cbase.trsm(L, want, trans=trans)
+        got = B.clone()
+        cbase._trsm_reuse(L, got, trans, it > 0, "test_reuse_" + trans)
+        err = float(((got - want).abs().max(dim=0).values / want.abs().max(dim=0).values).max())
+        assert err <= 1e-13, (it, err)

@@ -103,3 +103,29 @@ def test_program_matches_reference(grid16, trans, nrhs, order, ordered_sums):
     got = Bf.reshape(B0.shape, order="F")
     err = np.max(np.abs(got - want) / np.maximum(np.abs(want).max(axis=0), 1e-300))
     assert err <= 1e-12, err
+
+
+@pytest.mark.parametrize("trans", ["N", "T"])
+def test_reuse_program_takes_the_step_operands_from_the_workspace(grid16, trans):
+    """chb_trsm_reuse: the program with flag 2 has no diagonal-tile inverse or
+    coupling tasks and, run on the workspace a full solve left, solves again
+    (a second right-hand side) to the reference's result."""
+    s, L = grid16
+    flags = 1 if trans == "T" else 0
+    pl = Plan(s, device=-1)
+    full = taskvm.Program(pl.handle, N.OP_TRSM, k=8, flags=flags, nsn=s.Nsn)
+    again = taskvm.Program(pl.handle, N.OP_TRSM, k=8, flags=flags | 2, nsn=s.Nsn)
+    assert again.ws_doubles == full.ws_doubles
+    assert int(np.sum(again.tasks["op"] == taskvm.T_POTRF)) == 0
+    assert int(np.sum(full.tasks["op"] == taskvm.T_POTRF)) > 0
+    ws = np.full(full.ws_doubles, np.nan)
+    for prog, seed in ((full, 1), (again, 2)):
+        B0 = np.asfortranarray(np.random.default_rng(seed).standard_normal((s.n, 8)))
+        want = B0.copy(order="F")
+        ref.trsm(s, L.copy(), want, alpha=0.5, trans=trans)
+        Bf = B0.reshape(-1, order="F").copy()
+        vm = taskvm.VM(prog, {0: L.copy(), 1: ws, 4: Bf}, s.relidx, s.chidx, perm=s.p, ldb=s.n, alpha=0.5)
+        vm.run("random", seed=seed)
+        got = Bf.reshape(B0.shape, order="F")
+        err = np.max(np.abs(got - want) / np.maximum(np.abs(want).max(axis=0), 1e-300))
+        assert err <= 1e-12, err
