@@ -253,8 +253,7 @@ def _trsm_reuse(L, B, trans, reuse, slot):
         raise ValueError("B must be a column-major float64 tensor on the device of L")
     nrhs, ld = B.shape[1], B.stride(1)
     plan = L.symb.plan(dev.index)
-    flags = (1 if trans == 'T' else 0) | 2
-    ws, nb = plan.workspace(N.OP_TRSM, nrhs, flags, slot=slot)
+    ws, nb = plan.workspace(N.OP_TRSM, nrhs, (1 if trans == 'T' else 0) | (2 if reuse else 0), slot=slot)
     s = _stream(dev)
     _check(N.trsm_reuse(plan.handle, trans.encode(), int(nrhs), 1.0, v.data_ptr(), B.data_ptr(), int(ld), ws, nb,
                         1 if reuse else 0, s), "launch")

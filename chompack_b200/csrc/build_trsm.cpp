@@ -147,9 +147,14 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool 
     B.add(t, {-3, 0, 0, 0, (int)(r0 / RCH), 0}, gath, 1.5 + (double)RCH * nrhs / 4000.0);
   }
   // step operands of every diagonal block (independent of the sweep): the
-  // inverse M_c, then G_c, G2_c / H_c, H2_c from it; with `reuse` they are
+  // inverse M_c, then G_c, G2_c / H_c, H2_c from it.  With `reuse` they are
   // left in the workspace by an earlier solve with the same factor, trans
-  // and nrhs (the layout depends on nothing else), and not computed again
+  // and nrhs, and each of their tasks is a no-op: the program keeps the
+  // same tasks and counters, so its workspace has the same layout
+  auto add_step_operand = [&](const Task& t, const SchedKey& key) {
+    if (!reuse) return B.add(t, key);
+    return B.add(make_task(T_NOP), key, -1, 0.3);
+  };
   std::vector<std::vector<int>> inv(N);
   std::vector<std::vector<std::array<int, 2>>> coup(N);
   for (int64_t k = 0; k < N; k++) {
@@ -158,7 +163,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool 
     auto bw = [&](int c) { return std::min(T, nn - c * T); };
     inv[k].assign(NBc, -1);
     coup[k].assign(NBc, {-1, -1});
-    for (int c = 0; c < NBc && !reuse; c++) {
+    for (int c = 0; c < NBc; c++) {
       const int cT = c * T;
       Task t = make_task(T_POTRF);
       t.m = t.n = bw(c);
@@ -169,9 +174,9 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool 
       t.aux[0] = cT;
       t.aux[1] = 1;
       t.aux[2] = 1;
-      inv[k][c] = B.add(t, {-2, 0, 0, (int)k, c, 0});
+      inv[k][c] = add_step_operand(t, {-2, 0, 0, (int)k, c, 0});
     }
-    for (int c = 0; c < NBc && !reuse; c++) {
+    for (int c = 0; c < NBc; c++) {
       const int cT = c * T, ld = sld[k][c];
       for (int d = 1; d <= 2; d++) {
         if (!trans && c >= d) {
@@ -181,7 +186,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool 
           Operand a = opnd(B_WS, soff[k][c] + mcol * ld, ld);
           Operand b = opnd(B_X, f.blk + (int64_t)(cT - d * T) * nj + cT, nj, OM_T);
           Task g = gemm(bw(c), T, bw(c), -1.0, a, b, 0.0, opnd(B_WS, soff[k][c] + (mcol - (int64_t)d * T) * ld, ld));
-          coup[k][c][d - 1] = B.add(g, {-1, 0, 0, (int)k, c, d});
+          coup[k][c][d - 1] = add_step_operand(g, {-1, 0, 0, (int)k, c, d});
           B.wait_task(coup[k][c][d - 1], inv[k][c]);
         } else if (trans && c + d < NBc) {
           // -H_c (d = 1) / -H2_c (d = 2) = -L_{c+d,c} M_c  (bw(c+d) x 64),
@@ -189,7 +194,7 @@ int build_trsm(const chb_plan& P, Program& prog, int64_t nrhs, bool trans, bool 
           Operand a = opnd(B_X, f.blk + (int64_t)cT * nj + cT + d * T, nj);
           Operand b = opnd(B_WS, soff[k][c], ld, OM_T);
           Task h = gemm(bw(c + d), T, T, -1.0, a, b, 0.0, opnd(B_WS, soff[k][c] + d * T, ld));
-          coup[k][c][d - 1] = B.add(h, {-1, 0, 0, (int)k, c, d});
+          coup[k][c][d - 1] = add_step_operand(h, {-1, 0, 0, (int)k, c, d});
           B.wait_task(coup[k][c][d - 1], inv[k][c]);
         }
       }

@@ -107,15 +107,18 @@ def test_program_matches_reference(grid16, trans, nrhs, order, ordered_sums):
 
 @pytest.mark.parametrize("trans", ["N", "T"])
 def test_reuse_program_takes_the_step_operands_from_the_workspace(grid16, trans):
-    """chb_trsm_reuse: the program with flag 2 has no diagonal-tile inverse or
-    coupling tasks and, run on the workspace a full solve left, solves again
-    (a second right-hand side) to the reference's result."""
+    """chb_trsm_reuse: the program with flag 2 has no-ops for the diagonal-tile
+    inverse and coupling tasks and, run on the workspace a full solve left,
+    solves again (a second right-hand side) to the reference's result."""
     s, L = grid16
     flags = 1 if trans == "T" else 0
     pl = Plan(s, device=-1)
     full = taskvm.Program(pl.handle, N.OP_TRSM, k=8, flags=flags, nsn=s.Nsn)
     again = taskvm.Program(pl.handle, N.OP_TRSM, k=8, flags=flags | 2, nsn=s.Nsn)
     assert again.ws_doubles == full.ws_doubles
+    # the same tasks and counters (so the same workspace layout on the
+    # device), the operand tasks turned into no-ops
+    assert again.ntasks == full.ntasks and again.ncounters == full.ncounters
     assert int(np.sum(again.tasks["op"] == taskvm.T_POTRF)) == 0
     assert int(np.sum(full.tasks["op"] == taskvm.T_POTRF)) > 0
     ws = np.full(full.ws_doubles, np.nan)
