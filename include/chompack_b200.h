@@ -349,7 +349,8 @@ int chb_set_trace(chb_plan* plan, void* buffer, int64_t capacity_tasks);
  * its waiters; CTAs claim ready tasks near the lowest list positions), 1
  * static (CTAs take tasks in list order and wait for their dependencies),
  * -1 the default (CHB_SCHEDULE=static|dynamic from the environment, else
- * static for cholesky, llt and trsm and dynamic for the others).  Both give
+ * static for cholesky, llt and trsm, and for projected_inverse on a merged
+ * plan, and dynamic for the others).  Both give
  * bit-identical results, except for the triangular solve unless
  * CHB_OPT_ORDERED_SUMS is set (its additions into vector blocks use atomics
  * by default). */
