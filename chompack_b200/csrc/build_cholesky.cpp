@@ -126,7 +126,9 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       for (int j = nn; j < nj; j++) colwork[j] += nj - j;  // zeroing of U_k
       double total = 0.0;
       for (double w : colwork) total += w;
-      const double target = std::max(4096.0, total / 256.0);
+      // (a merged plan, a batch of independent trees, is bound by its total
+      // work rather than by one tree's chain: fewer, larger chunks there)
+      const double target = std::max(P.seg.size() > 2 ? 16384.0 : 4096.0, total / 256.0);
       int j0 = 0;
       while (j0 < nj) {
         int j1 = j0;
