@@ -223,19 +223,26 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           B.group_size[yfinal]++;
         }
     }
-    // children's updates
+    // children's updates, CH columns per task (on a merged plan, a batch
+    // bound by its total work, columns up to about 16k entries per task)
+    const bool merged = P.seg.size() > 2;
     for (int l = f.chbeg; l < f.chend; l++) {
       const int c = P.chidx[l];
       const int Nc = P.fronts[c].na;
-      for (int q0 = 0; q0 < Nc; q0 += CH) {
+      for (int q0 = 0, q1 = 0; q0 < Nc; q0 = q1) {
+        q1 = std::min(Nc, q0 + CH);
+        if (merged) {
+          int64_t w = 0;
+          for (q1 = q0; q1 < Nc && (q1 - q0 < CH || w < 16384) && q1 - q0 < 4 * CH; q1++) w += Nc - q1;
+        }
         Task t = make_task(T_EXTRACT);
         t.aux[0] = c;
         t.aux[1] = q0;
-        t.aux[2] = std::min(Nc, q0 + CH);
+        t.aux[2] = q1;
         t.a = opnd(B_WS, Y, nn);
         t.b = opnd(B_WS, na > 0 ? S : 0, std::max(na, 1));
         t.c = opnd(B_WS, upd, std::max(na, 1));
-        int id = B.add(t, {lv, 5, 0, (int)k, c, q0}, vready[c], 3.0 + (double)(Nc - q0) * CH / 2000.0);
+        int id = B.add(t, {lv, 5, 0, (int)k, c, q0}, vready[c], 3.0 + (double)(Nc - q0) * (q1 - q0) / 2000.0);
         B.wait_group(id, yfinal);
         B.wait_group(id, sgroup);
       }
