@@ -585,6 +585,7 @@ def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
     Hu = U.copy()
     ref.hessian(s, Lr, Yr, [Hu], adj=None, factored_updates=True)
     second_ref = -ref.dot(s, U.copy(), Hu)
+    memory = autograd_memory(dev, s, x0, reps, g)
     return {"workload": "3-D 7-point grid %d^3 (n=%d), AMD, merge_size_fill(32,32), %d value sets through "
                         "chompack_b200.autograd.logdet_values (torch.autograd.grad)" % (side, s.n, value_sets),
             "fwd_bwd_ms": round(ms, 3), "gflops": round(flops / ms / 1e6, 1),
@@ -593,7 +594,57 @@ def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
                                  "reduction (2 kernels) and the gradient weights (1 kernel)"},
             "gradient_rel_error_vs_reference": abs(gU - want) / abs(want),
             "gradient_fd_rel_error": abs(gU - fd) / abs(fd), "fd_step": h,
-            "hvp_rel_error_vs_reference": abs(second - second_ref) / abs(second_ref)}
+            "hvp_rel_error_vs_reference": abs(second - second_ref) / abs(second_ref),
+            "memory": memory}
+
+
+def autograd_memory(dev, s, x0, reps, g_default):
+    """Memory against time for the autograd workload: the sweeps' workspace
+    (update matrices, per-front scratch, counters) with every update matrix
+    in memory of its own (the default), and with them in a pool limited to
+    the reference's postorder stack size per value set (plan option
+    scratch_limit); the forward + backward time with that limit, and with
+    the factor recomputed in the backward instead of kept (recompute_factor).
+    Each variant's gradient must be bit-identical to the default's."""
+    import torch
+    from chompack_b200 import _native as N, autograd
+    sets = int(x0.shape[0])
+    Bt = autograd._value_sets(s, sets, x0.device)
+    ops = (("cholesky", N.OP_CHOLESKY), ("projected_inverse", N.OP_PROJECTED_INVERSE))
+
+    def workspace():
+        return {name: Bt.plan.pool_info(op)["workspace_bytes"] for name, op in ops}
+
+    def run(**kw):
+        x = x0.detach().requires_grad_(True)
+        ld = autograd.logdet_values(x, s, **kw)
+        (g,) = torch.autograd.grad(ld.sum(), x)
+        return g
+
+    nv = int(s.blkptr[-1])
+    limit = int(s.memory["stack_mem"]) * 8 * sets
+    out = {"update_matrices_bytes": int(sum(int(f) ** 2 for f in _update_orders(s))) * 8 * sets,
+           "reference_stack_bytes": limit, "factor_kept_bytes": nv * 8 * sets,
+           "default": {"workspace_bytes": workspace()}}
+    for label, kw in (("scratch_limit", {"scratch_limit": limit}), ("recompute_factor", {"recompute_factor": True})):
+        ms = _event_ms(dev, lambda: run(**kw), reps)
+        g = run(**kw)
+        entry = {"fwd_bwd_ms": round(ms, 3), "gradient_bit_identical": bool(torch.equal(g, g_default))}
+        if "scratch_limit" in kw:
+            entry["scratch_limit_bytes"] = limit
+            entry["workspace_bytes"] = workspace()
+            entry["pool_bytes"] = {name: Bt.plan.pool_info(op)["pool_bytes"] for name, op in ops}
+        else:
+            entry["factor_kept_bytes"] = 0
+        out[label] = entry
+        autograd._limit_scratch(Bt.plan, None)
+    return out
+
+
+def _update_orders(s):
+    """|A_k| of every supernode (the order of its update matrix)."""
+    nn = np.diff(np.asarray(s.snptr))
+    return np.diff(np.asarray(s.blkptr)) // nn - nn
 
 
 def _engine_occupancy():

@@ -67,6 +67,7 @@ plan_destroy = _sig("chb_plan_destroy", ctypes.c_int, [PPLAN])
 workspace_size = _sig("chb_workspace_size", ctypes.c_int,
                       [PPLAN, ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)])
 program_info = _sig("chb_program_info", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64])
+program_pool = _sig("chb_program_pool", ctypes.c_int, [PPLAN, ctypes.c_int, i64, ctypes.c_int, P64])
 cholesky = _sig("chb_cholesky", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 projected_inverse = _sig("chb_projected_inverse", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
 llt = _sig("chb_llt", ctypes.c_int, [PPLAN, vp, vp, ctypes.c_size_t, vp])
@@ -128,5 +129,5 @@ add_sparse = _sig("chb_add_sparse", ctypes.c_int, [PPLAN, vp, vp, vp, i64, vp, v
 plan_set_option = _sig("chb_plan_set_option", ctypes.c_int, [PPLAN, ctypes.c_int, i64])
 plan_get_option = _sig("chb_plan_get_option", ctypes.c_int, [PPLAN, ctypes.c_int, ctypes.POINTER(i64)])
 OPTIONS = {"small_front_nj": 0, "subtrees": 1, "chol_ksplit": 2, "pinv_ksplit": 3, "fused_la": 4,
-           "tf32_tcgen05": 5, "ordered_sums": 6}
+           "tf32_tcgen05": 5, "ordered_sums": 6, "scratch_limit": 7}
 engine_occupancy = _sig("chb_engine_occupancy", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int)])

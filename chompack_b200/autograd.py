@@ -27,7 +27,15 @@ on the symbolic object, with per-set log dets from a segmented reduction.
 
 What the backward keeps is the factor L (the size of X per value set), not
 the fronts or update matrices of the forward sweep: the projected inverse
-needs only L, so no front has to be checkpointed or recomputed.
+needs only L.  Two options trade time for memory where that does not fit:
+`recompute_factor=True` keeps only X (which autograd holds anyway) and
+recomputes L by one more cholesky sweep in the backward, and
+`scratch_limit` (bytes) puts the update matrices of the cholesky and
+projected_inverse sweeps, by default several times the factor, in a shared
+pool of about that size (the plan option CHB_OPT_SCRATCH_LIMIT: fronts
+reuse the memory of update matrices already consumed, as the reference's
+postorder stack does, waiting for their readers).  Neither changes a bit
+of the results.
 """
 import torch
 
@@ -45,6 +53,14 @@ def _stream(dev):
 def _check(rc, what):
     if rc < 0:
         raise RuntimeError("%s failed: %s" % (what, N.last_error().decode()))
+
+
+def _limit_scratch(plan, limit):
+    """Sets a plan's scratch limit (bytes, None: no limit) when it changes
+    (changing it drops the plan's compiled programs)."""
+    if getattr(plan, "_scratch_limit", None) != limit:
+        plan.set_option("scratch_limit", limit)
+        plan._scratch_limit = limit
 
 
 def _factor(symb, x):
@@ -93,16 +109,24 @@ class _LogdetGrad(torch.autograd.Function):
 
 class _Logdet(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, symb):
+    def forward(ctx, x, symb, recompute):
         L = _factor(symb, x)
-        ctx.save_for_backward(x, L.blkval)
+        ctx.recompute = recompute
+        if recompute:
+            ctx.save_for_backward(x)
+        else:
+            ctx.save_for_backward(x, L.blkval)
         ctx.symb = symb
         return _logdet_of_factor(symb, L)
 
     @staticmethod
     def backward(ctx, g):
-        x, Lv = ctx.saved_tensors
-        return g * _LogdetGrad.apply(x, Lv, ctx.symb), None
+        if ctx.recompute:
+            (x,) = ctx.saved_tensors
+            Lv = _factor(ctx.symb, x).blkval
+        else:
+            x, Lv = ctx.saved_tensors
+        return g * _LogdetGrad.apply(x, Lv, ctx.symb), None, None
 
 
 def _value_sets(symb, count, device):
@@ -136,42 +160,58 @@ class _LogdetGradBatch(torch.autograd.Function):
         return Bt.sym_weight(U, -1.0).reshape(L.shape), None, None
 
 
+def _factor_sets(Bt, x):
+    L = x.detach().reshape(-1).clone()
+    Bt.cholesky(L)
+    return L.reshape(x.shape)
+
+
 class _LogdetBatch(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, symb):
+    def forward(ctx, x, symb, recompute):
         Bt = _value_sets(symb, x.shape[0], x.device)
-        L = x.detach().reshape(-1).clone()
-        Bt.cholesky(L)
-        L = L.reshape(x.shape)
-        ctx.save_for_backward(x, L)
+        L = _factor_sets(Bt, x)
+        ctx.recompute = recompute
+        if recompute:
+            ctx.save_for_backward(x)
+        else:
+            ctx.save_for_backward(x, L)
         ctx.symb = symb
         return Bt.logdet(L.reshape(-1))
 
     @staticmethod
     def backward(ctx, g):
-        x, L = ctx.saved_tensors
-        return g[:, None] * _LogdetGradBatch.apply(x, L, ctx.symb), None
+        if ctx.recompute:
+            (x,) = ctx.saved_tensors
+            L = _factor_sets(_value_sets(ctx.symb, x.shape[0], x.device), x)
+        else:
+            x, L = ctx.saved_tensors
+        return g[:, None] * _LogdetGradBatch.apply(x, L, ctx.symb), None, None
 
 
-def logdet_values(x, symb):
+def logdet_values(x, symb, scratch_limit=None, recompute_factor=False):
     """log det of the chordal SPD matrix with block values x (1-D, or
     (B, n_values) for B value sets on `symb`'s pattern, swept together),
-    differentiable (first and second order)."""
+    differentiable (first and second order).  scratch_limit: bytes for the
+    update matrices of the sweeps (None: each its own memory);
+    recompute_factor: keep only x for the backward and factor again there."""
     if not isinstance(x, torch.Tensor) or x.device.type != "cuda" or x.dtype != torch.float64:
         raise ValueError("values must be a float64 CUDA tensor")
     if x.dim() == 1:
-        return _Logdet.apply(x, symb)
+        _limit_scratch(symb.plan(x.device.index), scratch_limit)
+        return _Logdet.apply(x, symb, bool(recompute_factor))
     if x.dim() != 2 or x.shape[1] != int(symb.blkptr[-1]):
         raise ValueError("batched values must have shape (B, %d)" % int(symb.blkptr[-1]))
-    return _LogdetBatch.apply(x.contiguous(), symb)
+    _limit_scratch(_value_sets(symb, x.shape[0], x.device).plan, scratch_limit)
+    return _LogdetBatch.apply(x.contiguous(), symb, bool(recompute_factor))
 
 
-def logdet(X):
+def logdet(X, scratch_limit=None, recompute_factor=False):
     """log det of a cspmatrix X (not a factor), differentiable through
-    X.blkval."""
+    X.blkval (options as logdet_values)."""
     if X.is_factor is not False:
         raise ValueError("X must be a cspmatrix")
-    return logdet_values(X.blkval, X.symb)
+    return logdet_values(X.blkval, X.symb, scratch_limit, recompute_factor)
 
 
 def logdet_gradient(X):

@@ -52,6 +52,10 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     }
   }
   prog.ws_doubles = ws;
+  // pooled update matrices (under a scratch limit): U_k is first written by
+  // front k's extend-add tasks (or its one-task front, or its bundle) and
+  // dead once the parent's extend-add has read it
+  const std::vector<int> ubuf = pool_update_matrices(P, prog, B);
 
   // small subtrees: one warp per range, four ranges per task; the parent of
   // a range's root waits on the whole task (utask)
@@ -64,6 +68,13 @@ int build_cholesky(const chb_plan& P, Program& prog) {
     int id = B.add(bundle_task(P, bd, (int)b, T_SUBTREE), {P.fronts[r0].level, -1, 0, r0, 0, 0}, -1, bd.cost[b]);
     for (int r : bd.roots[b]) utask[r] = id;
   }
+  for (int64_t k = 0; k < N; k++)
+    if (bd.of[k] >= 0 && ubuf[k] >= 0) {
+      const int id = utask[bd.roots[bd.of[k]].front()];
+      const int p = P.fronts[k].parent;
+      B.pool_entry(ubuf[k], id);
+      if (p >= 0 && p < N && p != k && bd.of[p] == bd.of[k]) B.pool_exit_task(ubuf[k], id);
+    }
   auto wait_child = [&](int id, int c) {
     if (utask[c] >= 0) B.wait_task(id, utask[c]);
     else B.wait_group(id, uc_group[c]);
@@ -109,7 +120,11 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       t.c = opnd(B_WS, upd, std::max(na, 1));
       const double est = 3.0 + 0.02 * nn * (double)nj + 0.002 * (double)nj * nj;
       int id = B.add(t, {lv, -1, 0, (int)k, 0, 0}, uc_group[k], est);
-      for (int l = f.chbeg; l < f.chend; l++) wait_child(id, P.chidx[l]);
+      for (int l = f.chbeg; l < f.chend; l++) {
+        wait_child(id, P.chidx[l]);
+        B.pool_exit_task(ubuf[P.chidx[l]], id);
+      }
+      B.pool_entry(ubuf[k], id);
       continue;
     }
 
@@ -145,8 +160,10 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         // against 6.55 ms for w / 2000
         int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group, 3.0 + w / 1000.0);
         for (int l = f.chbeg; l < f.chend; l++) wait_child(id, P.chidx[l]);
+        B.pool_entry(ubuf[k], id);
         j0 = j1;
       }
+      for (int l = f.chbeg; l < f.chend; l++) B.pool_exit_group(ubuf[P.chidx[l]], asm_group);
     }
 
     last_top.assign((size_t)NBc * NBc, -1);
@@ -341,7 +358,9 @@ int build_cholesky(const chb_plan& P, Program& prog) {
       }
     }
   }
-  return B.finish(prog, P.grid > 0 ? P.grid : 296);
+  const int rc = B.finish(prog, P.grid > 0 ? P.grid : 296);
+  if (rc == 0) pooled_fronts(P, B, prog);
+  return rc;
 }
 
 }  // namespace chb

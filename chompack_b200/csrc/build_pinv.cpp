@@ -51,6 +51,12 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     return o;
   };
 
+  // pooled update matrices (under a scratch limit): V_k is first written by
+  // the parent's extract tasks (or the parent's one-task front, or k's
+  // bundle) and dead once k's S21 products and its own extract tasks, which
+  // read it, are done
+  const std::vector<int> ubuf = pool_update_matrices(P, prog, B);
+
   // group: the parent's extract tasks that produce V_k (k non-root); the
   // parent's own task when the parent is a small front
   std::vector<int> vready(N, -1);
@@ -65,6 +71,9 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
   // small subtrees: one warp per range, four ranges per task, each task
   // added once the parents of all its roots are (their V_k), parents first
   const Bundles bd = make_bundles(P);
+  std::vector<std::vector<int>> in_bundle(bd.tasks.size());
+  for (int64_t k = 0; k < N; k++)
+    if (bd.of[k] >= 0) in_bundle[bd.of[k]].push_back((int)k);
   std::vector<std::pair<int64_t, int>> pending;  // (smallest parent of a root, bundle)
   for (size_t b = 0; b < bd.tasks.size(); b++) {
     int64_t m = N;
@@ -86,6 +95,14 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       int id = B.add(t, {P.nlevels - P.fronts[r0].level, 0, 0, r0, 0, 0}, -1, 1.5 * bd.cost[b]);
       for (int r : bd.roots[b])
         if (P.fronts[r].na > 0) wait_v(id, r);
+      for (int q : in_bundle[b]) {
+        const int p = P.fronts[q].parent;
+        if (!(p >= 0 && p < N && p != q && bd.of[p] == b)) B.pool_exit_task(ubuf[q], id);  // a root: V from outside
+        else {
+          B.pool_entry(ubuf[q], id);
+          B.pool_exit_task(ubuf[q], id);
+        }
+      }
     }
   };
 
@@ -116,7 +133,11 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       for (int l = f.chbeg; l < f.chend; l++) est += 0.001 * P.fronts[P.chidx[l]].na * (double)P.fronts[P.chidx[l]].na;
       int id = B.add(t, {lv, 0, 0, (int)k, 0, 0}, -1, est);
       if (na > 0) wait_v(id, k);
-      for (int l = f.chbeg; l < f.chend; l++) vtask[P.chidx[l]] = id;
+      for (int l = f.chbeg; l < f.chend; l++) {
+        vtask[P.chidx[l]] = id;
+        B.pool_entry(ubuf[P.chidx[l]], id);
+      }
+      B.pool_exit_task(ubuf[k], id);
       continue;
     }
 
@@ -201,6 +222,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           for (int id : st.parts) wait_v(id, k);
         }
       }
+      B.pool_exit_group(ubuf[k], sgroup);
       // Y11 -= S21^T W (long K split)
       for (int i = 0; i < NBc; i++) {
         for (int j = 0; j <= i; j++) {
@@ -245,7 +267,9 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         int id = B.add(t, {lv, 5, 0, (int)k, c, q0}, vready[c], 3.0 + (double)(Nc - q0) * (q1 - q0) / 2000.0);
         B.wait_group(id, yfinal);
         B.wait_group(id, sgroup);
+        B.pool_entry(ubuf[c], id);
       }
+      B.pool_exit_group(ubuf[k], vready[c]);
     }
     // copy back into blkval (all readers of the factor block are done once
     // the final Y11 tiles are: they wait on every M tile and S21 tile), one
@@ -295,7 +319,9 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
   }
   prog.ws_doubles = ws;
   emit_bundles(-1);
-  return B.finish(prog, P.grid > 0 ? P.grid : 296);
+  const int rc = B.finish(prog, P.grid > 0 ? P.grid : 296);
+  if (rc == 0) pooled_fronts(P, B, prog);
+  return rc;
 }
 
 }  // namespace chb

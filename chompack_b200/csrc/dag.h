@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <queue>
 #include <string>
@@ -66,6 +67,51 @@ struct DagBuilder {
   std::vector<int32_t> early_owner;  // per group: owning task, or -1
   std::vector<int32_t> early_of;     // per task: its early group, or -1
   std::vector<double> early_at;      // per task: estimated time of the signal after its start
+
+  // Pooled update matrices (a scratch limit).  The builder lays the
+  // workspace out as [update matrices | per-front scratch], the update
+  // matrices in [0, pool_region), and declares each one as a buffer: its
+  // entry tasks touch it first (every other access waits on one of them)
+  // and it is dead once its exits (tasks, or groups complete) have run.
+  // finish() then places the buffers of at least pool_min doubles, in
+  // creation order, in a pool of at most pool_limit doubles where it can: a
+  // buffer that takes memory an earlier one held makes its entry tasks wait
+  // on that one's exits.  Memory is only taken from buffers whose exits
+  // were all created before the taker's entry tasks, so every added wait
+  // names an earlier task and the creation order stays topological.  Of the
+  // windows of memory it may take, a buffer takes one whose holders are
+  // done by its first use in the simulated list schedule, else (at the
+  // limit) the one that makes it wait least.  Smaller buffers keep memory of their own
+  // after the pool; the scratch beyond pool_region moves down behind them.
+  struct PoolBuf {
+    int64_t off = 0, size = 0;   // in the builder's layout (doubles)
+    std::vector<int> entry;      // task ids
+    std::vector<Wait> exit;      // tasks and groups
+    int64_t new_off = -1;        // placement
+  };
+  std::vector<PoolBuf> pool;
+  int64_t pool_limit = -1;       // doubles; < 0: no pooling
+  int64_t pool_min = 4096;       // smaller buffers are not pooled
+  int64_t pool_region = 0;
+  int64_t pool_doubles = 0;      // result: the pool's size
+  int64_t region_doubles = 0;    // result: pool + unpooled buffers
+  int64_t pool_waits = 0;        // result: reuse waits added
+
+  int pool_buffer(int64_t off, int64_t size) {
+    pool.emplace_back();
+    pool.back().off = off;
+    pool.back().size = size;
+    return (int)pool.size() - 1;
+  }
+  void pool_entry(int buf, int task) {
+    if (buf >= 0 && task >= 0) pool[buf].entry.push_back(task);
+  }
+  void pool_exit_task(int buf, int task) {
+    if (buf >= 0 && task >= 0) pool[buf].exit.push_back({task, 1, false});
+  }
+  void pool_exit_group(int buf, int group) {
+    if (buf >= 0 && group >= 0) pool[buf].exit.push_back({group, -1, true});
+  }
 
   int new_group() {
     group_size.push_back(0);
@@ -269,6 +315,152 @@ struct DagBuilder {
     }
   }
 
+  // Placement of the pooled buffers (see PoolBuf) from a simulated schedule
+  // (start and end time of every task), then the reuse waits and the
+  // workspace offsets of every task rewritten to the new layout.
+  int place_pool(Program& prog, const std::vector<double>& start, const std::vector<double>& endt,
+                 const std::vector<std::vector<int>>& members) {
+    const int nb = (int)pool.size();
+    std::vector<int> emin(nb, INT32_MAX), xmax(nb, -1);
+    std::vector<double> ta(nb, 0.0), tf(nb, 0.0);
+    std::vector<int> cand;
+    for (int b = 0; b < nb; b++) {
+      PoolBuf& p = pool[b];
+      if (p.off < 0 || p.size < 0 || p.off + p.size > pool_region)
+        return set_error(-24, "pooled buffer %d outside the update-matrix region", b);
+      double t0 = 1e300;
+      for (int e : p.entry) {
+        emin[b] = std::min(emin[b], e);
+        t0 = std::min(t0, start[e]);
+      }
+      for (const Wait& w : p.exit) {
+        if (w.is_group) {
+          for (int u : members[w.id]) {
+            xmax[b] = std::max(xmax[b], u);
+            tf[b] = std::max(tf[b], endt[u]);
+          }
+        } else {
+          xmax[b] = std::max(xmax[b], w.id);
+          tf[b] = std::max(tf[b], endt[w.id]);
+        }
+      }
+      ta[b] = t0;
+      if (p.size >= pool_min && !p.entry.empty() && xmax[b] >= 0) cand.push_back(b);
+    }
+    // in creation order, in which a buffer's memory becomes legal to take:
+    // the order of the reference's postorder stack for a bottom-up sweep
+    std::stable_sort(cand.begin(), cand.end(), [&](int x, int y) { return emin[x] < emin[y]; });
+    // the pool as contiguous blocks, each last held by `owner` (-1: never)
+    struct Blk {
+      int64_t off, size;
+      int owner;
+    };
+    std::vector<Blk> blks;
+    int64_t psize = 0;
+    for (int b : cand) {
+      const int64_t s = pool[b].size;
+      // best window of consecutive blocks from i: no delay, then least
+      // delay, then least growth of the pool, then least waste
+      int bi = -1, bj = -1;
+      double bdelay = 0.0;
+      int64_t bext = 0, bwaste = 0;
+      bool have = false;
+      for (int i = 0; i <= (int)blks.size(); i++) {
+        int64_t acc = 0;
+        double ready = -1e300;
+        bool ok = true;
+        int j = i;
+        for (; j < (int)blks.size() && acc < s; j++) {
+          const int o = blks[j].owner;
+          if (o >= 0 && xmax[o] >= emin[b]) {
+            ok = false;
+            break;
+          }
+          if (o >= 0) ready = std::max(ready, tf[o]);
+          acc += blks[j].size;
+        }
+        if (!ok) continue;
+        const int64_t ext = acc < s ? s - acc : 0;
+        if (ext > 0 && psize + ext > pool_limit && (have || i < (int)blks.size())) continue;
+        const double delay = std::max(0.0, ready - ta[b]);
+        const int64_t waste = acc > s ? acc - s : 0;
+        const bool better = !have || ((delay > 0.0) != (bdelay > 0.0) ? delay <= 0.0
+                                      : delay != bdelay ? delay < bdelay
+                                      : ext != bext ? ext < bext : waste < bwaste);
+        if (better) {
+          have = true;
+          bi = i;
+          bj = j;
+          bdelay = delay;
+          bext = ext;
+          bwaste = waste;
+        }
+        if (i == (int)blks.size()) break;
+      }
+      // waits on every earlier holder of the window, once per holder
+      std::vector<int> owners;
+      for (int j = bi; j < bj; j++)
+        if (blks[j].owner >= 0 && std::find(owners.begin(), owners.end(), blks[j].owner) == owners.end())
+          owners.push_back(blks[j].owner);
+      for (int o : owners)
+        for (int e : pool[b].entry)
+          for (const Wait& w : pool[o].exit) {
+            waits[e].push_back(w);
+            pool_waits++;
+          }
+      const int64_t off = bi < (int)blks.size() ? blks[bi].off : psize;
+      int64_t acc = 0;
+      for (int j = bi; j < bj; j++) acc += blks[j].size;
+      Blk nb_ = {off, s, b};
+      std::vector<Blk> repl(1, nb_);
+      if (acc > s) repl.push_back({off + s, acc - s, blks[bj - 1].owner});
+      blks.erase(blks.begin() + bi, blks.begin() + bj);
+      blks.insert(blks.begin() + bi, repl.begin(), repl.end());
+      if (acc < s) psize += s - acc;
+      pool[b].new_off = off;
+    }
+    // unpooled buffers after the pool, in their old order
+    int64_t next = psize;
+    std::vector<int> by_off(nb);
+    std::iota(by_off.begin(), by_off.end(), 0);
+    std::stable_sort(by_off.begin(), by_off.end(), [&](int x, int y) { return pool[x].off < pool[y].off; });
+    for (int b : by_off)
+      if (pool[b].new_off < 0) {
+        pool[b].new_off = next;
+        next += pool[b].size;
+      }
+    pool_doubles = psize;
+    region_doubles = next;
+    // rewrite the workspace offsets: inside a buffer -> its placement;
+    // past the region -> moved down; elsewhere in the region (operands of
+    // empty extents) -> 0
+    std::vector<int64_t> offs(nb);
+    for (int i = 0; i < nb; i++) offs[i] = pool[by_off[i]].off;
+    auto remap = [this, offs, by_off](int64_t o) -> int64_t {
+      if (o >= pool_region) return o - pool_region + region_doubles;
+      for (int i = (int)(std::upper_bound(offs.begin(), offs.end(), o) - offs.begin()) - 1; i >= 0; i--) {
+        const PoolBuf& p = pool[by_off[i]];  // p.off <= o
+        if (o < p.off + p.size) return p.new_off + (o - p.off);
+        if (p.size > 0) break;  // buffers do not overlap: o lies in none
+      }
+      return 0;
+    };
+    for (Task& t : tasks) {
+      if (t.off2 != 0) return set_error(-24, "pooled update matrices: task with an update-region offset");
+      for (Operand* o : {&t.a, &t.b, &t.c})
+        if (o->base == B_WS) o->off = remap(o->off);
+      if (t.op == T_MROW && t.aux[0] == B_WS) {
+        const int64_t m = remap((int64_t)(uint32_t)t.aux[2] | ((int64_t)t.aux[3] << 32));
+        t.aux[2] = (int32_t)(uint32_t)(m & 0xffffffffLL);
+        t.aux[3] = (int32_t)(m >> 32);
+      }
+    }
+    pool_remap = remap;
+    prog.ws_doubles -= pool_region - region_doubles;
+    return 0;
+  }
+  std::function<int64_t(int64_t)> pool_remap;
+
   // Sort into execution order and emit the device program.
   //
   // The order is the start order of a simulated list schedule on `slots`
@@ -286,7 +478,7 @@ struct DagBuilder {
     std::vector<std::vector<int>> members(ng);
     for (int t = 0; t < nt; t++)
       if (group_of[t] >= 0) members[group_of[t]].push_back(t);
-    std::vector<double> rank(nt, 0.0), start(nt, 0.0), extra(nt, 0.0);
+    std::vector<double> rank(nt, 0.0), start(nt, 0.0), extra(nt, 0.0), endt(nt, 0.0);
     auto compute_rank = [&]() {
       std::fill(rank.begin(), rank.end(), 0.0);
       // creation order is topological (every wait names an earlier task)
@@ -311,17 +503,23 @@ struct DagBuilder {
     // waiters of each task / group, and unmet wait counts
     std::vector<std::vector<int>> task_waiters(nt), group_waiters(ng);
     std::vector<int> unmet0(nt, 0);
-    for (int t = 0; t < nt; t++) {
-      for (const Wait& wt : waits[t]) {
-        if (wt.is_group) {
-          if (group_size[wt.id] == 0) continue;
-          group_waiters[wt.id].push_back(t);
-        } else {
-          task_waiters[wt.id].push_back(t);
+    auto find_waiters = [&]() {
+      for (auto& v : task_waiters) v.clear();
+      for (auto& v : group_waiters) v.clear();
+      std::fill(unmet0.begin(), unmet0.end(), 0);
+      for (int t = 0; t < nt; t++) {
+        for (const Wait& wt : waits[t]) {
+          if (wt.is_group) {
+            if (group_size[wt.id] == 0) continue;
+            group_waiters[wt.id].push_back(t);
+          } else {
+            task_waiters[wt.id].push_back(t);
+          }
+          unmet0[t]++;
         }
-        unmet0[t]++;
       }
-    }
+    };
+    find_waiters();
     std::vector<std::vector<int>> mid_waiters(nt);
     std::vector<int> mid_unmet0(nt, 0);
     for (int t = 0; t < nt; t++)
@@ -384,6 +582,7 @@ struct DagBuilder {
           free_slots++;
           done++;
           const int t = e.second;
+          endt[t] = now;
           if (post_cost[t] <= 0.0 || late_release[t])
             for (int w : task_waiters[t]) release(w);
           for (int w : mid_waiters[t])
@@ -400,6 +599,13 @@ struct DagBuilder {
     // (otherwise nothing waits on them and the schedule leaves them last).
     compute_rank();
     if (simulate() != 0) return -23;
+    if (pool_limit >= 0 && !pool.empty()) {
+      const int rc = place_pool(prog, start, endt, members);
+      if (rc) return rc;
+      find_waiters();
+      compute_rank();
+      if (simulate() != 0) return -23;
+    }
     if (!arrival_of_chunk.empty()) {
       // Incoming copies in earliest-deadline order: chunk j is due at the
       // latest start (critical path minus upward rank) of the first task
@@ -610,6 +816,44 @@ inline bool tf32_tcgen05(const chb_plan& P) {
 inline bool ordered_sums(const chb_plan& P) {
   if (P.opt[CHB_OPT_ORDERED_SUMS] >= 0) return P.opt[CHB_OPT_ORDERED_SUMS] != 0;
   return std::getenv("CHB_ORDERED_SUMS") != nullptr;
+}
+
+// Bytes for the update matrices of cholesky and projected_inverse
+// (CHB_OPT_SCRATCH_LIMIT, or CHB_SCRATCH_LIMIT in the environment; -1, the
+// default: no limit, each front's update matrix in memory of its own).
+inline int64_t scratch_limit_bytes(const chb_plan& P) {
+  const int64_t v = plan_option(P, CHB_OPT_SCRATCH_LIMIT, "CHB_SCRATCH_LIMIT", -1);
+  return v < 0 ? -1 : v;
+}
+
+// Sets a builder up to pool the update matrices under the plan's scratch
+// limit (nothing without one, or for a streamed program).  Returns the
+// buffer of each front's update matrix (-1: none).
+inline std::vector<int> pool_update_matrices(const chb_plan& P, const Program& prog, DagBuilder& B) {
+  std::vector<int> buf(P.nsn, -1);
+  const int64_t lim = scratch_limit_bytes(P);
+  if (lim < 0 || prog.io.in || prog.io.out) return buf;
+  B.pool_limit = lim / (int64_t)sizeof(double);
+  B.pool_region = P.upd_total;
+  // (CHB_SCRATCH_POOL_MIN: smallest pooled update matrix in doubles, default
+  // 4096; smaller ones keep their own memory, which keeps the placement's
+  // work near (pooled buffers)^2 for trees of many small fronts)
+  if (const char* e = std::getenv("CHB_SCRATCH_POOL_MIN")) B.pool_min = std::max<int64_t>(1, std::atoll(e));
+  for (int64_t k = 0; k < P.nsn; k++) {
+    const FrontDesc& f = P.fronts[k];
+    if (f.na > 0) buf[k] = B.pool_buffer(f.upd, (int64_t)f.na * f.na);
+  }
+  return buf;
+}
+
+// After finish(): the program's own supernode descriptors, with the pooled
+// offsets of the update matrices.
+inline void pooled_fronts(const chb_plan& P, const DagBuilder& B, Program& prog) {
+  if (B.pool_limit < 0 || B.pool.empty() || !B.pool_remap) return;
+  prog.fronts = P.fronts;
+  for (FrontDesc& f : prog.fronts) f.upd = f.na > 0 ? B.pool_remap(f.upd) : 0;
+  prog.pool_doubles = B.pool_doubles;
+  prog.pool_waits = B.pool_waits;
 }
 
 // cholesky's fused diagonal task (CHB_OPT_FUSED_LA = 1, the default where it

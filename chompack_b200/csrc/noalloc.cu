@@ -73,12 +73,14 @@ extern "C" int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream
   if (rc) return rc;
   Program* prog = build_host_program(plan, CHB_OP_CHOLESKY, 0, 0);
   if (!prog) return -2;
+  // the program's own update-matrix offsets under a scratch limit
+  const std::vector<FrontDesc>& fronts = prog->fronts.empty() ? plan->fronts : prog->fronts;
 
   // layout inside the static array
   const size_t ctl_off = 0;
   const size_t cnt_off = 256;
   const size_t fr_off = align256(cnt_off + (size_t)prog->ncounters * sizeof(int));
-  const size_t rel_off = align256(fr_off + plan->fronts.size() * sizeof(FrontDesc));
+  const size_t rel_off = align256(fr_off + fronts.size() * sizeof(FrontDesc));
   const size_t ch_off = align256(rel_off + plan->relidx.size() * sizeof(int32_t));
   const size_t tk_off = align256(ch_off + plan->chidx.size() * sizeof(int32_t));
   const size_t wt_off = align256(tk_off + prog->tasks.size() * sizeof(Task));
@@ -94,9 +96,9 @@ extern "C" int chb_cholesky_noalloc(chb_plan* plan, double* blkval, void* stream
   cudaStream_t stream = (cudaStream_t)stream_v;
   unsigned char* base = g_scratch_addr[dev];
   cudaError_t e = cudaMemsetAsync(base + ctl_off, 0, fr_off - ctl_off, stream);
-  if (e == cudaSuccess && !plan->fronts.empty())
-    e = cudaMemcpyAsync(base + fr_off, plan->fronts.data(), plan->fronts.size() * sizeof(FrontDesc),
-                        cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess && !fronts.empty())
+    e = cudaMemcpyAsync(base + fr_off, fronts.data(), fronts.size() * sizeof(FrontDesc), cudaMemcpyHostToDevice,
+                        stream);
   if (e == cudaSuccess && !plan->relidx.empty())
     e = cudaMemcpyAsync(base + rel_off, plan->relidx.data(), plan->relidx.size() * sizeof(int32_t),
                         cudaMemcpyHostToDevice, stream);

@@ -21,6 +21,7 @@ Program::~Program() {
   if (d_ctarget) cudaFree(d_ctarget);
   if (d_ready0) cudaFree(d_ready0);
   if (d_summ0) cudaFree(d_summ0);
+  if (d_fronts) cudaFree(d_fronts);
 }
 
 static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -61,6 +62,7 @@ static int upload_program(Program& prog) {
     return 0;
   };
   int rc = up(&prog.d_npend, prog.npend);
+  if (!rc) rc = up(&prog.d_fronts, prog.fronts);
   if (!rc) rc = up(&prog.d_succ_off, prog.succ_off);
   if (!rc) rc = up(&prog.d_succ, prog.succ);
   if (!rc) rc = up(&prog.d_ctarget, prog.ctarget);
@@ -236,7 +238,7 @@ int run_program(chb_plan* plan, Program* prog, void* work, size_t work_bytes, do
   ra.counters = (int*)(w + L.counters_off);
   for (int i = 0; i < nbases && i < MAX_BASES; i++) ra.bases[i] = bases[i];
   ra.bases[B_WS] = (double*)(w + L.dbl_off);
-  ra.fronts = plan->d_fronts;
+  ra.fronts = prog->d_fronts ? prog->d_fronts : plan->d_fronts;
   ra.relidx = plan->d_relidx;
   ra.chidx = plan->d_chidx;
   ra.spin_limit = plan->spin_limit >= 0 ? plan->spin_limit : kDefaultSpinLimit;
@@ -586,6 +588,17 @@ extern "C" int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, in
   return 0;
 }
 
+extern "C" int chb_program_pool(chb_plan* plan, int op, int64_t k, int flags, int64_t* info) {
+  clear_error();
+  if (!plan || !info) return set_error(-1, "null argument");
+  Program* p = build_host_program(plan, op, k, flags);
+  if (!p) return -2;
+  info[0] = p->fronts.empty() ? -1 : p->pool_doubles * (int64_t)sizeof(double);
+  info[1] = p->pool_waits;
+  info[2] = (int64_t)ws_layout(*p).total;
+  return 0;
+}
+
 extern "C" int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits,
                                   void* fronts) {
   clear_error();
@@ -594,7 +607,8 @@ extern "C" int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, 
   if (!p) return -2;
   if (tasks) std::memcpy(tasks, p->tasks.data(), p->tasks.size() * sizeof(Task));
   if (waits) std::memcpy(waits, p->waits.data(), p->waits.size() * sizeof(int2));
-  if (fronts) std::memcpy(fronts, plan->fronts.data(), plan->fronts.size() * sizeof(FrontDesc));
+  const std::vector<FrontDesc>& fr = p->fronts.empty() ? plan->fronts : p->fronts;
+  if (fronts) std::memcpy(fronts, fr.data(), fr.size() * sizeof(FrontDesc));
   return 0;
 }
 
@@ -671,6 +685,7 @@ extern "C" int chb_plan_get_option(const chb_plan* plan, int option, int64_t* va
     case CHB_OPT_FUSED_LA: *value = fused_la_allowed(*plan) ? 1 : 0; break;
     case CHB_OPT_TF32_TCGEN05: *value = tf32_tcgen05(*plan) ? 1 : 0; break;
     case CHB_OPT_ORDERED_SUMS: *value = ordered_sums(*plan) ? 1 : 0; break;
+    case CHB_OPT_SCRATCH_LIMIT: *value = scratch_limit_bytes(*plan); break;
     default: return set_error(-2, "unknown option %d", option);
   }
   return 0;

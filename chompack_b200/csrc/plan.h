@@ -42,6 +42,13 @@ struct Program {
   bool tf32_tiles = false;      // some GEMM tile computes in TF32 (one product)
   IoSpec io;                    // streaming of the values (set before building)
   std::vector<int> out_order;   // chunks in the list order of their signals
+  // Own layout of the update matrices (a scratch limit): the supernode
+  // descriptors with this program's update-matrix offsets (empty: the
+  // plan's), the pool's size and the reuse waits it took.
+  std::vector<FrontDesc> fronts;
+  FrontDesc* d_fronts = nullptr;
+  int64_t pool_doubles = 0;
+  int64_t pool_waits = 0;
   Task* d_tasks = nullptr;
   int2* d_waits = nullptr;
   // dynamic scheduling data (filled by DagBuilder::finish)
@@ -106,7 +113,7 @@ struct chb_plan {
   int grid_tc = 0;              // persistent grid size of the tcgen05 instantiation
   int schedule = -1;            // -1 default (CHB_SCHEDULE, else per sweep), 0 dynamic, 1 static list order
   int64_t spin_limit = -1;      // polls before a wait gives up; -1: the default (kDefaultSpinLimit)
-  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1, -1, -1};  // program-build options (-1: default)
+  int64_t opt[CHB_OPT_COUNT] = {-1, -1, -1, -1, -1, -1, -1, -1};  // program-build options (-1: default)
   unsigned long long* trace = nullptr;  // optional per-task timing buffer (device)
   int64_t trace_cap = 0;                // tasks it can hold
   std::map<chb::ProgKey, std::unique_ptr<chb::Program>> progs;

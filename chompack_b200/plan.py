@@ -106,14 +106,25 @@ class Plan(object):
     def set_option(self, name, value=None):
         """Program-build option of this plan's sweeps (chb_plan_set_option):
         "small_front_nj", "subtrees", "chol_ksplit", "pinv_ksplit",
-        "fused_la", "tf32_tcgen05" or "ordered_sums" (trsm's additions in a
-        fixed order, bit-reproducible); None restores the default.  Drops the compiled programs
-        (the device is synchronised first, so no sweep of the plan is in
-        flight)."""
+        "fused_la", "tf32_tcgen05", "ordered_sums" (trsm's additions in a
+        fixed order, bit-reproducible) or "scratch_limit" (bytes for the
+        update matrices of cholesky and projected_inverse, shared where the
+        schedule allows; see `pool_info`); None restores the default.
+        Drops the compiled programs (the device is synchronised first, so
+        no sweep of the plan is in flight)."""
         if self.device >= 0:
             torch.cuda.synchronize(self.device)
         v = -1 if value is None else int(value)
         N.check(N.plan_set_option(self.handle, N.OPTIONS[name], v), "plan_set_option")
+
+    def pool_info(self, op, k=0, flags=0):
+        """The update-matrix pool of a sweep's program under a scratch
+        limit: {"pool_bytes" (None without a pool), "reuse_waits",
+        "workspace_bytes"}."""
+        info = (ctypes.c_int64 * 3)()
+        N.check(N.program_pool(self.handle, op, int(k), int(flags), info), "program_pool")
+        return {"pool_bytes": None if info[0] < 0 else int(info[0]), "reuse_waits": int(info[1]),
+                "workspace_bytes": int(info[2])}
 
     def option(self, name):
         """The value the next program build uses for an option."""

@@ -36,11 +36,15 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32", "tf32x3"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--scratch-limit", default=None,
+                    help="bytes for the update matrices (plan option scratch_limit), or 'stack' for the "
+                         "reference's postorder stack size")
     args = ap.parse_args()
     if args.batch:
         return run_batch(args)
     A = grids.grid2d(args.side, seed=0) if args.grid2d else grids.grid3d(args.side, seed=0)
     s = symbolic(A, p=amd.order(A), merge_function=merge_size_fill(args.merge, args.merge))
+    limit = _scratch_limit(args, s)
     X0 = cspmatrix(s) + A
     base = X0.blkval
     if args.sweep == "trsm":
@@ -61,8 +65,22 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
-    print(json.dumps({"sweep": args.sweep, "precision": args.precision, "n": s.n, "nsn": s.Nsn,
-                      "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}))
+    out = {"sweep": args.sweep, "precision": args.precision, "n": s.n, "nsn": s.Nsn,
+           "ms": [round(t, 3) for t in times], "median_ms": round(float(np.median(times)), 3)}
+    if limit is not None:
+        from . import _native as N
+        op = N.OP_CHOLESKY if args.sweep == "cholesky" else N.OP_PROJECTED_INVERSE
+        out["scratch_limit"] = limit
+        out["pool"] = s.plan(base.device.index).pool_info(op)
+    print(json.dumps(out))
+
+
+def _scratch_limit(args, s):
+    if args.scratch_limit is None:
+        return None
+    limit = int(s.memory["stack_mem"]) * 8 if args.scratch_limit == "stack" else int(args.scratch_limit)
+    s.plan(torch.cuda.current_device()).set_option("scratch_limit", limit)
+    return limit
 
 
 def run_trsm(args, s, base):

@@ -162,6 +162,10 @@ int chb_program_io(chb_plan* plan, int op, int64_t k, int flags, int64_t* counts
  * the per-supernode descriptors into caller buffers of those sizes. */
 int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
 int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits, void* fronts);
+/* The update-matrix pool of a compiled sweep under CHB_OPT_SCRATCH_LIMIT:
+ * info[0..2] = the pool's bytes (-1: the program has no pool), the reuse
+ * waits it added, the workspace bytes of the program. */
+int chb_program_pool(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
 /* The dynamic-schedule data of a compiled sweep: sizes[0..5] = lengths of
  * the pending counts per task, the successor offsets per counter (counters
  * + 1), the successor list, the completion value per counter, the initial
@@ -376,6 +380,19 @@ int chb_plan_set_schedule(chb_plan* plan, int mode);
  *   CHB_OPT_ORDERED_SUMS    trsm: every addition into a vector block in a
  *                           fixed order (1: bit-reproducible, slower) or
  *                           with atomics as inputs arrive (0, the default)
+ *   CHB_OPT_SCRATCH_LIMIT   cholesky and projected_inverse: bytes for the
+ *                           update matrices of the fronts.  By default each
+ *                           front's update matrix has memory of its own
+ *                           (the sum over all fronts, several times the
+ *                           factor).  With a limit they share a pool of at
+ *                           most that size where the schedule allows: a
+ *                           front that takes memory another one held waits
+ *                           until that one's readers are done (memory the
+ *                           reference's stack, symbolic.py:634-661, reuses
+ *                           in postorder).  The pool grows past the limit
+ *                           only where no memory can be shared; the
+ *                           results are bit-identical to the unlimited
+ *                           layout.  chb_workspace_size reports the total.
  * chb_plan_get_option gives the value the next program build uses. */
 enum chb_option {
   CHB_OPT_SMALL_FRONT_NJ = 0,
@@ -385,7 +402,8 @@ enum chb_option {
   CHB_OPT_FUSED_LA = 4,
   CHB_OPT_TF32_TCGEN05 = 5,
   CHB_OPT_ORDERED_SUMS = 6,
-  CHB_OPT_COUNT = 7
+  CHB_OPT_SCRATCH_LIMIT = 7,
+  CHB_OPT_COUNT = 8
 };
 int chb_plan_set_option(chb_plan* plan, int option, int64_t value);
 int chb_plan_get_option(const chb_plan* plan, int option, int64_t* value);

@@ -1,0 +1,132 @@
+"""Update matrices under a scratch limit (CHB_OPT_SCRATCH_LIMIT), on the CPU.
+
+With a limit, cholesky and projected_inverse place the fronts' update
+matrices in a shared pool: a front that takes memory another front's update
+matrix held waits for that matrix's readers.  The task interpreter runs the
+pooled programs in random orders allowed by their waits (a missing reuse
+wait shows up as a wrong result: the workspace starts as NaN and a reused
+region holds another front's values) and under the dynamic release rules,
+against the oracle's C restatement of the reference's sweeps."""
+import os
+
+import numpy as np
+import pytest
+
+import chompack_b200 as cp
+from chompack_b200 import _native as N
+from chompack_b200.plan import Plan
+from helpers import problem, assert_blocks_close
+from oracle import oracle
+import taskvm
+
+# (kind, args, merge): fronts of several 64-column blocks (merged 3-D and
+# 2-D grids) and a tree of many small fronts in bundles (unmerged 3-D grid)
+CASES = [("grid3d", (10,), (32, 32)), ("grid2d", (70,), (64, 64)), ("grid3d", (12,), None)]
+
+
+@pytest.fixture(autouse=True)
+def _pool_every_matrix():
+    old = os.environ.get("CHB_SCRATCH_POOL_MIN")
+    os.environ["CHB_SCRATCH_POOL_MIN"] = "1"
+    yield
+    if old is None:
+        os.environ.pop("CHB_SCRATCH_POOL_MIN", None)
+    else:
+        os.environ["CHB_SCRATCH_POOL_MIN"] = old
+
+
+def _programs(s, op, limit):
+    pl = Plan(s, device=-1)
+    if limit is not None:
+        pl.set_option("scratch_limit", limit)
+    prog = taskvm.Program(pl.handle, op, nsn=s.Nsn)
+    sch = taskvm.Schedule(pl.handle, op)
+    return pl, prog, sch
+
+
+def _upd_bytes(s):
+    nn = np.diff(np.asarray(s.snptr))
+    na = np.diff(np.asarray(s.blkptr)) // nn - nn
+    return int((na.astype(np.int64) ** 2).sum()) * 8
+
+
+def _stack_bytes(s):
+    """The reference's postorder stack of update matrices (its largest
+    size), the least memory a sequential sweep needs."""
+    return int(s.memory["stack_mem"]) * 8
+
+
+@pytest.mark.parametrize("kind,args,merge", CASES)
+@pytest.mark.parametrize("limit", [0, "stack"])
+@pytest.mark.parametrize("order,seed", [("random", 0), ("random", 1), ("dynamic", 2)])
+def test_pooled_cholesky(kind, args, merge, limit, order, seed):
+    A, s = problem(kind, *args, merge=merge, seed=3)
+    lim = _stack_bytes(s) if limit == "stack" else limit
+    pl, prog, sch = _programs(s, N.OP_CHOLESKY, lim)
+    info = pl.pool_info(N.OP_CHOLESKY)
+    assert info["pool_bytes"] is not None and info["pool_bytes"] < _upd_bytes(s)
+    assert info["reuse_waits"] > 0
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    ref = x0.copy()
+    assert oracle.cholesky(s, ref) == 0
+    x = x0.copy()
+    bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, x, ref)
+
+
+@pytest.mark.parametrize("kind,args,merge", CASES)
+@pytest.mark.parametrize("limit", [0, "stack"])
+@pytest.mark.parametrize("order,seed", [("random", 3), ("dynamic", 4)])
+def test_pooled_projected_inverse(kind, args, merge, limit, order, seed):
+    A, s = problem(kind, *args, merge=merge, seed=3)
+    lim = _stack_bytes(s) if limit == "stack" else limit
+    pl, prog, sch = _programs(s, N.OP_PROJECTED_INVERSE, lim)
+    info = pl.pool_info(N.OP_PROJECTED_INVERSE)
+    assert info["pool_bytes"] is not None and info["pool_bytes"] < _upd_bytes(s)
+    L = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    assert oracle.cholesky(s, L) == 0
+    ref = L.copy()
+    assert oracle.projected_inverse(s, ref) == 0
+    x = L.copy()
+    bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+    assert taskvm.VM(prog, bases, s.relidx, s.chidx).run(order, seed=seed, schedule=sch) == 0
+    assert_blocks_close(s, x, ref)
+
+
+@pytest.mark.parametrize("op", [N.OP_CHOLESKY, N.OP_PROJECTED_INVERSE])
+def test_pool_shrinks_workspace(op):
+    """Without a limit there is no pool; with one the update matrices take
+    less memory than their sum, and a generous limit bounds the pool."""
+    A, s = problem("grid3d", 12, merge=None, seed=3)
+    total = _upd_bytes(s)
+    base = None
+    for lim in (None, total, 4 * _stack_bytes(s), _stack_bytes(s), 0):
+        pl = Plan(s, device=-1)
+        if lim is not None:
+            pl.set_option("scratch_limit", lim)
+        assert pl.option("scratch_limit") == (-1 if lim is None else lim)
+        info = pl.pool_info(op)
+        if lim is None:
+            assert info["pool_bytes"] is None and info["reuse_waits"] == 0
+            base = info["workspace_bytes"]
+            continue
+        assert info["pool_bytes"] < total
+        assert info["workspace_bytes"] < base
+        if lim >= total:
+            assert info["pool_bytes"] <= lim
+
+
+def test_pooled_program_same_arithmetic():
+    """A pooled program computes what the unpooled one does, in the same
+    order per task: the results in list order are bit-identical."""
+    A, s = problem("grid3d", 10, merge=(32, 32), seed=5)
+    x0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    out = []
+    for lim in (None, 0):
+        pl, prog, sch = _programs(s, N.OP_CHOLESKY, lim)
+        x = x0.copy()
+        bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+        assert taskvm.VM(prog, bases, s.relidx, s.chidx).run("list") == 0
+        out.append(x)
+    assert np.array_equal(out[0], out[1])

@@ -106,3 +106,20 @@ def test_noalloc_rejects_problems_beyond_the_static_scratch():
     rc = _noalloc(s.plan(Y.device.index), Y)
     assert rc == -40
     assert "limited to" in N.last_error().decode()
+
+
+def test_noalloc_under_a_scratch_limit():
+    """Under a scratch limit the program carries its own update-matrix
+    offsets (a pool); the allocation-free entry point stages those, and
+    the result is bit-identical to the unlimited layout."""
+    A, s = problem("grid3d", 12, merge=(32, 32), seed=13)
+    X = cp.cspmatrix(s) + A
+    plan = Plan(s, device=-1)
+    Y0 = X.blkval.clone()
+    assert _noalloc(plan, Y0) == 0, N.last_error().decode()
+    plan.set_option("scratch_limit", 0)
+    assert plan.pool_info(N.OP_CHOLESKY)["pool_bytes"] is not None
+    Y1 = X.blkval.clone()
+    assert _noalloc(plan, Y1) == 0, N.last_error().decode()
+    torch.cuda.synchronize()
+    assert torch.equal(Y0, Y1)
