@@ -54,8 +54,32 @@ int build_cholesky(const chb_plan& P, Program& prog) {
   prog.ws_doubles = ws;
   // pooled update matrices (under a scratch limit): U_k is first written by
   // front k's extend-add tasks (or its one-task front, or its bundle) and
-  // dead once the parent's extend-add has read it
+  // dead once the parent's extend-add has read it.  Front k's scratch
+  // (S_k, M_k and the split partials, contiguous) is pooled too: first
+  // touched after its extend-add tasks (or its first diagonal task), dead
+  // once its Schur complement (group uc_group[k]) and its blk21 products
+  // are done, or, for a front without update, its last diagonal task,
+  // which follows every other task of the front.
   const std::vector<int> ubuf = pool_update_matrices(P, prog, B);
+  std::vector<int> sbuf(N, -1);
+  if (B.pool_limit >= 0) {
+    for (int64_t k = 0; k < N; k++) {
+      int64_t lo = -1, hi = -1;
+      for (int64_t o : {scrS[k], scrM[k], scrK[k]})
+        if (o >= 0) lo = lo < 0 ? o : std::min(lo, o);
+      if (lo < 0) continue;
+      const FrontDesc& f = P.fronts[k];
+      hi = lo;
+      if (scrS[k] >= 0) hi = std::max(hi, scrS[k] + (int64_t)f.na * f.nn);
+      if (scrM[k] >= 0) hi = std::max(hi, scrM[k] + (int64_t)f.nn * f.nn);
+      if (scrK[k] >= 0) {
+        const int64_t NBb = ceil_div(f.na, T);
+        hi = std::max(hi, scrK[k] + NBb * (NBb + 1) / 2 * split_count(f.nn, kc) * (int64_t)T * T);
+      }
+      sbuf[k] = B.pool_buffer(lo, hi - lo);
+    }
+    B.pool_region = ws;
+  }
 
   // small subtrees: one warp per range, four ranges per task; the parent of
   // a range's root waits on the whole task (utask)
@@ -161,6 +185,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         int id = B.add(t, {lv, -1, 0, (int)k, j0, 0}, asm_group, 3.0 + w / 1000.0);
         for (int l = f.chbeg; l < f.chend; l++) wait_child(id, P.chidx[l]);
         B.pool_entry(ubuf[k], id);
+        B.pool_entry(sbuf[k], id);
         j0 = j1;
       }
       for (int l = f.chbeg; l < f.chend; l++) B.pool_exit_group(ubuf[P.chidx[l]], asm_group);
@@ -197,6 +222,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         if (fuse) t.k = bw(c + 1);
         const int gend = fuse ? B.new_group() : -1;
         pot = B.add(t, {lv, c, 0, (int)k, 0, 0}, gend);
+        if (c == 0 && asm_group < 0) B.pool_entry(sbuf[k], pot);
         if (c == 0) B.wait_group(pot, asm_group);
         else if (diag_end >= 0) B.wait_group(pot, diag_end);
         else B.wait_task(pot, last_top[(size_t)c * NBc + c]);
@@ -317,7 +343,13 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         }
       }
     }
-    if (na == 0) continue;
+    if (na == 0) {
+      B.pool_exit_task(sbuf[k], pot);
+      continue;
+    }
+    B.pool_exit_group(sbuf[k], uc_group[k]);
+    const int b21 = sbuf[k] >= 0 ? B.new_group() : -1;
+    B.pool_exit_group(sbuf[k], b21);
     // Schur complement U_k -= S_k S_k^T (cholesky.c:64-69); with a split
     // K the partial products are summed in a fixed order into U_k
     int64_t part = 0;
@@ -351,7 +383,7 @@ int build_cholesky(const chb_plan& P, Program& prog) {
         Operand mb = opnd(B_WS, M + (int64_t)jT * nn + jT, nn, OM_TRI_T, 0);
         Operand cc = opnd(B_X, blk + (int64_t)jT * nj + nn + iT, nj);
         Task t = gemm(bh(i), bw(j), nn - jT, 1.0, sa, mb, 0.0, cc);
-        int id = B.add(t, {lv, NBc, 1, (int)k, j, i});
+        int id = B.add(t, {lv, NBc, 1, (int)k, j, i}, b21);
         B.wait_task(id, trsmb[i]);
         B.wait_task(id, pot);
         if (j < NBc - 1) B.wait_task(id, last_mrow[j]);

@@ -116,6 +116,15 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
     const int lv = maxlv - f.level;  // roots first
     const int NBc = ceil_div(nn, T), NBb = ceil_div(na, T);
     const int64_t blk = f.blk, upd = f.upd, M = scrM[k], Y = scrY[k], S = scrS[k];
+    // front k's scratch under a scratch limit: [M | Y11 | S21] and the split
+    // partials it is handed below, first touched by the inverses of the
+    // diagonal tiles and the S21 products (every other task of the front
+    // waits on one of them), dead once the copies back and the extractions
+    // for the children, which read Y11 and S21 last, are done
+    const bool pool_scr = B.pool_limit >= 0;
+    const int64_t part0 = ws;
+    std::vector<int> scr_entry;
+    const int copies = pool_scr ? B.new_group() : -1;
     auto bw = [&](int c) { return std::min(T, nn - c * T); };
     auto bh = [&](int i) { return std::min(T, na - i * T); };
 
@@ -153,6 +162,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
       t.aux[1] = 1;
       t.aux[2] = 1;  // invert only
       inv[c] = B.add(t, {lv, 0, 0, (int)k, c, 0});
+      scr_entry.push_back(inv[c]);
     }
     // M below the diagonal tiles, right-looking by block column j: as soon
     // as M(l, j) is final, T(c, j) += L(c, l) M(l, j) for every c > l
@@ -219,7 +229,10 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
           Operand c = opnd(B_WS, S + (int64_t)jT * na + iT, na);
           Task t = gemm(bh(i), bw(j), na, -1.0, a, b, 0.0, c);
           SplitTask st = add_split_gemm(B, t, KSPLIT, scratch(t.k, KSPLIT), {lv, 3, 0, (int)k, j, i}, sgroup);
-          for (int id : st.parts) wait_v(id, k);
+          for (int id : st.parts) {
+            wait_v(id, k);
+            scr_entry.push_back(id);
+          }
         }
       }
       B.pool_exit_group(ubuf[k], sgroup);
@@ -285,7 +298,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         t.a = opnd(B_WS, Y + (int64_t)jT * nn + jT, nn);
         t.c = opnd(B_X, blk + (int64_t)jT * nj + jT, nj);
         t.aux[0] = 3;
-        int id = B.add(t, {lv, 6, 0, (int)k, j, j});
+        int id = B.add(t, {lv, 6, 0, (int)k, j, j}, copies);
         B.wait_group(id, yfinal);
       }
       if (jT + T < nn) {
@@ -294,7 +307,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         t.n = bw(j);
         t.a = opnd(B_WS, Y + (int64_t)jT * nn + jT + T, nn);
         t.c = opnd(B_X, blk + (int64_t)jT * nj + jT + T, nj);
-        int id = B.add(t, {lv, 6, 0, (int)k, j, j + 1}, -1, 3.0 + (double)t.m * t.n / 4096.0);
+        int id = B.add(t, {lv, 6, 0, (int)k, j, j + 1}, copies, 3.0 + (double)t.m * t.n / 4096.0);
         B.wait_group(id, yfinal);
       }
       if (jT > 0) {
@@ -303,7 +316,7 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         t.n = bw(j);
         t.aux[0] = 4;  // zeros
         t.c = opnd(B_X, blk + (int64_t)jT * nj, nj);
-        int id = B.add(t, {lv, 6, 1, (int)k, j, 0}, -1, 3.0 + (double)t.m * t.n / 8192.0);
+        int id = B.add(t, {lv, 6, 1, (int)k, j, 0}, copies, 3.0 + (double)t.m * t.n / 8192.0);
         B.wait_group(id, yfinal);
       }
       if (na > 0) {
@@ -312,12 +325,23 @@ int build_projected_inverse(const chb_plan& P, Program& prog) {
         t.n = bw(j);
         t.a = opnd(B_WS, S + (int64_t)jT * na, na);
         t.c = opnd(B_X, blk + (int64_t)jT * nj + nn, nj);
-        int id = B.add(t, {lv, 6, 2, (int)k, j, 0}, -1, 3.0 + (double)t.m * t.n / 4096.0);
+        int id = B.add(t, {lv, 6, 2, (int)k, j, 0}, copies, 3.0 + (double)t.m * t.n / 4096.0);
         B.wait_group(id, yfinal);
+      }
+    }
+    if (pool_scr) {
+      const int main_buf = B.pool_buffer(M, (S >= 0 ? S + (int64_t)na * nn : Y + (int64_t)nn * nn) - M);
+      const int part_buf = ws > part0 ? B.pool_buffer(part0, ws - part0) : -1;
+      for (int b : {main_buf, part_buf}) {
+        if (b < 0) continue;
+        for (int id : scr_entry) B.pool_entry(b, id);
+        B.pool_exit_group(b, copies);
+        for (int l = f.chbeg; l < f.chend; l++) B.pool_exit_group(b, vready[P.chidx[l]]);
       }
     }
   }
   prog.ws_doubles = ws;
+  if (B.pool_limit >= 0) B.pool_region = ws;
   emit_bundles(-1);
   const int rc = B.finish(prog, P.grid > 0 ? P.grid : 296);
   if (rc == 0) pooled_fronts(P, B, prog);
