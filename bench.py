@@ -601,10 +601,12 @@ def autograd_section(dev, side=32, value_sets=16, reps=5, h=1e-6):
 def autograd_memory(dev, s, x0, reps, g_default):
     """Memory against time for the autograd workload: the sweeps' workspace
     (update matrices, per-front scratch, counters) with every update matrix
-    in memory of its own (the default), and with them in a pool limited to
-    the reference's postorder stack size per value set (plan option
-    scratch_limit); the forward + backward time with that limit, and with
-    the factor recomputed in the backward instead of kept (recompute_factor).
+    in memory of its own (the default), and with them in a pool (plan option
+    scratch_limit) limited to the reference's postorder stack size per value
+    set, or unlimited (2^40 bytes: the pool reuses only memory the simulated
+    schedule has freed, no added delay); the forward + backward time with
+    each, and with the factor recomputed in the backward instead of kept
+    (recompute_factor).
     Each variant's gradient must be bit-identical to the default's."""
     import torch
     from chompack_b200 import _native as N, autograd
@@ -626,12 +628,15 @@ def autograd_memory(dev, s, x0, reps, g_default):
     out = {"update_matrices_bytes": int(sum(int(f) ** 2 for f in _update_orders(s))) * 8 * sets,
            "reference_stack_bytes": limit, "factor_kept_bytes": nv * 8 * sets,
            "default": {"workspace_bytes": workspace()}}
-    for label, kw in (("scratch_limit", {"scratch_limit": limit}), ("recompute_factor", {"recompute_factor": True})):
+    variants = (("scratch_limit", {"scratch_limit": limit}),
+                ("scratch_limit_no_delay", {"scratch_limit": 1 << 40}),
+                ("recompute_factor", {"recompute_factor": True}))
+    for label, kw in variants:
         ms = _event_ms(dev, lambda: run(**kw), reps)
         g = run(**kw)
         entry = {"fwd_bwd_ms": round(ms, 3), "gradient_bit_identical": bool(torch.equal(g, g_default))}
         if "scratch_limit" in kw:
-            entry["scratch_limit_bytes"] = limit
+            entry["scratch_limit_bytes"] = kw["scratch_limit"]
             entry["workspace_bytes"] = workspace()
             entry["pool_bytes"] = {name: Bt.plan.pool_info(op)["pool_bytes"] for name, op in ops}
         else:

@@ -37,8 +37,8 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--scratch-limit", default=None,
-                    help="bytes for the update matrices (plan option scratch_limit), or 'stack' for the "
-                         "reference's postorder stack size")
+                    help="bytes for the update matrices and fronts' scratch (plan option scratch_limit), or "
+                         "'stack' / '<m>stack' for (m times) the reference's postorder stack size")
     args = ap.parse_args()
     if args.batch:
         return run_batch(args)
@@ -78,7 +78,11 @@ def main():
 def _scratch_limit(args, s):
     if args.scratch_limit is None:
         return None
-    limit = int(s.memory["stack_mem"]) * 8 if args.scratch_limit == "stack" else int(args.scratch_limit)
+    v = args.scratch_limit
+    if v.endswith("stack"):   # "stack", "2stack", ...: multiples of the reference's stack size
+        limit = int(float(v[:-5] or 1) * int(s.memory["stack_mem"]) * 8)
+    else:
+        limit = int(v)
     s.plan(torch.cuda.current_device()).set_option("scratch_limit", limit)
     return limit
 
