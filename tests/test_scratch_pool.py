@@ -136,3 +136,34 @@ def test_pooled_program_same_arithmetic():
         assert taskvm.VM(prog, bases, s.relidx, s.chidx).run("list") == 0
         out.append(x)
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_pooled_merged_plan(seed):
+    """A merged plan (three trees: two value sets on one pattern and a
+    second pattern) under a scratch limit: buffers of one tree take memory
+    of another's, and random orders still give each tree's results."""
+    from chompack_b200.batch import batch
+    A1, s1 = problem("grid3d", 9, merge=(32, 32), seed=3)
+    A2, s2 = problem("grid2d", 40, merge=(16, 16), seed=4)
+    symbs, As = [s1, s2, s1], [A1, A2, A1]
+    Bt = batch(symbs, device=-1)
+    Bt.plan.set_option("scratch_limit", 0)
+    info = Bt.plan.pool_info(N.OP_CHOLESKY)
+    assert info["pool_bytes"] is not None and info["reuse_waits"] > 0
+    relidx = np.concatenate([np.asarray(s.relidx) for s in symbs])
+    chidx = np.concatenate([np.asarray(s.chidx) + off for s, off in
+                            zip(symbs, np.cumsum([0] + [s.Nsn for s in symbs[:-1]]))])
+    xs = [(cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy() for s, A in zip(symbs, As)]
+    xs[2] = np.where(xs[2] != 0, xs[2] * 1.25, 0.0)
+    x = np.concatenate(xs)
+    nsn = Bt.plan.batch_segments()[-1]
+    for op, fn in ((N.OP_CHOLESKY, oracle.cholesky), (N.OP_PROJECTED_INVERSE, oracle.projected_inverse)):
+        prog = taskvm.Program(Bt.plan.handle, op, nsn=nsn)
+        sch = taskvm.Schedule(Bt.plan.handle, op)
+        bases = {0: x, 1: np.full(prog.ws_doubles, np.nan)}
+        order = "random" if op == N.OP_CHOLESKY else "dynamic"
+        assert taskvm.VM(prog, bases, relidx, chidx).run(order, seed=seed, schedule=sch) == 0
+        for m, s in enumerate(symbs):
+            assert fn(s, xs[m]) == 0
+            assert_blocks_close(s, x[Bt.offsets[m]:Bt.offsets[m + 1]], xs[m])
