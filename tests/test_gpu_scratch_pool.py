@@ -110,3 +110,24 @@ def test_logdet_scratch_limit_and_recompute():
         assert np.array_equal(r[1], res[0][1])
         assert np.array_equal(r[2], res[0][2])
         assert np.array_equal(r[3], res[0][3])
+
+
+@pytest.mark.parametrize("precision", ["tf32", "tf32x3"])
+def test_pooled_mixed_precision_bit_identical(precision):
+    """The mixed-precision programs (TF32 GEMM tiles) take the limit too,
+    with bit-identical results."""
+    A, s = problem("grid3d", 16, merge=(32, 32), seed=5)
+    blk0 = (cp.cspmatrix(s, device="cpu") + A).blkval.numpy().copy()
+    pl = s.plan(0)
+    out = []
+    for limit in (None, 0):
+        pl.set_option("scratch_limit", limit)
+        X = cp.cspmatrix(s, blkval=torch.from_numpy(blk0.copy()).cuda(), factor=False)
+        cp.cholesky(X, precision=precision)
+        L = X.blkval.clone()
+        cp.projected_inverse(X, precision=precision)
+        torch.cuda.synchronize()
+        out.append((L.cpu().numpy(), X.blkval.cpu().numpy()))
+    pl.set_option("scratch_limit", None)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
