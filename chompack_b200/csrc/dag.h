@@ -96,6 +96,7 @@ struct DagBuilder {
   int64_t pool_doubles = 0;      // result: the pool's size
   int64_t region_doubles = 0;    // result: pool + unpooled buffers
   int64_t pool_waits = 0;        // result: reuse waits added
+  static constexpr int POOL_PASSES = 3;
 
   int pool_buffer(int64_t off, int64_t size) {
     pool.emplace_back();
@@ -316,11 +317,12 @@ struct DagBuilder {
   }
 
   // Placement of the pooled buffers (see PoolBuf) from a simulated schedule
-  // (start and end time of every task), then the reuse waits and the
-  // workspace offsets of every task rewritten to the new layout.
-  int place_pool(Program& prog, const std::vector<double>& start, const std::vector<double>& endt,
+  // (start and end time of every task), with the reuse waits it needs.
+  int place_pool(const std::vector<double>& start, const std::vector<double>& endt,
                  const std::vector<std::vector<int>>& members) {
     const int nb = (int)pool.size();
+    pool_waits = 0;
+    for (PoolBuf& p : pool) p.new_off = -1;
     std::vector<int> emin(nb, INT32_MAX), xmax(nb, -1);
     std::vector<double> ta(nb, 0.0), tf(nb, 0.0);
     std::vector<int> cand;
@@ -431,6 +433,15 @@ struct DagBuilder {
       }
     pool_doubles = psize;
     region_doubles = next;
+    return 0;
+  }
+
+  // The workspace offsets of every task rewritten to the placed layout.
+  int remap_pool(Program& prog) {
+    const int nb = (int)pool.size();
+    std::vector<int> by_off(nb);
+    std::iota(by_off.begin(), by_off.end(), 0);
+    std::stable_sort(by_off.begin(), by_off.end(), [&](int x, int y) { return pool[x].off < pool[y].off; });
     // rewrite the workspace offsets: inside a buffer -> its placement;
     // past the region -> moved down; elsewhere in the region (operands of
     // empty extents) -> 0
@@ -600,7 +611,37 @@ struct DagBuilder {
     compute_rank();
     if (simulate() != 0) return -23;
     if (pool_limit >= 0 && !pool.empty()) {
-      const int rc = place_pool(prog, start, endt, members);
+      // a few placements, each from the simulated schedule of the one
+      // before (the first from the schedule without reuse waits); the one
+      // whose simulated schedule ends first is kept
+      const std::vector<std::vector<Wait>> plain = waits;
+      std::vector<std::vector<Wait>> best_waits;
+      std::vector<int64_t> best_off(pool.size());
+      int64_t best_psize = 0, best_region = 0, best_nw = 0;
+      double best_span = 0.0;
+      for (int pass = 0; pass < POOL_PASSES; pass++) {
+        if (pass > 0) waits = plain;
+        const int rc = place_pool(start, endt, members);
+        if (rc) return rc;
+        find_waiters();
+        compute_rank();
+        if (simulate() != 0) return -23;
+        const double span = *std::max_element(endt.begin(), endt.end());
+        if (pass == 0 || span < best_span) {
+          best_span = span;
+          best_waits = waits;
+          for (size_t b = 0; b < pool.size(); b++) best_off[b] = pool[b].new_off;
+          best_psize = pool_doubles;
+          best_region = region_doubles;
+          best_nw = pool_waits;
+        }
+      }
+      waits.swap(best_waits);
+      for (size_t b = 0; b < pool.size(); b++) pool[b].new_off = best_off[b];
+      pool_doubles = best_psize;
+      region_doubles = best_region;
+      pool_waits = best_nw;
+      const int rc = remap_pool(prog);
       if (rc) return rc;
       find_waiters();
       compute_rank();
@@ -650,6 +691,7 @@ struct DagBuilder {
       compute_rank();
       if (simulate() != 0) return -23;
     }
+    prog.sim_span_us = nt > 0 ? *std::max_element(endt.begin(), endt.end()) : 0.0;
     std::vector<int> order(nt);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {

@@ -596,6 +596,7 @@ extern "C" int chb_program_pool(chb_plan* plan, int op, int64_t k, int flags, in
   info[0] = p->fronts.empty() ? -1 : p->pool_doubles * (int64_t)sizeof(double);
   info[1] = p->pool_waits;
   info[2] = (int64_t)ws_layout(*p).total;
+  info[3] = (int64_t)(p->sim_span_us * 1000.0);
   return 0;
 }
 

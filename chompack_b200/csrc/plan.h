@@ -49,6 +49,7 @@ struct Program {
   FrontDesc* d_fronts = nullptr;
   int64_t pool_doubles = 0;
   int64_t pool_waits = 0;
+  double sim_span_us = 0.0;  // span of the simulated list schedule that ordered the tasks
   Task* d_tasks = nullptr;
   int2* d_waits = nullptr;
   // dynamic scheduling data (filled by DagBuilder::finish)

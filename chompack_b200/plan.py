@@ -120,11 +120,12 @@ class Plan(object):
     def pool_info(self, op, k=0, flags=0):
         """The update-matrix pool of a sweep's program under a scratch
         limit: {"pool_bytes" (None without a pool), "reuse_waits",
-        "workspace_bytes"}."""
-        info = (ctypes.c_int64 * 3)()
+        "workspace_bytes", "model_span_us" (the span of the planner's
+        simulated schedule, a model, not a measurement)}."""
+        info = (ctypes.c_int64 * 4)()
         N.check(N.program_pool(self.handle, op, int(k), int(flags), info), "program_pool")
         return {"pool_bytes": None if info[0] < 0 else int(info[0]), "reuse_waits": int(info[1]),
-                "workspace_bytes": int(info[2])}
+                "workspace_bytes": int(info[2]), "model_span_us": info[3] / 1000.0}
 
     def option(self, name):
         """The value the next program build uses for an option."""

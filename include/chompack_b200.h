@@ -163,8 +163,10 @@ int chb_program_io(chb_plan* plan, int op, int64_t k, int flags, int64_t* counts
 int chb_program_info(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
 int chb_program_export(chb_plan* plan, int op, int64_t k, int flags, void* tasks, void* waits, void* fronts);
 /* The update-matrix pool of a compiled sweep under CHB_OPT_SCRATCH_LIMIT:
- * info[0..2] = the pool's bytes (-1: the program has no pool), the reuse
- * waits it added, the workspace bytes of the program. */
+ * info[0..3] = the pool's bytes (-1: the program has no pool), the reuse
+ * waits it added, the workspace bytes of the program, and the span (ns) of
+ * the simulated list schedule that ordered its tasks (the planner's model,
+ * not a measurement). */
 int chb_program_pool(chb_plan* plan, int op, int64_t k, int flags, int64_t* info);
 /* The dynamic-schedule data of a compiled sweep: sizes[0..5] = lengths of
  * the pending counts per task, the successor offsets per counter (counters
