@@ -96,7 +96,7 @@ struct DagBuilder {
   int64_t pool_doubles = 0;      // result: the pool's size
   int64_t region_doubles = 0;    // result: pool + unpooled buffers
   int64_t pool_waits = 0;        // result: reuse waits added
-  static constexpr int POOL_PASSES = 3;
+  static constexpr int POOL_PASSES = 6;
 
   int pool_buffer(int64_t off, int64_t size) {
     pool.emplace_back();
