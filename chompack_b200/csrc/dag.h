@@ -81,7 +81,9 @@ struct DagBuilder {
   // names an earlier task and the creation order stays topological.  Of the
   // windows of memory it may take, a buffer takes one whose holders are
   // done by its first use in the simulated list schedule, else (at the
-  // limit) the one that makes it wait least.  Smaller buffers keep memory of their own
+  // limit) the one that makes it wait least.  finish() makes POOL_PASSES
+  // placements, each from the simulated schedule of the one before, and
+  // keeps the one whose simulated schedule ends first.  Smaller buffers keep memory of their own
   // after the pool; the scratch beyond pool_region moves down behind them.
   struct PoolBuf {
     int64_t off = 0, size = 0;   // in the builder's layout (doubles)
