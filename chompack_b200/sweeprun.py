@@ -10,7 +10,11 @@ with --grid2d) with AMD ordering and merge_size_fill(merge, merge), or with
 with two extra neighbours per node, AMD, no merging) in one merged plan;
 each repetition refreshes the values and launches the sweep once
 (projected_inverse and trsm run on the factor of a preceding, untimed
-cholesky; trsm on --nrhs seeded N(0,1) right-hand sides).
+cholesky; trsm on --nrhs seeded N(0,1) right-hand sides).  With
+--scratch-limit (bytes, or 'stack' / '<m>stack' for m times the
+reference's postorder stack size) the update matrices and the fronts'
+scratch share a pool of about that size; the line then also reports the
+pool (chb_program_pool).
 """
 import argparse
 import json
