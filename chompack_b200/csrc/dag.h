@@ -83,7 +83,8 @@ struct DagBuilder {
   // done by its first use in the simulated list schedule, else (at the
   // limit) the one that makes it wait least.  finish() makes POOL_PASSES
   // placements, each from the simulated schedule of the one before, and
-  // keeps the one whose simulated schedule ends first.  Smaller buffers keep memory of their own
+  // keeps the one whose simulated schedule ends first among those that
+  // take at most 5 % more memory than the first placement or the limit.  Smaller buffers keep memory of their own
   // after the pool; the scratch beyond pool_region moves down behind them.
   struct PoolBuf {
     int64_t off = 0, size = 0;   // in the builder's layout (doubles)
@@ -98,7 +99,7 @@ struct DagBuilder {
   int64_t pool_doubles = 0;      // result: the pool's size
   int64_t region_doubles = 0;    // result: pool + unpooled buffers
   int64_t pool_waits = 0;        // result: reuse waits added
-  static constexpr int POOL_PASSES = 6;
+  static constexpr int POOL_PASSES = 10;
 
   int pool_buffer(int64_t off, int64_t size) {
     pool.emplace_back();
@@ -621,6 +622,7 @@ struct DagBuilder {
       std::vector<int64_t> best_off(pool.size());
       int64_t best_psize = 0, best_region = 0, best_nw = 0;
       double best_span = 0.0;
+      int64_t first_region = 0;
       for (int pass = 0; pass < POOL_PASSES; pass++) {
         if (pass > 0) waits = plain;
         const int rc = place_pool(start, endt, members);
@@ -628,8 +630,12 @@ struct DagBuilder {
         find_waiters();
         compute_rank();
         if (simulate() != 0) return -23;
+        // (a pass may take at most 5 % more memory than the first one, or
+        // than the limit)
         const double span = *std::max_element(endt.begin(), endt.end());
-        if (pass == 0 || span < best_span) {
+        if (pass == 0) first_region = region_doubles;
+        const bool fits = (double)region_doubles <= 1.05 * (double)std::max(first_region, pool_limit);
+        if (pass == 0 || (span < best_span && fits)) {
           best_span = span;
           best_waits = waits;
           for (size_t b = 0; b < pool.size(); b++) best_off[b] = pool[b].new_off;
